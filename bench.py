@@ -1,0 +1,432 @@
+#!/usr/bin/env python3
+"""Benchmark: verified signatures per second on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one pass of the hot path over one batch: one launch that verifies
+the 1,048,576-signature BIP-340 batch (seeded keys, 32-byte x-only keys,
+uniform messages, seeded aux_rand; 1% of signatures with one flipped bit in
+s or R.x, 0.1% of keys off the curve).  Signatures are made on the GPU by the
+library's batch signer (byte-identical to the reference's CPU signer; checked
+by the tests).
+
+* value: whole-job sigs/s with inputs resident in HBM (device-pointer entry
+  ufsecp_gpu_ext_schnorr_verify_device), CUDA events on the launching stream,
+  max over ranks.
+* e2e: the same work through the reference ABI call
+  ufsecp_gpu_schnorr_verify_batch with host buffers, copies included.
+* roofline: integer-pipe (IMAD) bound; achieved = sigs/s x the canonical
+  3.33e5 IMAD-class ops per signature, against the device's IMAD issue rate
+  measured in this run; HBM bytes of the same launch beside it.
+* cpu_baseline: the reference library (oracle/_ref, compiled from the
+  reference sources) on all host threads over a bounded sample.
+Multi-GPU: one process per GPU (torchrun), every rank verifies its own batch
+(weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "verified sigs/sec on 1 B200 (ECDSA, BIP-340) batched vs plain kernel; p50/p99"
+N_ORDER = 0xFFFFFFFFFFFFFFFFFFFFFFFFFFFFFFFEBAAEDCE6AF48A03BBFD25E8CD0364141
+P_FIELD = 2**256 - 2**32 - 977
+W_SIG = 3.33e5            # IMAD-class ops per verified signature (canonical work model)
+BYTES_PER_SIG = 32 + 32 + 64 + 1
+BATCH = 1 << 20
+CPU_SAMPLE = 200_000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers --
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def profile_traffic():
+    """dram bytes per launch of the verify kernel from the committed ncu summary."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clk", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+def offcurve_x(rng):
+    while True:
+        x = int.from_bytes(rng.bytes(32), "big") % P_FIELD
+        if pow((x**3 + 7) % P_FIELD, (P_FIELD - 1) // 2, P_FIELD) != 1:
+            return x
+
+
+def tamper(rng, xs, sigs, expect):
+    """1% of items: one flipped bit in s or R.x; 0.1%: x-only key off the curve."""
+    n = xs.shape[0]
+    idx = rng.choice(n, size=n // 100, replace=False)
+    for i in idx:
+        bit = int(rng.integers(0, 256))
+        off = 0 if rng.integers(0, 2) else 32
+        sigs[i, off + bit // 8] ^= 1 << (bit % 8)
+    expect[idx] = 0
+    idx = rng.choice(n, size=max(1, n // 1000), replace=False)
+    for i in idx:
+        xs[i] = np.frombuffer(offcurve_x(rng).to_bytes(32, "big"), np.uint8)
+    expect[idx] = 0
+
+
+def make_schnorr_batch(ctx, torch, n: int, seed: int):
+    """Seeded BIP-340 batch, signed on the GPU; returns device tensors, host
+    copies and the verdict every item must get (by construction)."""
+    rng = np.random.default_rng(seed)
+    sks = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    # keys uniform in [1, n-1]: redraw the (astronomically rare) values outside
+    hi = sks[:, 0] == 0xFF
+    for i in np.nonzero(hi)[0]:
+        while not (0 < int.from_bytes(sks[i].tobytes(), "big") < N_ORDER):
+            sks[i] = rng.integers(0, 256, 32, dtype=np.uint8)
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    aux = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    d_msgs, d_sks, d_aux = dev(msgs), dev(sks), dev(aux)
+    d_xs = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+    d_sigs = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+    d_ok = torch.empty(n, dtype=torch.uint8, device="cuda")
+    ctx.sign_device(1, d_msgs.data_ptr(), d_sks.data_ptr(), d_aux.data_ptr(), n, d_xs.data_ptr(),
+                    d_sigs.data_ptr(), d_ok.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert bool(d_ok.all()), "signer rejected a key"
+    del d_sks, d_aux
+    xs = d_xs.cpu().numpy().reshape(n, 32)
+    sigs = d_sigs.cpu().numpy().reshape(n, 64)
+    expect = np.ones(n, np.uint8)
+    tamper(rng, xs, sigs, expect)
+    d_xs = dev(xs)
+    d_sigs = dev(sigs)
+    d_out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    return (d_msgs, d_xs, d_sigs, d_out), (msgs, xs, sigs), expect
+
+
+def cpu_reference_rate(msgs, xs, sigs, sample: int):
+    """Reference library, all host threads, ufsecp_schnorr_verify per signature."""
+    from oracle import RefDriver
+    drv = RefDriver()
+    threads = os.cpu_count() or 1
+    m, x, s = msgs[:sample], xs[:sample], sigs[:sample]
+    drv.verify(1, m[:2048], x[:2048], s[:2048], threads)          # one-time table set-up
+    t0 = time.perf_counter()
+    verdicts = drv.verify(1, m, x, s, threads)
+    dt = time.perf_counter() - t0
+    return sample / dt, threads, verdicts, dt
+
+
+# -------------------------------------------------------------- reference arm --
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import REF_SO, RefDriver
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+        return 0
+    # the reference arm makes its corpus with the reference's own signer, same seeds and tamper rules
+    drv = RefDriver()
+    threads = os.cpu_count() or 1
+    n = min(args.batch, 1 << 17)
+    rng = np.random.default_rng(20261203)
+    sks = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    aux = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    xs, sigs, ok = drv.sign(1, msgs, sks, aux, threads)
+    expect = ok.copy()
+    tamper(rng, xs, sigs, expect)
+    per_step = min(n, max(8192, 1500 * threads))
+    drv.verify(1, msgs[:2048], xs[:2048], sigs[:2048], threads)
+    for _ in range(args.warmup):
+        drv.verify(1, msgs[:per_step], xs[:per_step], sigs[:per_step], threads)
+    t0 = time.perf_counter()
+    agree = 0
+    for k in range(args.steps):
+        off = (k * per_step) % max(1, n - per_step + 1)
+        v = drv.verify(1, msgs[off:off + per_step], xs[off:off + per_step], sigs[off:off + per_step], threads)
+        agree += int((v == expect[off:off + per_step]).sum())
+    dt = time.perf_counter() - t0
+    rate = args.steps * per_step / dt
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "sigs/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded BIP-340 corpus (1% flipped bits, 0.1% off-curve keys)",
+            "config": {"workload": "bip340_verify_1M_one_launch", "signatures_per_step": per_step,
+                       "parallelism": f"{threads} host threads, one ufsecp_ctx each"},
+            "cpu_baseline": {"value": rate, "unit": "sigs/s", "cores": threads, "kind": "reference",
+                             "sample": f"{per_step} signatures per step from the seeded 1M-signature BIP-340 batch, "
+                                       "ufsecp_schnorr_verify per signature"},
+            "e2e": {"value": rate, "unit": "sigs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "verdict_agreement": agree / (args.steps * per_step)}
+    print(json.dumps(line))
+    return 0
+
+
+# -------------------------------------------------------------------- our arm --
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import ultrafastsecp256k1_b200 as uf
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=180), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    ctx = uf.GpuContext(local)
+    n = args.batch
+    (d_msgs, d_xs, d_sigs, d_out), (msgs, xs, sigs), expect = make_schnorr_batch(ctx, torch, n,
+                                                                                 seed=20261203 + rank)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def launch():
+        ctx.schnorr_verify_device(d_msgs.data_ptr(), d_xs.data_ptr(), d_sigs.data_ptr(), n, d_out.data_ptr(), sptr)
+
+    # ---- device-resident throughput (value) --------------------------------
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    agree = int((d_out.cpu().numpy() == expect).sum())
+    imad_peak = ctx.imad_peak()
+    barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t_start.record(stream)
+        for k in range(args.steps):
+            evs[k][0].record(stream)
+            launch()
+            evs[k][1].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    clocks = clk.summary()
+    total_ms = max_over_ranks(t_start.elapsed_time(t_end))
+    launch_ms = [a.elapsed_time(b) for a, b in evs]
+    avg_launch_ms = max_over_ranks(sum(launch_ms) / len(launch_ms))
+    total_sigs = sum_over_ranks(float(n * args.steps))
+    value = total_sigs / (total_ms * 1e-3)
+
+    # ---- end to end through the reference ABI call (host buffers) ----------
+    s_ctx = torch.cuda.ExternalStream(ctx.stream())
+    for _ in range(max(1, args.warmup)):
+        ctx.schnorr_verify_batch(msgs, xs, sigs)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e_steps = max(2, args.steps // 2)
+    e0.record(s_ctx)
+    for _ in range(e_steps):
+        res = ctx.schnorr_verify_batch(msgs, xs, sigs)
+    e1.record(s_ctx)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = sum_over_ranks(float(n * e_steps)) / (e2e_ms * 1e-3)
+    e2e_agree = int((res == expect).sum())
+
+    # ---- secondary: plain ECDSA on 4096 signatures (one launch) -----------
+    ecdsa_rate = None
+    if rank == 0:
+        ecdsa_rate = ecdsa_4096_rate(ctx, torch)
+
+    # ---- CPU baseline (rank 0, one GPU only) --------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sample = min(CPU_SAMPLE, n)
+            rate, threads, verdicts, dt = cpu_reference_rate(msgs, xs, sigs, sample)
+            cpu = {"value": rate, "unit": "sigs/s", "cores": threads, "kind": "reference",
+                   "sample": f"first {sample:,} signatures of the 1,048,576-signature BIP-340 batch "
+                             f"({dt:.1f} s wall), ufsecp_schnorr_verify per signature, one ufsecp_ctx per thread",
+                   "verdicts_equal_gpu": bool((verdicts == d_out.cpu().numpy()[:sample]).all())}
+        except Exception as e:  # reference library missing on this box
+            cpu = {"value": None, "unit": "sigs/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        peaks = measured_peaks()
+        traffic = profile_traffic().get("k_verify_schnorr_bytes_per_sig")
+        per_launch_s = avg_launch_ms * 1e-3
+        sigs_per_rank_s = n / per_launch_s
+        achieved = sigs_per_rank_s * W_SIG / 1e9
+        peak = imad_peak / 1e9
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        hbm_achieved = n * BYTES_PER_SIG / per_launch_s / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "sigs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic: seeded keys / messages / aux_rand, signed on the GPU (bytes identical to the "
+                    "reference signer), 1% one-bit flips in s or R.x, 0.1% off-curve x-only keys",
+            "config": {"workload": "bip340_verify_1M_one_launch", "signatures_per_launch": n,
+                       "kernel": "plain (one signature per thread)",
+                       "parallelism": f"{world} rank(s), one independent batch per GPU",
+                       "l2": "inputs 134 MB per launch > 126 MB L2 (no flush needed)"},
+            "e2e": {"value": e2e_value, "unit": "sigs/s", "h2d_bytes_per_step": n * 128, "d2h_bytes_per_step": n,
+                    "api": "ufsecp_gpu_schnorr_verify_batch (host buffers)",
+                    "verdict_agreement": e2e_agree / n},
+            "roofline": {"bound": "int", "achieved": achieved, "peak": peak, "unit": "Gop/s",
+                         "frac": achieved / peak if peak else None,
+                         "traffic": (traffic * n) if traffic else None,
+                         "ops_per_sig": W_SIG, "launch_ms": avg_launch_ms,
+                         "peak_source": "measured in this run: 32-bit IMAD issue rate (ufsecp_gpu_ext_imad_peak)",
+                         "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                                 "frac": hbm_achieved / hbm_peak, "peak_source": "of measured (MEASURED_PEAKS.json)"}},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+            "verdict_agreement": agree / n,
+            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate},
+        }
+        print(json.dumps(line))
+    del d_msgs, d_xs, d_sigs, d_out
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def ecdsa_4096_rate(ctx, torch):
+    """Plain ECDSA, 4096 signatures in one launch (the small-batch case)."""
+    n = 4096
+    rng = np.random.default_rng(4096)
+    sks = rng.integers(1, 255, (n, 32), dtype=np.uint8)
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    d_m, d_k = dev(msgs), dev(sks)
+    d_p = torch.empty(n * 33, dtype=torch.uint8, device="cuda")
+    d_s = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+    d_ok = torch.empty(n, dtype=torch.uint8, device="cuda")
+    d_out = torch.empty(n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream()
+    ctx.sign_device(0, d_m.data_ptr(), d_k.data_ptr(), 0, n, d_p.data_ptr(), d_s.data_ptr(), d_ok.data_ptr(),
+                    st.cuda_stream)
+    for _ in range(3):
+        ctx.ecdsa_verify_device(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), n, d_out.data_ptr(), st.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(10):
+        ctx.ecdsa_verify_device(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), n, d_out.data_ptr(), st.cuda_stream)
+    b.record(st)
+    torch.cuda.synchronize()
+    assert bool(d_out.all())
+    return n * 10 / (a.elapsed_time(b) * 1e-3)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

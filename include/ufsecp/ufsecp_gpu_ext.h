@@ -1,0 +1,80 @@
+/* ufsecp_gpu_ext.h -- B200 extensions of the verify ABI (additive).
+ *
+ * These entry points have no counterpart in the reference header; they expose
+ * what a B200 deployment needs beyond the synchronous host-buffer calls of
+ * ufsecp_gpu.h: verification over buffers already resident in device memory
+ * (asynchronous on a caller stream), the context's stream for event timing,
+ * and probes used by the test-suite and the benchmark.  All of them use the
+ * same context and error codes as ufsecp_gpu.h. */
+#ifndef UFSECP_GPU_EXT_H
+#define UFSECP_GPU_EXT_H
+
+#include "ufsecp_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Device-resident verify.  All pointers are device pointers (cudaMalloc or
+ * torch CUDA storage) of the same layout as the host calls; msgs, x-only keys
+ * and signatures must be 16-byte aligned.  The launch is enqueued on `stream`
+ * (a cudaStream_t; NULL = the context's stream) and the call returns without
+ * waiting; d_out[i] = 1 / 0 once the stream reaches that point. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_ecdsa_verify_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
+                                                             const uint8_t* d_pubkeys33, const uint8_t* d_sigs64,
+                                                             size_t count, uint8_t* d_out_results, void* stream);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
+                                                               const uint8_t* d_pubkeys_x32, const uint8_t* d_sigs64,
+                                                               size_t count, uint8_t* d_out_results, void* stream);
+
+/* Batch signing for synthetic workloads (device pointers, asynchronous on
+ * `stream`): kind 0 = ECDSA, RFC 6979 nonce, low-S compact r||s, 33-byte
+ * compressed pubkeys out; kind 1 = BIP-340 with aux_rand (d_aux32), 32-byte
+ * x-only pubkeys out.  d_ok[i] = 0 when sk[i] is 0 or >= n.  Output bytes are
+ * those of the reference's CPU signers ufsecp_ecdsa_sign / ufsecp_schnorr_sign. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_sign_device(ufsecp_gpu_ctx* ctx, uint32_t kind, const uint8_t* d_msgs32,
+                                                     const uint8_t* d_privkeys32, const uint8_t* d_aux32,
+                                                     size_t count, uint8_t* d_pubkeys_out, uint8_t* d_sigs64_out,
+                                                     uint8_t* d_ok, void* stream);
+
+/* The context's own stream (cudaStream_t), on which every host-buffer call of
+ * ufsecp_gpu.h enqueues its copies and kernels. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_stream(ufsecp_gpu_ctx* ctx, void** stream_out);
+
+/* SM count of the context's device, and blocks per SM the ECDSA (kind 0) /
+ * BIP-340 (kind 1) verify kernels reach. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* sm_count, int* ecdsa_blocks_per_sm,
+                                                      int* schnorr_blocks_per_sm);
+
+/* Measured 32-bit integer multiply-add issue rate of the device (ops / s):
+ * every thread of a full grid runs 16 independent mad.lo.u32 chains. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s);
+
+/* Device arithmetic probes (one item per thread), host buffers in and out.
+ * op  in -> out bytes per item
+ *  1  a|b (64) -> a*b mod p (32)         2  a (32) -> a^2 mod p (32)
+ *  3  a (32) -> a^-1 mod p (32)          4  a (32) -> ok (1) | sqrt (32)
+ *  5  a|b (64) -> a*b mod n (32)         6  a (32) -> a^-1 mod n (32)
+ *  7  k (32) -> |k1| (16) | |k2| (16) | neg1 | neg2    (GLV split)
+ *  8  k (32) -> (k*G).x | (k*G).y (64), zeros for infinity
+ *  9  a|x|b (96) -> finite (1) | x (32) | y (32) of a*G + b*P, P = lift_x(x)
+ * 10  r|p|m (96) -> BIP-340 challenge digest (32)
+ * All values big-endian. */
+#define UFSECP_EXT_DIAG_FE_MUL    1
+#define UFSECP_EXT_DIAG_FE_SQR    2
+#define UFSECP_EXT_DIAG_FE_INV    3
+#define UFSECP_EXT_DIAG_FE_SQRT   4
+#define UFSECP_EXT_DIAG_SC_MUL    5
+#define UFSECP_EXT_DIAG_SC_INV    6
+#define UFSECP_EXT_DIAG_GLV       7
+#define UFSECP_EXT_DIAG_GEN_MUL   8
+#define UFSECP_EXT_DIAG_DUAL_MUL  9
+#define UFSECP_EXT_DIAG_CHALLENGE 10
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_diag(ufsecp_gpu_ctx* ctx, uint32_t op, const uint8_t* in, size_t n,
+                                              uint8_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UFSECP_GPU_EXT_H */

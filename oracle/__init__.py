@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import tempfile
 import threading
 from concurrent.futures import ThreadPoolExecutor
 
@@ -29,6 +30,13 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libufsecp_ref.so")
+
+# The reference library writes its generator precompute cache (cache_w*.bin,
+# ~250 MB) to SECP256K1_CACHE_DIR, else to the working directory
+# (src/cpu/src/precompute.cpp:3267-3275); keep it out of the repository.
+_CACHE_DIR = os.path.join(tempfile.gettempdir(), "ufsecp_ref_cache")
+os.makedirs(_CACHE_DIR, exist_ok=True)
+os.environ.setdefault("SECP256K1_CACHE_DIR", _CACHE_DIR)
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 
@@ -233,6 +241,45 @@ class RefLib:
         """ufsecp_schnorr_batch_verify over 128-byte rows pk|msg|sig (RLC form)."""
         rows = _as_u8(rows128)
         return self.L.ufsecp_schnorr_batch_verify(self.ctx(), _ptr(rows), rows.size // 128)
+
+
+class RefDriver:
+    """Times the reference library's per-signature C ABI on all host threads
+    (oracle/refdrv.c: one ufsecp_ctx per thread, static partition)."""
+
+    def __init__(self, ref_path: str = REF_SO, drv_path: str = os.path.join(HERE, "librefdrv.so")):
+        if not os.path.exists(ref_path):
+            raise FileNotFoundError(f"{ref_path} missing")
+        if not os.path.exists(drv_path):
+            raise FileNotFoundError(f"{drv_path} missing: run `make -C oracle oracle`")
+        self.L = ctypes.CDLL(drv_path)
+        self.L.refdrv_open.argtypes = [ctypes.c_char_p]
+        self.L.refdrv_verify.argtypes = [ctypes.c_int, _u8p, _u8p, _u8p, ctypes.c_size_t, _u8p, ctypes.c_int]
+        self.L.refdrv_sign.argtypes = [ctypes.c_int, _u8p, _u8p, _u8p, ctypes.c_size_t, _u8p, _u8p, _u8p,
+                                       ctypes.c_int]
+        rc = self.L.refdrv_open(ref_path.encode())
+        if rc != 0:
+            raise RuntimeError(f"refdrv_open failed: {rc}")
+
+    def verify(self, kind: int, msgs, pubs, sigs, threads: int) -> np.ndarray:
+        msgs, pubs, sigs = _as_u8(msgs), _as_u8(pubs), _as_u8(sigs)
+        n = msgs.size // 32
+        out = np.zeros(n, np.uint8)
+        rc = self.L.refdrv_verify(kind, _ptr(msgs), _ptr(pubs), _ptr(sigs), n, _ptr(out), int(threads))
+        if rc != 0:
+            raise RuntimeError(f"refdrv_verify failed: {rc}")
+        return out
+
+
+    def sign(self, kind: int, msgs, sks, auxs, threads: int):
+        """Reference signers on all threads: returns (pubs, sigs, ok)."""
+        msgs, sks = _as_u8(msgs), _as_u8(sks)
+        auxs = _as_u8(auxs) if auxs is not None else np.zeros(1, np.uint8)
+        n = msgs.size // 32
+        ps = 33 if kind == 0 else 32
+        pubs, sigs, ok = np.zeros(n * ps, np.uint8), np.zeros(n * 64, np.uint8), np.zeros(n, np.uint8)
+        self.L.refdrv_sign(kind, _ptr(msgs), _ptr(sks), _ptr(auxs), n, _ptr(pubs), _ptr(sigs), _ptr(ok), int(threads))
+        return pubs.reshape(n, ps), sigs.reshape(n, 64), ok
 
 
 def ref_available() -> bool:

@@ -1,0 +1,128 @@
+"""Shared fixtures.  Tests marked `gpu` need a CUDA device (run with -m gpu);
+everything else runs on the CPU (-m "not gpu")."""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+NATIVE = os.path.join(ROOT, "tests", "native")
+P = 2**256 - 2**32 - 977
+N = 0xFFFFFFFFFFFFFFFFFFFFFFFFFFFFFFFEBAAEDCE6AF48A03BBFD25E8CD0364141
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
+    config.addinivalue_line("markers", "slow: longer CPU test")
+
+
+def _newer(target: str, *sources: str) -> bool:
+    return os.path.exists(target) and all(os.path.getmtime(target) >= os.path.getmtime(s) for s in sources)
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import Oracle, ORACLE_SO
+    src = os.path.join(ROOT, "oracle", "secp_oracle.c")
+    if not _newer(ORACLE_SO, src):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True, capture_output=True)
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def reflib():
+    from oracle import RefLib, ref_available
+    if not ref_available():
+        pytest.skip("reference library not built (oracle/_ref)")
+    return RefLib()
+
+
+@pytest.fixture(scope="session")
+def host_math():
+    """Host build of the device math headers (test harness, see tests/native)."""
+    import ctypes
+    import glob
+    so = os.path.join(NATIVE, "libdevmath_host.so")
+    src = os.path.join(NATIVE, "devmath_host.cpp")
+    hdrs = glob.glob(os.path.join(ROOT, "ultrafastsecp256k1_b200", "csrc", "*.cuh"))
+    if not _newer(so, src, *hdrs):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", so, src], check=True)
+    return ctypes.CDLL(so)
+
+
+@pytest.fixture(scope="session")
+def gpu_ctx():
+    import ultrafastsecp256k1_b200 as uf
+    ctx = uf.GpuContext(0)
+    yield ctx
+    ctx.close()
+
+
+def load_golden():
+    import json
+    vecs = json.load(open(os.path.join(GOLDEN, "bip340_vectors.json")))
+    wy = dict(np.load(os.path.join(GOLDEN, "wycheproof_ecdsa.npz")))
+    edge = dict(np.load(os.path.join(GOLDEN, "edge_corpus.npz")))
+    return vecs, wy, edge
+
+
+def rand_keys(rng, n):
+    """Private keys uniform in [1, n-1] (rejection sampling)."""
+    out = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    for i in range(n):
+        while True:
+            v = int.from_bytes(out[i].tobytes(), "big")
+            if 1 <= v < N:
+                break
+            out[i] = rng.integers(0, 256, 32, dtype=np.uint8)
+    return out
+
+
+def flip_random_bits(rng, arrs, frac):
+    """Flip one random bit in msg, r or s (chosen uniformly) of a `frac` share of items.
+    arrs = (msgs[n,32], sigs[n,64]); returns the tampered index set."""
+    msgs, sigs = arrs
+    n = msgs.shape[0]
+    idx = rng.choice(n, size=int(round(frac * n)), replace=False)
+    for i in idx:
+        where = rng.integers(0, 3)
+        bit = int(rng.integers(0, 256))
+        if where == 0:
+            msgs[i, bit // 8] ^= 1 << (bit % 8)
+        elif where == 1:
+            sigs[i, bit // 8] ^= 1 << (bit % 8)
+        else:
+            sigs[i, 32 + bit // 8] ^= 1 << (bit % 8)
+    return set(int(i) for i in idx)
+
+
+def ecdsa_corpus(oracle, n, seed, tamper=0.1):
+    rng = np.random.default_rng(seed)
+    sks = rand_keys(rng, n)
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    pubs, sigs, ok = oracle.ecdsa_sign_batch(msgs, sks)
+    assert ok.all()
+    pubs = pubs.reshape(n, 33)
+    sigs = sigs.reshape(n, 64)
+    flip_random_bits(rng, (msgs, sigs), tamper)
+    return msgs, pubs, sigs
+
+
+def schnorr_corpus(oracle, n, seed, tamper=0.01):
+    rng = np.random.default_rng(seed)
+    sks = rand_keys(rng, n)
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    aux = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    xs, sigs, ok = oracle.schnorr_sign_batch(msgs, sks, aux)
+    assert ok.all()
+    xs = xs.reshape(n, 32)
+    sigs = sigs.reshape(n, 64)
+    flip_random_bits(rng, (msgs, sigs), tamper)
+    return msgs, xs, sigs

@@ -1,0 +1,278 @@
+"""Parity of the sm_100a verify path with the oracle, through the C ABI.
+
+Bit-exact per-signature verdicts are required everywhere.  Small cases are
+compared item by item with the oracle; the full-size configurations (4096
+ECDSA, 1,048,576 BIP-340 in one launch) are compared against verdicts that are
+known by construction (oracle-verified seed corpora tiled across the launch,
+tampered copies)."""
+import numpy as np
+import pytest
+
+import ultrafastsecp256k1_b200 as uf
+from conftest import N, P, ecdsa_corpus, load_golden, rand_keys, schnorr_corpus
+
+pytestmark = pytest.mark.gpu
+
+LAM = 0x5363AD4CC05C30E0A5261C028812645A122E22EA20816678DF02967C1B23BD72
+
+
+def be(v):
+    return int(v).to_bytes(32, "big")
+
+
+def _cat(hexes):
+    return np.frombuffer(b"".join(bytes.fromhex(h) for h in hexes), np.uint8)
+
+
+# ------------------------------------------------------------ building blocks --
+def test_diag_field_and_scalar(gpu_ctx):
+    rng = np.random.default_rng(1)
+    special = [0, 1, 2, P - 1, P, P + 1, 2**256 - 1, 2**255, N - 1, N]
+    vals = special + [int.from_bytes(rng.bytes(32), "big") for _ in range(4000)]
+    a = vals
+    b = vals[7:] + vals[:7]
+    ab = np.frombuffer(b"".join(be(x) + be(y) for x, y in zip(a, b)), np.uint8)
+    out = gpu_ctx.diag(1, ab)
+    assert [int.from_bytes(r.tobytes(), "big") for r in out] == [x * y % P for x, y in zip(a, b)]
+    out = gpu_ctx.diag(2, np.frombuffer(b"".join(be(x) for x in a), np.uint8))
+    assert [int.from_bytes(r.tobytes(), "big") for r in out] == [x * x % P for x in a]
+    nz = [x for x in a if x % P]
+    out = gpu_ctx.diag(3, np.frombuffer(b"".join(be(x) for x in nz), np.uint8))
+    assert [int.from_bytes(r.tobytes(), "big") for r in out] == [pow(x, -1, P) for x in nz]
+    an = [x % N for x in a]
+    bn = [x % N for x in b]
+    out = gpu_ctx.diag(5, np.frombuffer(b"".join(be(x) + be(y) for x, y in zip(an, bn)), np.uint8))
+    assert [int.from_bytes(r.tobytes(), "big") for r in out] == [x * y % N for x, y in zip(an, bn)]
+    nzn = [x for x in an if x]
+    out = gpu_ctx.diag(6, np.frombuffer(b"".join(be(x) for x in nzn), np.uint8))
+    assert [int.from_bytes(r.tobytes(), "big") for r in out] == [pow(x, -1, N) for x in nzn]
+
+
+def test_diag_sqrt_glv_challenge(gpu_ctx):
+    import hashlib
+    rng = np.random.default_rng(2)
+    xs = [int.from_bytes(rng.bytes(32), "big") % P for _ in range(2000)]
+    out = gpu_ctx.diag(4, np.frombuffer(b"".join(be(x) for x in xs), np.uint8))
+    for x, r in zip(xs, out):
+        qr = pow(x, (P - 1) // 2, P) in (0, 1)
+        assert bool(r[0]) == qr
+        if qr:
+            y = int.from_bytes(r[1:].tobytes(), "big")
+            assert y * y % P == x
+    ks = [0, 1, N - 1, LAM] + [int.from_bytes(rng.bytes(32), "big") % N for _ in range(4000)]
+    out = gpu_ctx.diag(7, np.frombuffer(b"".join(be(k) for k in ks), np.uint8))
+    for k, r in zip(ks, out):
+        k1 = int.from_bytes(r[:16].tobytes(), "big") * (-1 if r[32] else 1)
+        k2 = int.from_bytes(r[16:32].tobytes(), "big") * (-1 if r[33] else 1)
+        assert (k1 + k2 * LAM - k) % N == 0
+    tag = hashlib.sha256(b"BIP0340/challenge").digest()
+    data = [rng.bytes(96) for _ in range(1000)]
+    out = gpu_ctx.diag(10, np.frombuffer(b"".join(data), np.uint8))
+    for d, r in zip(data, out):
+        assert r.tobytes() == hashlib.sha256(tag + tag + d).digest()
+
+
+def test_diag_gen_mul_vs_oracle(gpu_ctx, oracle):
+    rng = np.random.default_rng(3)
+    ks = [1, 2, 3, N - 1, N - 2, 2**128, LAM] + [int.from_bytes(rng.bytes(32), "big") % N for _ in range(500)]
+    out = gpu_ctx.diag(8, np.frombuffer(b"".join(be(k) for k in ks), np.uint8))
+    for k, r in zip(ks, out):
+        x, y = oracle.gen_mul(be(k))
+        assert r[:32].tobytes() == x and r[32:].tobytes() == y
+    out = gpu_ctx.diag(8, np.frombuffer(be(0) + be(N), np.uint8))
+    assert not out.any()
+
+
+def test_diag_dual_mul_exceptional(gpu_ctx, oracle):
+    """a*G + b*P including results at infinity and doublings inside the adds."""
+    rng = np.random.default_rng(4)
+    rows, want = [], []
+    for i in range(64):
+        d = int.from_bytes(rng.bytes(32), "big") % (N - 1) + 1
+        X, Y = (int.from_bytes(v, "big") for v in oracle.gen_mul(be(d)))
+        if Y & 1:
+            d = N - d
+        a, b = (int.from_bytes(rng.bytes(32), "big") % N for _ in range(2))
+        if i == 0:
+            a, b = (N - d) % N, 1          # a*G + P = infinity
+        elif i == 1:
+            a, b = d, 1                    # = 2P
+        elif i == 2:
+            a, b = 0, 3
+        elif i == 3:
+            a, b = 5, 0
+        rows.append(be(a) + be(X) + be(b))
+        want.append((a + b * d) % N)
+    out = gpu_ctx.diag(9, np.frombuffer(b"".join(rows), np.uint8))
+    for r, k in zip(out, want):
+        if k == 0:
+            assert r[0] == 0
+        else:
+            x, y = oracle.gen_mul(be(k))
+            assert r[0] == 1 and r[1:33].tobytes() == x and r[33:].tobytes() == y
+
+
+# ---------------------------------------------------------------- golden data --
+def test_bip340_vectors(gpu_ctx):
+    vecs, _, _ = load_golden()
+    got = gpu_ctx.schnorr_verify_batch(_cat(v["msg"] for v in vecs), _cat(v["pk"] for v in vecs),
+                                       _cat(v["sig"] for v in vecs))
+    assert list(got) == [int(v["ref_valid"]) for v in vecs]
+
+
+def test_wycheproof_ecdsa(gpu_ctx):
+    _, wy, _ = load_golden()
+    got = gpu_ctx.ecdsa_verify_batch(wy["msgs"], wy["pubs"], wy["sigs"])
+    assert (got == wy["ref_valid"]).all()
+
+
+def test_edge_corpus(gpu_ctx):
+    _, _, e = load_golden()
+    assert (gpu_ctx.ecdsa_verify_batch(e["ecdsa_msgs"], e["ecdsa_pubs"], e["ecdsa_sigs"]) == e["ecdsa_ref_valid"]).all()
+    assert (gpu_ctx.schnorr_verify_batch(e["schnorr_msgs"], e["schnorr_pubs"], e["schnorr_sigs"])
+            == e["schnorr_ref_valid"]).all()
+
+
+# ---------------------------------------------------------- seeded workloads --
+def test_ecdsa_4096_tampered(gpu_ctx, oracle):
+    """Plain ECDSA verify, 4096 signatures, 10% with one flipped bit in msg, r or s."""
+    m, p, s = ecdsa_corpus(oracle, 4096, seed=20261203, tamper=0.10)
+    want = oracle.ecdsa_verify_batch(m, p, s)
+    got = gpu_ctx.ecdsa_verify_batch(m, p, s)
+    assert (got == want).all()
+    assert 0.85 * 4096 < want.sum() < 0.95 * 4096
+
+
+def _offcurve_x(rng):
+    while True:
+        x = int.from_bytes(rng.bytes(32), "big") % P
+        if pow((x**3 + 7) % P, (P - 1) // 2, P) != 1:
+            return x
+
+
+def test_schnorr_1m_one_launch(gpu_ctx, oracle):
+    """BIP-340, 1,048,576 signatures in one launch: 1% flipped bits in s or R.x,
+    0.1% x-only keys off the curve.  16,384 oracle-verified items tiled 64x."""
+    base = 16384
+    rng = np.random.default_rng(7)
+    m, x, s = schnorr_corpus(oracle, base, seed=8, tamper=0.0)
+    for i in rng.choice(base, size=base // 100, replace=False):
+        bit = int(rng.integers(0, 256))
+        s[i, (0 if rng.integers(0, 2) else 32) + bit // 8] ^= 1 << (bit % 8)
+    for i in rng.choice(base, size=max(1, base // 1000), replace=False):
+        x[i] = np.frombuffer(be(_offcurve_x(rng)), np.uint8)
+    want = oracle.schnorr_verify_batch(m, x, s)
+    reps = (1 << 20) // base
+    got = gpu_ctx.schnorr_verify_batch(np.tile(m, (reps, 1)), np.tile(x, (reps, 1)), np.tile(s, (reps, 1)))
+    assert got.shape == (1 << 20,)
+    assert (got == np.tile(want, reps)).all()
+
+
+def test_chunked_host_call(gpu_ctx, oracle):
+    """A call larger than one device chunk (2^22 items) keeps per-item order."""
+    base = 4096
+    m, x, s = schnorr_corpus(oracle, base, seed=9, tamper=0.05)
+    want = oracle.schnorr_verify_batch(m, x, s)
+    n = (1 << 22) + 4099
+    reps = -(-n // base)
+    got = gpu_ctx.schnorr_verify_batch(np.tile(m, (reps, 1))[:n], np.tile(x, (reps, 1))[:n],
+                                       np.tile(s, (reps, 1))[:n])
+    assert (got == np.tile(want, reps)[:n]).all()
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 127, 129, 1000])
+def test_ragged_sizes(gpu_ctx, oracle, n):
+    m, p, s = ecdsa_corpus(oracle, n, seed=100 + n, tamper=0.3)
+    assert (gpu_ctx.ecdsa_verify_batch(m, p, s) == oracle.ecdsa_verify_batch(m, p, s)).all()
+    m, x, s = schnorr_corpus(oracle, n, seed=200 + n, tamper=0.3)
+    assert (gpu_ctx.schnorr_verify_batch(m, x, s) == oracle.schnorr_verify_batch(m, x, s)).all()
+
+
+def test_collect_semantics(gpu_ctx, oracle):
+    m, p, s = ecdsa_corpus(oracle, 777, seed=31, tamper=0.2)
+    want = oracle.ecdsa_verify_batch(m, p, s)
+    kb = np.full(777, 0xA5, np.uint8)
+    gpu_ctx.ecdsa_verify_collect(m, p, s, kb)
+    assert ((kb == 0) == (want == 1)).all() and (kb[want == 0] == 0xA5).all()
+    m, x, s = schnorr_corpus(oracle, 555, seed=32, tamper=0.2)
+    want = oracle.schnorr_verify_batch(m, x, s)
+    kb = np.arange(1, 556, dtype=np.uint32).astype(np.uint8) | 1
+    before = kb.copy()
+    gpu_ctx.schnorr_verify_collect(m, x, s, kb)
+    assert ((kb == 0) == (want == 1)).all() and (kb[want == 0] == before[want == 0]).all()
+
+
+def test_gpu_signers_match_oracle(gpu_ctx, oracle):
+    import torch
+    n = 512
+    rng = np.random.default_rng(41)
+    sks = rand_keys(rng, n)
+    sks[0] = 0                               # invalid key -> ok = 0
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    aux = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    dm, dk, da = dev(msgs), dev(sks), dev(aux)
+    for kind, ps in ((0, 33), (1, 32)):
+        dp = torch.zeros(n * ps, dtype=torch.uint8, device="cuda")
+        ds = torch.zeros(n * 64, dtype=torch.uint8, device="cuda")
+        dok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        gpu_ctx.sign_device(kind, dm.data_ptr(), dk.data_ptr(), da.data_ptr(), n, dp.data_ptr(), ds.data_ptr(),
+                            dok.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        if kind == 0:
+            p2, s2, ok2 = oracle.ecdsa_sign_batch(msgs[1:], sks[1:])
+        else:
+            p2, s2, ok2 = oracle.schnorr_sign_batch(msgs[1:], sks[1:], aux[1:])
+        ok = dok.cpu().numpy()
+        assert ok[0] == 0 and ok[1:].all()
+        assert (dp.cpu().numpy()[ps:] == p2).all() and (ds.cpu().numpy()[64:] == s2).all()
+
+
+def test_device_api_matches_host_api(gpu_ctx, oracle):
+    import torch
+    m, p, s = ecdsa_corpus(oracle, 3000, seed=51, tamper=0.1)
+    want = gpu_ctx.ecdsa_verify_batch(m, p, s)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    dm, dp, ds = dev(m), dev(p), dev(s)
+    dout = torch.full((3000,), 7, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    gpu_ctx.ecdsa_verify_device(dm.data_ptr(), dp.data_ptr(), ds.data_ptr(), 3000, dout.data_ptr(), stream)
+    torch.cuda.synchronize()
+    assert (dout.cpu().numpy() == want).all()
+    m, x, s = schnorr_corpus(oracle, 3000, seed=52, tamper=0.1)
+    want = gpu_ctx.schnorr_verify_batch(m, x, s)
+    dm, dx, ds = dev(m), dev(x), dev(s)
+    gpu_ctx.schnorr_verify_device(dm.data_ptr(), dx.data_ptr(), ds.data_ptr(), 3000, dout.data_ptr(), 0)
+    gpu_ctx_stream_sync(gpu_ctx)
+    assert (dout.cpu().numpy() == want).all()
+
+
+def gpu_ctx_stream_sync(ctx):
+    import torch
+    s = torch.cuda.ExternalStream(ctx.stream())
+    s.synchronize()
+
+
+def test_abi_gating_with_context(gpu_ctx):
+    L = uf.load_library()
+    h = gpu_ctx.handle
+    out = np.full(4, 9, np.uint8)
+    # count == 0: OK, buffers untouched
+    assert L.ufsecp_gpu_ecdsa_verify_batch(h, None, None, None, 0, out.ctypes.data) == 0 and (out == 9).all()
+    # over the 2^26 cap
+    assert L.ufsecp_gpu_schnorr_verify_batch(h, 1, 1, 1, (1 << 26) + 1, out.ctypes.data) == uf.UFSECP_ERR_BAD_INPUT
+    # output cleared before the NULL-input check
+    assert L.ufsecp_gpu_ecdsa_verify_batch(h, None, None, None, 4, out.ctypes.data) == uf.UFSECP_ERR_NULL_ARG
+    assert (out == 0).all()
+    # collect: NULL check before the cap check, key buffer not cleared
+    kb = np.full(4, 3, np.uint8)
+    assert L.ufsecp_gpu_ecdsa_verify_collect(h, None, None, None, 4, kb.ctypes.data) == uf.UFSECP_ERR_NULL_ARG
+    assert (kb == 3).all()
+    # operations outside the verify path report UNSUPPORTED and clear their outputs
+    res = np.full(2, 5, np.uint8)
+    assert L.ufsecp_gpu_ecdsa_verify_lbtc_columns(h, out.ctypes.data, out.ctypes.data, out.ctypes.data, 2,
+                                                  res.ctypes.data) == uf.UFSECP_ERR_GPU_UNSUPPORTED
+    assert (res == 0).all()
+    assert gpu_ctx.is_ready()
+    info = uf.device_info(0)
+    assert info.compute_units > 0 and info.global_mem_bytes > 0

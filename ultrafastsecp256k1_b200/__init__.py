@@ -1,0 +1,264 @@
+"""ultrafastsecp256k1_b200 -- B200-native batch ECDSA / BIP-340 verification.
+
+The product is the C-ABI shared library ``lib/libufsecp_gpu.so`` (sm_100a
+kernels + C++ host runtime) exporting the reference's GPU verify ABI
+(``include/ufsecp/ufsecp_gpu.h``) plus B200 additions
+(``include/ufsecp/ufsecp_gpu_ext.h``).  This module is a thin ctypes mirror of
+that ABI for Python callers, the tests and the benchmark: same function names,
+same argument meaning, same error codes (a non-OK code raises
+``UfsecpError``).  There is no CPU path: if the library or a CUDA device is
+missing, the calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libufsecp_gpu.so")
+
+UFSECP_OK = 0
+UFSECP_ERR_NULL_ARG = 1
+UFSECP_ERR_BAD_INPUT = 5
+UFSECP_ERR_INTERNAL = 9
+UFSECP_ERR_GPU_UNAVAILABLE = 100
+UFSECP_ERR_GPU_DEVICE = 101
+UFSECP_ERR_GPU_LAUNCH = 102
+UFSECP_ERR_GPU_MEMORY = 103
+UFSECP_ERR_GPU_UNSUPPORTED = 104
+UFSECP_ERR_GPU_BACKEND = 105
+UFSECP_ERR_GPU_QUEUE = 106
+UFSECP_GPU_BACKEND_CUDA = 1
+MAX_BATCH = 1 << 26
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_vp = ctypes.c_void_p
+_lib: Optional[ctypes.CDLL] = None
+
+
+class UfsecpError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str = ""):
+        self.code = code
+        super().__init__(f"{where}: ufsecp error {code}{' (' + msg + ')' if msg else ''}")
+
+
+class DeviceInfo(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 128), ("global_mem_bytes", ctypes.c_uint64),
+                ("compute_units", ctypes.c_uint32), ("max_clock_mhz", ctypes.c_uint32),
+                ("max_threads_per_block", ctypes.c_uint32), ("backend_id", ctypes.c_uint32),
+                ("device_index", ctypes.c_uint32)]
+
+
+# name -> (restype, argtypes) of every symbol the mirror binds
+_SIGS = {
+    "ufsecp_gpu_backend_count": (ctypes.c_uint32, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32]),
+    "ufsecp_gpu_backend_name": (ctypes.c_char_p, [ctypes.c_uint32]),
+    "ufsecp_gpu_is_available": (ctypes.c_int, [ctypes.c_uint32]),
+    "ufsecp_gpu_device_count": (ctypes.c_uint32, [ctypes.c_uint32]),
+    "ufsecp_gpu_device_info": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(DeviceInfo)]),
+    "ufsecp_gpu_ctx_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_uint32, ctypes.c_uint32]),
+    "ufsecp_gpu_ctx_destroy": (None, [_vp]),
+    "ufsecp_gpu_is_ready": (ctypes.c_int, [_vp]),
+    "ufsecp_gpu_last_error": (ctypes.c_int, [_vp]),
+    "ufsecp_gpu_last_error_msg": (ctypes.c_char_p, [_vp]),
+    "ufsecp_gpu_error_str": (ctypes.c_char_p, [ctypes.c_int]),
+    "ufsecp_gpu_ecdsa_verify_batch": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "ufsecp_gpu_schnorr_verify_batch": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "ufsecp_gpu_ecdsa_verify_collect": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "ufsecp_gpu_schnorr_verify_collect": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "ufsecp_gpu_ext_ecdsa_verify_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp]),
+    "ufsecp_gpu_ext_schnorr_verify_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp]),
+    "ufsecp_gpu_ext_sign_device": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp,
+                                                  _vp]),
+    "ufsecp_gpu_ext_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "ufsecp_gpu_ext_device_props": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                                   ctypes.POINTER(ctypes.c_int)]),
+    "ufsecp_gpu_ext_imad_peak": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "ufsecp_gpu_ext_diag": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_size_t, _vp]),
+}
+
+
+def lib_path() -> str:
+    return LIB_PATH
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libufsecp_gpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run `python -m ultrafastsecp256k1_b200.build`")
+    L = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _buf(x, n_bytes: int, name: str) -> np.ndarray:
+    if isinstance(x, (bytes, bytearray, memoryview)):
+        a = np.frombuffer(bytes(x), dtype=np.uint8)
+    else:
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.uint8)).reshape(-1)
+    if a.size != n_bytes:
+        raise ValueError(f"{name}: expected {n_bytes} bytes, got {a.size}")
+    return a
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def backend_count() -> int:
+    return load_library().ufsecp_gpu_backend_count(None, 0)
+
+
+def is_available(backend_id: int = UFSECP_GPU_BACKEND_CUDA) -> bool:
+    return bool(load_library().ufsecp_gpu_is_available(backend_id))
+
+
+def device_count(backend_id: int = UFSECP_GPU_BACKEND_CUDA) -> int:
+    return int(load_library().ufsecp_gpu_device_count(backend_id))
+
+
+def device_info(device_index: int = 0, backend_id: int = UFSECP_GPU_BACKEND_CUDA) -> DeviceInfo:
+    info = DeviceInfo()
+    rc = load_library().ufsecp_gpu_device_info(backend_id, device_index, ctypes.byref(info))
+    if rc != UFSECP_OK:
+        raise UfsecpError(rc, "ufsecp_gpu_device_info")
+    return info
+
+
+def error_str(code: int) -> str:
+    return load_library().ufsecp_gpu_error_str(code).decode()
+
+
+class GpuContext:
+    """One ``ufsecp_gpu_ctx`` (single-thread, like the reference's)."""
+
+    def __init__(self, device_index: int = 0, backend_id: int = UFSECP_GPU_BACKEND_CUDA):
+        self.L = load_library()
+        self._ctx = _vp()
+        rc = self.L.ufsecp_gpu_ctx_create(ctypes.byref(self._ctx), backend_id, device_index)
+        if rc != UFSECP_OK:
+            raise UfsecpError(rc, "ufsecp_gpu_ctx_create", error_str(rc))
+
+    @property
+    def handle(self) -> int:
+        return self._ctx.value
+
+    def close(self) -> None:
+        if self._ctx:
+            self.L.ufsecp_gpu_ctx_destroy(self._ctx)
+            self._ctx = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def is_ready(self) -> bool:
+        return bool(self.L.ufsecp_gpu_is_ready(self._ctx))
+
+    def last_error(self) -> int:
+        return int(self.L.ufsecp_gpu_last_error(self._ctx))
+
+    def last_error_msg(self) -> str:
+        return self.L.ufsecp_gpu_last_error_msg(self._ctx).decode()
+
+    def _check(self, rc: int, where: str) -> None:
+        if rc != UFSECP_OK:
+            raise UfsecpError(rc, where, self.last_error_msg())
+
+    # ---- ufsecp_gpu.h verify calls (host buffers) ----------------------------
+    def _verify(self, fn, name, msgs, pubs, pub_sz, sigs, count=None, out=None) -> np.ndarray:
+        n = (len(msgs) if isinstance(msgs, (bytes, bytearray)) else np.asarray(msgs).size) // 32 \
+            if count is None else count
+        m = _buf(msgs, 32 * n, "msg_hashes32")
+        p = _buf(pubs, pub_sz * n, "pubkeys")
+        s = _buf(sigs, 64 * n, "sigs64")
+        if out is None:
+            out = np.zeros(n, dtype=np.uint8)
+        rc = fn(self._ctx, _ptr(m), _ptr(p), _ptr(s), n, _ptr(out))
+        self._check(rc, name)
+        return out
+
+    def ecdsa_verify_batch(self, msg_hashes32, pubkeys33, sigs64) -> np.ndarray:
+        """ufsecp_gpu_ecdsa_verify_batch: per-item verdicts (1 valid / 0 invalid)."""
+        return self._verify(self.L.ufsecp_gpu_ecdsa_verify_batch, "ufsecp_gpu_ecdsa_verify_batch",
+                            msg_hashes32, pubkeys33, 33, sigs64)
+
+    def schnorr_verify_batch(self, msg_hashes32, pubkeys_x32, sigs64) -> np.ndarray:
+        """ufsecp_gpu_schnorr_verify_batch: per-item BIP-340 verdicts."""
+        return self._verify(self.L.ufsecp_gpu_schnorr_verify_batch, "ufsecp_gpu_schnorr_verify_batch",
+                            msg_hashes32, pubkeys_x32, 32, sigs64)
+
+    def ecdsa_verify_collect(self, msg_hashes32, pubkeys33, sigs64, key_buffer: np.ndarray) -> np.ndarray:
+        """ufsecp_gpu_ecdsa_verify_collect: valid rows of key_buffer become 0 in place."""
+        kb = np.ascontiguousarray(key_buffer, dtype=np.uint8)
+        return self._verify(self.L.ufsecp_gpu_ecdsa_verify_collect, "ufsecp_gpu_ecdsa_verify_collect",
+                            msg_hashes32, pubkeys33, 33, sigs64, count=kb.size, out=kb)
+
+    def schnorr_verify_collect(self, msg_hashes32, pubkeys_x32, sigs64, key_buffer: np.ndarray) -> np.ndarray:
+        kb = np.ascontiguousarray(key_buffer, dtype=np.uint8)
+        return self._verify(self.L.ufsecp_gpu_schnorr_verify_collect, "ufsecp_gpu_schnorr_verify_collect",
+                            msg_hashes32, pubkeys_x32, 32, sigs64, count=kb.size, out=kb)
+
+    # ---- ufsecp_gpu_ext.h -------------------------------------------------------
+    def ecdsa_verify_device(self, d_msgs: int, d_pubs33: int, d_sigs: int, count: int, d_out: int,
+                            stream: int = 0) -> None:
+        """Device pointers in / out, enqueued on `stream` (0 = context stream)."""
+        self._check(self.L.ufsecp_gpu_ext_ecdsa_verify_device(self._ctx, d_msgs, d_pubs33, d_sigs, count, d_out,
+                                                              stream or None), "ecdsa_verify_device")
+
+    def schnorr_verify_device(self, d_msgs: int, d_xonly: int, d_sigs: int, count: int, d_out: int,
+                              stream: int = 0) -> None:
+        self._check(self.L.ufsecp_gpu_ext_schnorr_verify_device(self._ctx, d_msgs, d_xonly, d_sigs, count, d_out,
+                                                                stream or None), "schnorr_verify_device")
+
+    def sign_device(self, kind: int, d_msgs: int, d_sks: int, d_auxs: int, count: int, d_pubs: int, d_sigs: int,
+                    d_ok: int, stream: int = 0) -> None:
+        """Batch signer for synthetic corpora (device pointers; kind 0 ECDSA, 1 BIP-340)."""
+        self._check(self.L.ufsecp_gpu_ext_sign_device(self._ctx, kind, d_msgs, d_sks, d_auxs or None, count, d_pubs,
+                                                      d_sigs, d_ok, stream or None), "sign_device")
+
+    def stream(self) -> int:
+        s = _vp()
+        self._check(self.L.ufsecp_gpu_ext_stream(self._ctx, ctypes.byref(s)), "ext_stream")
+        return s.value or 0
+
+    def device_props(self):
+        sms, be, bs = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.ufsecp_gpu_ext_device_props(self._ctx, ctypes.byref(sms), ctypes.byref(be),
+                                                       ctypes.byref(bs)), "device_props")
+        return {"sm_count": sms.value, "ecdsa_blocks_per_sm": be.value, "schnorr_blocks_per_sm": bs.value}
+
+    def imad_peak(self) -> float:
+        v = ctypes.c_double()
+        self._check(self.L.ufsecp_gpu_ext_imad_peak(self._ctx, ctypes.byref(v)), "imad_peak")
+        return v.value
+
+    _DIAG_IO = {1: (64, 32), 2: (32, 32), 3: (32, 32), 4: (32, 33), 5: (64, 32), 6: (32, 32), 7: (32, 34),
+                8: (32, 64), 9: (96, 65), 10: (96, 32)}
+
+    def diag(self, op: int, data) -> np.ndarray:
+        isz, osz = self._DIAG_IO[op]
+        a = np.ascontiguousarray(np.frombuffer(bytes(data), np.uint8) if isinstance(data, (bytes, bytearray))
+                                 else np.asarray(data, np.uint8)).reshape(-1)
+        n = a.size // isz
+        out = np.zeros(n * osz, np.uint8)
+        self._check(self.L.ufsecp_gpu_ext_diag(self._ctx, op, _ptr(a), n, _ptr(out)), "ext_diag")
+        return out.reshape(n, osz)

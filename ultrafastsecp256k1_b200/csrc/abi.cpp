@@ -1,0 +1,427 @@
+// extern "C" surface: ufsecp_gpu.h (the reference's GPU ABI) and
+// ufsecp_gpu_ext.h (B200 additions).
+//
+// Argument gating, output clearing and exception mapping follow the
+// reference's C ABI layer src/cpu/src/ufsecp_gpu_impl.cpp: batch cap 2^26
+// (:76), bad_alloc -> GPU_MEMORY / other exceptions -> INTERNAL (:79-81),
+// clear-before and clear-after-failure of result buffers (:117-140, :317-336).
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <limits>
+#include <memory>
+#include <new>
+
+#include "backend.h"
+#include "ufsecp/ufsecp_gpu.h"
+#include "ufsecp/ufsecp_gpu_ext.h"
+
+struct ufsecp_gpu_ctx {
+    std::unique_ptr<uf::Backend> backend;
+    uint32_t backend_id;
+    uint32_t device_index;
+};
+
+namespace {
+
+constexpr size_t kMaxBatch = size_t{1} << 26;
+
+bool clear_out(uint8_t* out, size_t count, size_t stride) {
+    if (!out || count == 0) return true;
+    if (count > std::numeric_limits<size_t>::max() / stride) return false;
+    memset(out, 0, count * stride);
+    return true;
+}
+
+ufsecp_error_t finish(ufsecp_error_t rc, uint8_t* out, size_t count, size_t stride) {
+    if (rc != UFSECP_OK) clear_out(out, count, stride);
+    return rc;
+}
+
+int cuda_device_count() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// Shared gating of the result-bearing verify calls.
+template <class F>
+ufsecp_error_t gated_verify(ufsecp_gpu_ctx* ctx, const uint8_t* a, const uint8_t* b, const uint8_t* c, size_t count,
+                            uint8_t* out, F&& run) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (count > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!clear_out(out, count, 1)) return UFSECP_ERR_BAD_INPUT;
+    if (!a || !b || !c || !out) return UFSECP_ERR_NULL_ARG;
+    try {
+        return finish(run(), out, count, 1);
+    } catch (const std::bad_alloc&) {
+        return finish(UFSECP_ERR_GPU_MEMORY, out, count, 1);
+    } catch (...) {
+        return finish(UFSECP_ERR_INTERNAL, out, count, 1);
+    }
+}
+
+template <class F>
+ufsecp_error_t gated_collect(ufsecp_gpu_ctx* ctx, const uint8_t* a, const uint8_t* b, const uint8_t* c, size_t count,
+                             uint8_t* key_buffer, F&& run) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (!a || !b || !c || !key_buffer) return UFSECP_ERR_NULL_ARG;
+    if (count > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    try {
+        return run();
+    } catch (const std::bad_alloc&) {
+        return UFSECP_ERR_GPU_MEMORY;
+    } catch (...) {
+        return UFSECP_ERR_INTERNAL;
+    }
+}
+
+ufsecp_error_t unsupported(ufsecp_gpu_ctx* ctx, size_t count) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    ctx->backend->set_error(UFSECP_ERR_GPU_UNSUPPORTED, "operation not implemented by the B200 verify backend");
+    return UFSECP_ERR_GPU_UNSUPPORTED;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- discovery -------------------------------------------------------------
+
+uint32_t ufsecp_gpu_backend_count(uint32_t* backend_ids, uint32_t max_ids) noexcept {
+    if (backend_ids && max_ids > 0) backend_ids[0] = UFSECP_GPU_BACKEND_CUDA;
+    return 1;
+}
+
+const char* ufsecp_gpu_backend_name(uint32_t backend_id) {
+    switch (backend_id) {
+        case UFSECP_GPU_BACKEND_CUDA: return "CUDA";
+        case UFSECP_GPU_BACKEND_OPENCL: return "OpenCL";
+        case UFSECP_GPU_BACKEND_METAL: return "Metal";
+        default: return "none";
+    }
+}
+
+int ufsecp_gpu_is_available(uint32_t backend_id) noexcept {
+    return backend_id == UFSECP_GPU_BACKEND_CUDA && cuda_device_count() > 0 ? 1 : 0;
+}
+
+uint32_t ufsecp_gpu_device_count(uint32_t backend_id) noexcept {
+    return backend_id == UFSECP_GPU_BACKEND_CUDA ? (uint32_t)cuda_device_count() : 0u;
+}
+
+ufsecp_error_t ufsecp_gpu_device_info(uint32_t backend_id, uint32_t device_index, ufsecp_gpu_device_info_t* info_out) {
+    if (!info_out) return UFSECP_ERR_NULL_ARG;
+    if (backend_id != UFSECP_GPU_BACKEND_CUDA) return UFSECP_ERR_GPU_UNAVAILABLE;
+    const int n = cuda_device_count();
+    if (n == 0) return UFSECP_ERR_GPU_UNAVAILABLE;
+    if ((int)device_index >= n) return UFSECP_ERR_GPU_DEVICE;
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, (int)device_index) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return UFSECP_ERR_GPU_DEVICE;
+    }
+    memset(info_out, 0, sizeof(*info_out));
+    strncpy(info_out->name, p.name, sizeof(info_out->name) - 1);
+    info_out->global_mem_bytes = p.totalGlobalMem;
+    info_out->compute_units = (uint32_t)p.multiProcessorCount;
+    int clk_khz = 0;
+    cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, (int)device_index);
+    info_out->max_clock_mhz = (uint32_t)(clk_khz / 1000);
+    info_out->max_threads_per_block = (uint32_t)p.maxThreadsPerBlock;
+    info_out->backend_id = UFSECP_GPU_BACKEND_CUDA;
+    info_out->device_index = device_index;
+    return UFSECP_OK;
+}
+
+// ---- lifecycle -------------------------------------------------------------
+
+ufsecp_error_t ufsecp_gpu_ctx_create(ufsecp_gpu_ctx** ctx_out, uint32_t backend_id, uint32_t device_index) {
+    if (!ctx_out) return UFSECP_ERR_NULL_ARG;
+    *ctx_out = nullptr;
+    if (backend_id != UFSECP_GPU_BACKEND_CUDA) return UFSECP_ERR_GPU_UNAVAILABLE;
+    try {
+        auto be = std::make_unique<uf::Backend>();
+        const int rc = be->init((int)device_index);
+        if (rc != UFSECP_OK) return rc;
+        auto* ctx = new (std::nothrow) ufsecp_gpu_ctx;
+        if (!ctx) return UFSECP_ERR_INTERNAL;
+        ctx->backend = std::move(be);
+        ctx->backend_id = backend_id;
+        ctx->device_index = device_index;
+        *ctx_out = ctx;
+        return UFSECP_OK;
+    } catch (const std::bad_alloc&) {
+        return UFSECP_ERR_GPU_MEMORY;
+    } catch (...) {
+        return UFSECP_ERR_INTERNAL;
+    }
+}
+
+void ufsecp_gpu_ctx_destroy(ufsecp_gpu_ctx* ctx) {
+    if (ctx) {
+        ctx->backend.reset();
+        delete ctx;
+    }
+}
+
+int ufsecp_gpu_is_ready(const ufsecp_gpu_ctx* ctx) noexcept {
+    return ctx && ctx->backend && ctx->backend->ready() ? 1 : 0;
+}
+
+ufsecp_error_t ufsecp_gpu_last_error(const ufsecp_gpu_ctx* ctx) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->last_error();
+}
+
+const char* ufsecp_gpu_last_error_msg(const ufsecp_gpu_ctx* ctx) {
+    if (!ctx) return "NULL GPU context";
+    return ctx->backend->last_error_msg();
+}
+
+const char* ufsecp_gpu_error_str(ufsecp_error_t err) {
+    switch (err) {
+        case UFSECP_OK: return "OK";
+        case UFSECP_ERR_NULL_ARG: return "NULL argument";
+        case UFSECP_ERR_BAD_KEY: return "invalid private key";
+        case UFSECP_ERR_BAD_PUBKEY: return "invalid public key";
+        case UFSECP_ERR_BAD_SIG: return "invalid signature";
+        case UFSECP_ERR_BAD_INPUT: return "bad input";
+        case UFSECP_ERR_VERIFY_FAIL: return "verification failed";
+        case UFSECP_ERR_ARITH: return "arithmetic error";
+        case UFSECP_ERR_SELFTEST: return "self-test failed";
+        case UFSECP_ERR_INTERNAL: return "internal error";
+        case UFSECP_ERR_BUF_TOO_SMALL: return "buffer too small";
+        case UFSECP_ERR_NOT_FOUND: return "not found";
+        case UFSECP_ERR_DEPRECATED_API: return "deprecated API";
+        case UFSECP_ERR_CANCELLED: return "cancelled";
+        case UFSECP_ERR_GPU_UNAVAILABLE: return "GPU backend unavailable";
+        case UFSECP_ERR_GPU_DEVICE: return "GPU device not found or init failed";
+        case UFSECP_ERR_GPU_LAUNCH: return "GPU kernel launch failed";
+        case UFSECP_ERR_GPU_MEMORY: return "GPU memory allocation or copy failed";
+        case UFSECP_ERR_GPU_UNSUPPORTED: return "operation not supported on this GPU backend";
+        case UFSECP_ERR_GPU_BACKEND: return "GPU driver / runtime error";
+        case UFSECP_ERR_GPU_QUEUE: return "GPU queue / stream error";
+        default: return "unknown error";
+    }
+}
+
+// ---- verify ----------------------------------------------------------------
+
+ufsecp_error_t ufsecp_gpu_ecdsa_verify_batch(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32, const uint8_t* pubkeys33,
+                                             const uint8_t* sigs64, size_t count, uint8_t* out_results) {
+    return gated_verify(ctx, msg_hashes32, pubkeys33, sigs64, count, out_results, [&] {
+        return ctx->backend->verify_host(0, msg_hashes32, pubkeys33, sigs64, count, out_results, false);
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_schnorr_verify_batch(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32,
+                                               const uint8_t* pubkeys_x32, const uint8_t* sigs64, size_t count,
+                                               uint8_t* out_results) {
+    return gated_verify(ctx, msg_hashes32, pubkeys_x32, sigs64, count, out_results, [&] {
+        return ctx->backend->verify_host(1, msg_hashes32, pubkeys_x32, sigs64, count, out_results, false);
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ecdsa_verify_collect(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32,
+                                               const uint8_t* pubkeys33, const uint8_t* sigs64, size_t count,
+                                               uint8_t* key_buffer) {
+    return gated_collect(ctx, msg_hashes32, pubkeys33, sigs64, count, key_buffer, [&] {
+        return ctx->backend->verify_host(0, msg_hashes32, pubkeys33, sigs64, count, key_buffer, true);
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_schnorr_verify_collect(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32,
+                                                 const uint8_t* pubkeys_x32, const uint8_t* sigs64, size_t count,
+                                                 uint8_t* key_buffer) {
+    return gated_collect(ctx, msg_hashes32, pubkeys_x32, sigs64, count, key_buffer, [&] {
+        return ctx->backend->verify_host(1, msg_hashes32, pubkeys_x32, sigs64, count, key_buffer, true);
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ecdsa_verify_opaque_rows(ufsecp_gpu_ctx* ctx, const uint8_t* rows, size_t stride,
+                                                   size_t count, uint8_t* out_results) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (count > kMaxBatch || stride < 129u) return UFSECP_ERR_BAD_INPUT;
+    if (!rows || !out_results) return UFSECP_ERR_NULL_ARG;
+    clear_out(out_results, count, 1);
+    return unsupported(ctx, count);
+}
+
+ufsecp_error_t ufsecp_gpu_ecdsa_verify_lbtc_rows(ufsecp_gpu_ctx* ctx, const uint8_t* rows, size_t stride, size_t count,
+                                                 uint8_t* out_results) {
+    return ufsecp_gpu_ecdsa_verify_opaque_rows(ctx, rows, stride, count, out_results);
+}
+
+ufsecp_error_t ufsecp_gpu_ecdsa_verify_lbtc_columns(ufsecp_gpu_ctx* ctx, const uint8_t* digests32,
+                                                    const uint8_t* pubkeys33, const uint8_t* sigs64, size_t count,
+                                                    uint8_t* out_results) {
+    return gated_verify(ctx, digests32, pubkeys33, sigs64, count, out_results,
+                        [&] { return unsupported(ctx, count); });
+}
+
+ufsecp_error_t ufsecp_gpu_schnorr_verify_lbtc_columns(ufsecp_gpu_ctx* ctx, const uint8_t* digests32,
+                                                      const uint8_t* xonly32, const uint8_t* sigs64, size_t count,
+                                                      uint8_t* out_results) {
+    return gated_verify(ctx, digests32, xonly32, sigs64, count, out_results, [&] { return unsupported(ctx, count); });
+}
+
+// ---- the rest of the reference surface: not implemented here -----------------
+
+ufsecp_error_t ufsecp_gpu_generator_mul_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_ecdh_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_hash160_pubkey_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_msm(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, size_t n, uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_xonly_validate(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t n, uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_commitment_verify(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, const uint8_t*,
+                                            const uint8_t*, size_t n, uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_tagged_hash(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, size_t, size_t n,
+                                      uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_pubkey_validate(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t n, uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_tagged_hash_var(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, const uint32_t*,
+                                          size_t, size_t n, uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_hash256(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t, size_t n, uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_hash256_var(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint32_t*, size_t, size_t n,
+                                      uint8_t*) {
+    return unsupported(ctx, n);
+}
+ufsecp_error_t ufsecp_gpu_frost_verify_partial_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*,
+                                                     const uint8_t*, const uint8_t*, const uint8_t*, const uint8_t*,
+                                                     const uint8_t*, const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_ecrecover_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, const int*,
+                                          size_t count, uint8_t*, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_zk_knowledge_verify_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*,
+                                                    const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_zk_dleq_verify_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, const uint8_t*,
+                                               const uint8_t*, const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_bulletproof_verify_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*,
+                                                   const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_bip324_aead_encrypt_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*,
+                                                    const uint8_t*, const uint32_t*, uint32_t, size_t count,
+                                                    uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_bip324_aead_decrypt_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*,
+                                                    const uint8_t*, const uint32_t*, uint32_t, size_t count, uint8_t*,
+                                                    uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_zk_ecdsa_snark_witness_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*,
+                                                       const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_gpu_zk_schnorr_snark_witness_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*,
+                                                         const uint8_t*, size_t count, uint8_t*) {
+    return unsupported(ctx, count);
+}
+ufsecp_error_t ufsecp_bip352_prepare_scan_plan(const uint8_t*, uint8_t*) { return UFSECP_ERR_GPU_UNSUPPORTED; }
+ufsecp_error_t ufsecp_gpu_bip352_scan_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, const uint8_t*,
+                                            size_t n_tweaks, uint64_t*) {
+    return unsupported(ctx, n_tweaks);
+}
+
+// ---- B200 extensions -------------------------------------------------------
+
+ufsecp_error_t ufsecp_gpu_ext_ecdsa_verify_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
+                                                  const uint8_t* d_pubkeys33, const uint8_t* d_sigs64, size_t count,
+                                                  uint8_t* d_out_results, void* stream) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (count > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!d_msg_hashes32 || !d_pubkeys33 || !d_sigs64 || !d_out_results) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->verify_device(0, d_msg_hashes32, d_pubkeys33, d_sigs64, count, d_out_results,
+                                       (cudaStream_t)stream);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
+                                                    const uint8_t* d_pubkeys_x32, const uint8_t* d_sigs64,
+                                                    size_t count, uint8_t* d_out_results, void* stream) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (count > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!d_msg_hashes32 || !d_pubkeys_x32 || !d_sigs64 || !d_out_results) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->verify_device(1, d_msg_hashes32, d_pubkeys_x32, d_sigs64, count, d_out_results,
+                                       (cudaStream_t)stream);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_sign_device(ufsecp_gpu_ctx* ctx, uint32_t kind, const uint8_t* d_msgs32,
+                                          const uint8_t* d_privkeys32, const uint8_t* d_aux32, size_t count,
+                                          uint8_t* d_pubkeys_out, uint8_t* d_sigs64_out, uint8_t* d_ok, void* stream) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (kind > 1 || count > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!d_msgs32 || !d_privkeys32 || (kind == 1 && !d_aux32) || !d_pubkeys_out || !d_sigs64_out || !d_ok)
+        return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->sign_device((int)kind, d_msgs32, d_privkeys32, d_aux32, count, d_pubkeys_out, d_sigs64_out,
+                                     d_ok, (cudaStream_t)stream);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_stream(ufsecp_gpu_ctx* ctx, void** stream_out) {
+    if (!ctx || !stream_out) return UFSECP_ERR_NULL_ARG;
+    *stream_out = (void*)ctx->backend->stream();
+    return UFSECP_OK;
+}
+
+ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* sm_count, int* ecdsa_blocks_per_sm,
+                                           int* schnorr_blocks_per_sm) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    const int sms = ctx->backend->sms();
+    if (sm_count) *sm_count = sms;
+    if (ecdsa_blocks_per_sm) *ecdsa_blocks_per_sm = sms ? ctx->backend->verify_grid(0) / sms : 0;
+    if (schnorr_blocks_per_sm) *schnorr_blocks_per_sm = sms ? ctx->backend->verify_grid(1) / sms : 0;
+    return UFSECP_OK;
+}
+
+ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) {
+    if (!ctx || !ops_per_s) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->imad_peak(ops_per_s);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_diag(ufsecp_gpu_ctx* ctx, uint32_t op, const uint8_t* in, size_t n, uint8_t* out) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (!in || !out) return UFSECP_ERR_NULL_ARG;
+    static const int in_sz[11] = {0, 64, 32, 32, 32, 64, 32, 32, 32, 96, 96};
+    static const int out_sz[11] = {0, 32, 32, 32, 33, 32, 32, 34, 64, 65, 32};
+    if (op < 1 || op > 10 || n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    return ctx->backend->diag(op, in, n, out, (size_t)in_sz[op], (size_t)out_sz[op]);
+}
+
+}  // extern "C"

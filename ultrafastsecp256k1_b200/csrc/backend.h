@@ -1,0 +1,78 @@
+// CUDA backend of the C ABI: one device, its stream, the generator tables and
+// grow-only staging buffers.
+//
+// Role in the reference: CudaBackend (src/gpu/src/gpu_backend_cuda.cu:833;
+// ecdsa_verify_batch :972, schnorr_verify_batch :1085) behind the GpuBackend
+// interface (src/gpu/include/gpu_backend.hpp:79-607).  Differences by design:
+// device buffers are kept and grown instead of cudaMalloc/cudaFree per call,
+// every launch goes to the context's own stream, and the kernels are the
+// sm_100a ones of kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <string>
+
+namespace uf {
+
+// ABI error codes (same values as ufsecp_error.h / ufsecp_gpu.h).
+enum : int {
+    kOk = 0, kErrNullArg = 1, kErrBadInput = 5, kErrInternal = 9,
+    kErrGpuUnavailable = 100, kErrGpuDevice = 101, kErrGpuLaunch = 102, kErrGpuMemory = 103,
+    kErrGpuUnsupported = 104, kErrGpuBackend = 105, kErrGpuQueue = 106,
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
+class Backend {
+public:
+    Backend() = default;
+    ~Backend();
+    Backend(const Backend&) = delete;
+    Backend& operator=(const Backend&) = delete;
+
+    int init(int device_index);
+    bool ready() const { return ready_; }
+    int last_error() const { return last_err_; }
+    const char* last_error_msg() const { return last_msg_.c_str(); }
+    int device() const { return dev_; }
+    cudaStream_t stream() const { return stream_; }
+    const void* gtab() const { return d_gtab_; }
+    int sms() const { return sms_; }
+
+    // Host buffers in, host verdicts out; synchronous (the reference contract).
+    int verify_host(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs, size_t count,
+                    uint8_t* out, bool collect);
+    // Device buffers in / out, asynchronous on `stream` (nullptr = context stream).
+    int verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pubs, const uint8_t* d_sigs, size_t count,
+                      uint8_t* d_out, cudaStream_t stream);
+    // Batch signing (workload generator), device buffers, asynchronous.
+    int sign_device(int kind, const uint8_t* d_msgs, const uint8_t* d_sks, const uint8_t* d_auxs, size_t count,
+                    uint8_t* d_pubs, uint8_t* d_sigs, uint8_t* d_ok, cudaStream_t stream);
+    int diag(uint32_t op, const uint8_t* in, size_t n, uint8_t* out, size_t in_sz, size_t out_sz);
+    int imad_peak(double* ops_per_s);
+
+    int verify_grid(int kind) const { return kind == 0 ? grid_ecdsa_ : grid_schnorr_; }
+
+    int set_error(int code, const char* what);
+    int cuda_error(cudaError_t e, const char* what);
+    void clear_error() { last_err_ = kOk; last_msg_ = "OK"; }
+
+private:
+    bool ready_ = false;
+    int dev_ = -1;
+    int sms_ = 0;
+    int grid_ecdsa_ = 0, grid_schnorr_ = 0;
+    cudaStream_t stream_ = nullptr;
+    void* d_gtab_ = nullptr;
+    DevBuf msgs_, pubs_, sigs_, out_, scratch_;
+    int last_err_ = kOk;
+    std::string last_msg_ = "OK";
+};
+
+}  // namespace uf

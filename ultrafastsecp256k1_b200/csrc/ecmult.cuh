@@ -1,0 +1,158 @@
+// R = a*G + b*P: the double-scalar multiplication at the centre of verify.
+//
+// Role in the reference: shamir_double_mul_glv (src/cuda/include/secp256k1.cuh:3575-3801,
+// a bit-by-bit 4-stream Strauss with a per-signature joint table) and the CPU's
+// Point::dual_scalar_mul_gen_point (src/cpu/src/point.cpp:4079).  Re-designed for
+// SIMT on sm_100a:
+//
+//  * both scalars are GLV-split, giving four 128-bit streams: a1*G, a2*(lambda G),
+//    b1*P, b2*(lambda P) with lambda(x, y) = (beta x, y);
+//  * every stream uses FIXED-position signed (Booth) windows recoded on the fly,
+//    so all 32 lanes of a warp add at the same loop positions (a wNAF's
+//    data-dependent positions would make the warp add at almost every bit);
+//  * P streams: 4-bit windows, table of 1P..8P (affine, one field inversion per
+//    signature through a batch-to-affine), lambda P via one beta multiplication;
+//  * G streams: 8-bit windows every second P window, tables of 1..128 multiples
+//    of G and of lambda G computed once per context and read through the L1;
+//  * 33 P windows x 4 bits = 132 >= 129 bits, so 128 doublings in total.
+#pragma once
+#include "common.cuh"
+#include "fe.cuh"
+#include "fn.cuh"
+#include "point.cuh"
+
+namespace uf {
+
+constexpr int kWP = 4;     // P window bits
+constexpr int kNWP = 33;   // P windows
+constexpr int kWG = 8;     // G window bits
+constexpr int kNWG = 17;   // G windows (one per two P windows)
+constexpr int kPTab = 8;   // 1P..8P
+constexpr int kGTab = 128; // 1G..128G (and the same for lambda G)
+
+// Signed fixed-window (Booth) digits of a magnitude k < 2^129:
+// d_i = b_{wi-1} + sum_{t<w-1} b_{wi+t} 2^t - b_{wi+w-1} 2^(w-1), d_i in [-2^(w-1), 2^(w-1)],
+// sum_i d_i 2^(wi) = k.
+template <int W, int NW, typename T>
+UF_HD void booth_recode(T* out, const uint32_t k[4]) {
+    const uint32_t kk[6] = {k[0], k[1], k[2], k[3], 0u, 0u};
+    const uint32_t mask = (1u << (W + 1)) - 1u;
+    UF_UNROLL
+    for (int i = 0; i < NW; ++i) {
+        const int pos = W * i - 1;
+        uint32_t raw;
+        if (pos < 0) {
+            raw = (kk[0] << 1) & mask;
+        } else {
+            const int li = pos >> 5, off = pos & 31;
+            const uint64_t v = ((uint64_t)kk[li + 1] << 32) | kk[li];
+            raw = (uint32_t)(v >> off) & mask;
+        }
+        out[i] = (T)((int)(raw & 1u) + (int)((raw >> 1) & ((1u << (W - 1)) - 1u)) - (int)((raw >> W) << (W - 1)));
+    }
+}
+
+// Table of (k+1)*P for k = 0..7, affine.  Tab must provide
+// store(k, Fe x, Fe y) / load(k, Fe& x, Fe& y).
+template <class Tab>
+UF_HDI void build_ptable(Tab& tab, const Fe& px, const Fe& py) {
+    Fe zs[kPTab - 1], cs[kPTab - 1];
+    tab.store(0, px, py);
+    UF_NOUNROLL
+    for (int k = 2; k <= kPTab; ++k) {
+        Jac t;
+        t.inf = false;
+        if ((k & 1) == 0) {
+            if (k == 2) {
+                jac_from_aff(t, px, py);
+            } else {
+                tab.load(k / 2 - 1, t.X, t.Y);
+                t.Z = zs[k / 2 - 2];
+            }
+            jac_dbl(t);
+        } else {
+            tab.load(k - 2, t.X, t.Y);
+            t.Z = zs[k - 3];
+            jac_add_aff(t, px, py);
+        }
+        tab.store(k - 1, t.X, t.Y);
+        zs[k - 2] = t.Z;
+        if (k == 2) cs[0] = t.Z;
+        else fe_mul(cs[k - 2], cs[k - 3], t.Z);
+    }
+    // one inversion for all seven Z (Montgomery's trick)
+    Fe inv;
+    fe_inv(inv, cs[kPTab - 2]);
+    UF_NOUNROLL
+    for (int k = kPTab; k >= 2; --k) {
+        Fe zi, zi2, X, Y;
+        if (k > 2) {
+            fe_mul(zi, inv, cs[k - 3]);
+            fe_mul(inv, inv, zs[k - 2]);
+        } else {
+            zi = inv;
+        }
+        fe_sqr(zi2, zi);
+        tab.load(k - 1, X, Y);
+        fe_mul(X, X, zi2);
+        fe_mul(zi2, zi2, zi);
+        fe_mul(Y, Y, zi2);
+        tab.store(k - 1, X, Y);
+    }
+}
+
+template <class Tab>
+UF_HD void add_ptab(Jac& R, const Tab& tab, int d, bool sneg, bool lam, const Fe& beta) {
+    if (d == 0) return;
+    const bool neg = (d < 0) != sneg;
+    const int idx = (d < 0 ? -d : d) - 1;
+    Fe x, y;
+    tab.load(idx, x, y);
+    if (lam) fe_mul(x, x, beta);
+    if (neg) fe_neg(y, y);
+    jac_add_aff(R, x, y);
+}
+
+template <class GT>
+UF_HD void add_gtab(Jac& R, const GT& gt, int d, bool sneg, int lam) {
+    if (d == 0) return;
+    const bool neg = (d < 0) != sneg;
+    const int idx = (d < 0 ? -d : d) - 1 + lam * kGTab;
+    Fe x, y;
+    gt.load(idx, x, y);
+    if (neg) fe_neg(y, y);
+    jac_add_aff(R, x, y);
+}
+
+// R = a*G + b*P for P = (px, py) on the curve (not infinity).
+template <class Tab, class GT>
+UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt) {
+    GlvSplit sa, sb;
+    glv_split(sa, a);
+    glv_split(sb, b);
+    int8_t dp1[kNWP], dp2[kNWP];
+    int16_t dg1[kNWG], dg2[kNWG];
+    booth_recode<kWP, kNWP>(dp1, sb.k1);
+    booth_recode<kWP, kNWP>(dp2, sb.k2);
+    booth_recode<kWG, kNWG>(dg1, sa.k1);
+    booth_recode<kWG, kNWG>(dg2, sa.k2);
+    build_ptable(tab, px, py);
+    Fe beta;
+    fe_beta(beta);
+    jac_set_inf(R);
+    UF_NOUNROLL
+    for (int i = kNWP - 1; i >= 0; --i) {
+        if (i != kNWP - 1) {
+            UF_UNROLL
+            for (int j = 0; j < kWP; ++j) jac_dbl(R);
+        }
+        add_ptab(R, tab, dp1[i], sb.neg1, false, beta);
+        add_ptab(R, tab, dp2[i], sb.neg2, true, beta);
+        if ((i & 1) == 0) {
+            add_gtab(R, gt, dg1[i >> 1], sa.neg1, 0);
+            add_gtab(R, gt, dg2[i >> 1], sa.neg2, 1);
+        }
+    }
+}
+
+}  // namespace uf

@@ -173,9 +173,19 @@ class RefLib:
         L.ufsecp_pubkey_xonly.argtypes = [ctypes.c_void_p, _u8p, _u8p]
         L.ufsecp_schnorr_batch_verify.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t]
         L.ufsecp_schnorr_batch_verify.restype = ctypes.c_int
+        L.ufsecp_set_cache_dir.argtypes = [ctypes.c_char_p]
+        L.ufsecp_set_cache_dir(_CACHE_DIR.encode())
         self._tls = threading.local()
         self._ctxs = []
         self._lock = threading.Lock()
+        # build the library's fixed-base tables once from the cache dir (it saves
+        # them to the working directory when the cache dir has no copy yet)
+        cwd = os.getcwd()
+        try:
+            os.chdir(_CACHE_DIR)
+            self.ecdsa_sign(bytes(32), bytes(31) + b"\x01")
+        finally:
+            os.chdir(cwd)
 
     def ctx(self):
         c = getattr(self._tls, "ctx", None)
@@ -253,11 +263,11 @@ class RefDriver:
         if not os.path.exists(drv_path):
             raise FileNotFoundError(f"{drv_path} missing: run `make -C oracle oracle`")
         self.L = ctypes.CDLL(drv_path)
-        self.L.refdrv_open.argtypes = [ctypes.c_char_p]
+        self.L.refdrv_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
         self.L.refdrv_verify.argtypes = [ctypes.c_int, _u8p, _u8p, _u8p, ctypes.c_size_t, _u8p, ctypes.c_int]
         self.L.refdrv_sign.argtypes = [ctypes.c_int, _u8p, _u8p, _u8p, ctypes.c_size_t, _u8p, _u8p, _u8p,
                                        ctypes.c_int]
-        rc = self.L.refdrv_open(ref_path.encode())
+        rc = self.L.refdrv_open(ref_path.encode(), _CACHE_DIR.encode())
         if rc != 0:
             raise RuntimeError(f"refdrv_open failed: {rc}")
 

@@ -11,6 +11,8 @@
  * sig64, pubkey_x32) (:992).  Verdict = return code == UFSECP_OK.
  */
 #include <dlfcn.h>
+#include <limits.h>
+#include <unistd.h>
 #include <pthread.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -26,7 +28,7 @@ static ctx_destroy_fn g_destroy;
 static verify_fn g_ecdsa, g_schnorr;
 
 /* Returns 0 on success. */
-int refdrv_open(const char *path) {
+int refdrv_open(const char *path, const char *cache_dir) {
     if (g_lib) return 0;
     g_lib = dlopen(path, RTLD_NOW | RTLD_LOCAL);
     if (!g_lib) { fprintf(stderr, "refdrv: %s\n", dlerror()); return 1; }
@@ -34,6 +36,26 @@ int refdrv_open(const char *path) {
     g_destroy = (ctx_destroy_fn)dlsym(g_lib, "ufsecp_ctx_destroy");
     g_ecdsa = (verify_fn)dlsym(g_lib, "ufsecp_ecdsa_verify");
     g_schnorr = (verify_fn)dlsym(g_lib, "ufsecp_schnorr_verify");
+    /* the library's generator cache goes where the caller says (ufsecp_set_cache_dir,
+     * include/ufsecp/ufsecp.h:136), not into the working directory */
+    int (*set_dir)(const char *) = (int (*)(const char *))dlsym(g_lib, "ufsecp_set_cache_dir");
+    if (set_dir && cache_dir) set_dir(cache_dir);
+    /* The first generator multiplication builds the library's fixed-base tables
+     * and saves them to the working directory when the cache dir has no copy yet
+     * (src/cpu/src/precompute.cpp:2235-2256), so do that once from the cache dir. */
+    typedef int (*pk_fn)(void *, const uint8_t *, uint8_t *);
+    pk_fn pk = (pk_fn)dlsym(g_lib, "ufsecp_pubkey_create");
+    char cwd[PATH_MAX];
+    if (pk && cache_dir && g_create && getcwd(cwd, sizeof cwd) && chdir(cache_dir) == 0) {
+        void *ctx = NULL;
+        uint8_t sk[32] = {0}, pub[33];
+        sk[31] = 1;
+        if (g_create(&ctx) == 0) {
+            pk(ctx, sk, pub);
+            g_destroy(ctx);
+        }
+        if (chdir(cwd) != 0) return 4;
+    }
     return (g_create && g_destroy && g_ecdsa && g_schnorr) ? 0 : 2;
 }
 

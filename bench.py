@@ -281,7 +281,9 @@ def run_ours(args):
     n = args.batch
     (d_msgs, d_xs, d_sigs, d_out), (msgs, xs, sigs), expect = make_schnorr_batch(ctx, torch, n,
                                                                                  seed=20261203 + rank)
-    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()   # inputs were written on the default stream
+    # an explicit stream: the launches and the events that time them share it
+    stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
 
     def launch():
@@ -406,7 +408,8 @@ def ecdsa_4096_rate(ctx, torch):
     d_s = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
     d_ok = torch.empty(n, dtype=torch.uint8, device="cuda")
     d_out = torch.empty(n, dtype=torch.uint8, device="cuda")
-    st = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    st = torch.cuda.Stream()
     ctx.sign_device(0, d_m.data_ptr(), d_k.data_ptr(), 0, n, d_p.data_ptr(), d_s.data_ptr(), d_ok.data_ptr(),
                     st.cuda_stream)
     for _ in range(3):

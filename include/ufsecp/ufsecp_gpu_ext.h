@@ -50,6 +50,15 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* 
  * every thread of a full grid runs 16 independent mad.lo.u32 chains. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s);
 
+/* Building-block throughput probe: launches blocks x threads threads, each
+ * running `iters` rounds of one operation on register-resident values, and
+ * returns the launch time in milliseconds (CUDA events).  op: 1 two fe_mul
+ * chains, 2 two fe_sqr chains, 3 fe_inv, 4 sqrt exponentiation, 5 Jacobian
+ * doubling, 6 Jacobian + affine add, 7 scalar inverse, 8 GLV split,
+ * 9 BIP-340 challenge hash. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int blocks, int threads, int iters,
+                                               float* ms_out);
+
 /* Device arithmetic probes (one item per thread), host buffers in and out.
  * op  in -> out bytes per item
  *  1  a|b (64) -> a*b mod p (32)         2  a (32) -> a^2 mod p (32)

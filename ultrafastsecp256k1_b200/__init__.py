@@ -78,6 +78,8 @@ _SIGS = {
                                                    ctypes.POINTER(ctypes.c_int)]),
     "ufsecp_gpu_ext_imad_peak": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "ufsecp_gpu_ext_diag": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_size_t, _vp]),
+    "ufsecp_gpu_ext_probe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_float)]),
 }
 
 
@@ -250,6 +252,12 @@ class GpuContext:
         v = ctypes.c_double()
         self._check(self.L.ufsecp_gpu_ext_imad_peak(self._ctx, ctypes.byref(v)), "imad_peak")
         return v.value
+
+    def probe(self, op: int, blocks: int, threads: int, iters: int) -> float:
+        """Building-block throughput probe; returns the launch time in ms."""
+        ms = ctypes.c_float()
+        self._check(self.L.ufsecp_gpu_ext_probe(self._ctx, op, blocks, threads, iters, ctypes.byref(ms)), "probe")
+        return ms.value
 
     _DIAG_IO = {1: (64, 32), 2: (32, 32), 3: (32, 32), 4: (32, 33), 5: (64, 32), 6: (32, 32), 7: (32, 34),
                 8: (32, 64), 9: (96, 65), 10: (96, 32)}

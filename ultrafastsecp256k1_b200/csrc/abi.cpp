@@ -414,6 +414,12 @@ ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) 
     return ctx->backend->imad_peak(ops_per_s);
 }
 
+ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int blocks, int threads, int iters, float* ms_out) {
+    if (!ctx || !ms_out) return UFSECP_ERR_NULL_ARG;
+    if (op < 1 || op > 9 || blocks < 1 || threads < 1 || threads > 1024 || iters < 1) return UFSECP_ERR_BAD_INPUT;
+    return ctx->backend->probe(op, blocks, threads, iters, ms_out);
+}
+
 ufsecp_error_t ufsecp_gpu_ext_diag(ufsecp_gpu_ctx* ctx, uint32_t op, const uint8_t* in, size_t n, uint8_t* out) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     if (n == 0) return UFSECP_OK;

@@ -206,4 +206,27 @@ int Backend::imad_peak(double* ops_per_s) {
     return kOk;
 }
 
+int Backend::probe(int op, int blocks, int threads, int iters, float* ms) {
+    if (!ready_) return set_error(kErrGpuDevice, "context not ready");
+    cudaError_t e = cudaSetDevice(dev_);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    if ((e = scratch_.ensure(4096 * sizeof(uint32_t))) != cudaSuccess) return cuda_error(e, "cudaMalloc");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    e = launch_probe(op, blocks, threads, 1, (uint32_t*)scratch_.p, stream_);   // warm-up
+    if (e == cudaSuccess) {
+        cudaEventRecord(a, stream_);
+        e = launch_probe(op, blocks, threads, iters, (uint32_t*)scratch_.p, stream_);
+        cudaEventRecord(b, stream_);
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) return cuda_error(e, "probe");
+    clear_error();
+    return kOk;
+}
+
 }  // namespace uf

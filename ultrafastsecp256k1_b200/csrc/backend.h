@@ -56,6 +56,7 @@ public:
                     uint8_t* d_pubs, uint8_t* d_sigs, uint8_t* d_ok, cudaStream_t stream);
     int diag(uint32_t op, const uint8_t* in, size_t n, uint8_t* out, size_t in_sz, size_t out_sz);
     int imad_peak(double* ops_per_s);
+    int probe(int op, int blocks, int threads, int iters, float* ms);
 
     int verify_grid(int kind) const { return kind == 0 ? grid_ecdsa_ : grid_schnorr_; }
 

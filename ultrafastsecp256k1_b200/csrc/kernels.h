@@ -45,4 +45,7 @@ cudaError_t launch_diag(uint32_t op, const uint8_t* in, uint32_t n, uint8_t* out
 // 16 independent 32-bit IMADs.  Returns a checksum so the work is not elided.
 cudaError_t launch_imad_peak(uint32_t* d_sink, int blocks, int threads, int iters, cudaStream_t s);
 
+// Building-block throughput probe (op codes in ufsecp_gpu_ext.h).
+cudaError_t launch_probe(int op, int blocks, int threads, int iters, uint32_t* sink, cudaStream_t s);
+
 }  // namespace uf

@@ -46,6 +46,16 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_stream(ufsecp_gpu_ctx* ctx, void** stre
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* sm_count, int* ecdsa_blocks_per_sm,
                                                       int* schnorr_blocks_per_sm);
 
+/* Verify-kernel variant per signature kind (0 ECDSA, 1 BIP-340).  The
+ * variants compute the same verdicts; they differ in how much of the field /
+ * point arithmetic is inlined (instruction-cache footprint vs. call overhead).
+ * ultrafastsecp256k1_b200.autotune measures them and writes the tuning file
+ * read at context creation (UFSECP_B200_TUNING). */
+#define UFSECP_EXT_VERIFY_VARIANTS 4
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_variant(ufsecp_gpu_ctx* ctx, int kind, int variant);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out,
+                                                     int* blocks_per_sm_out);
+
 /* Measured 32-bit integer multiply-add issue rate of the device (ops / s):
  * every thread of a full grid runs 16 independent mad.lo.u32 chains. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s);

@@ -76,6 +76,9 @@ _SIGS = {
     "ufsecp_gpu_ext_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "ufsecp_gpu_ext_device_props": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                                    ctypes.POINTER(ctypes.c_int)]),
+    "ufsecp_gpu_ext_set_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "ufsecp_gpu_ext_get_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                  ctypes.POINTER(ctypes.c_int)]),
     "ufsecp_gpu_ext_imad_peak": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "ufsecp_gpu_ext_diag": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_probe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -247,6 +250,15 @@ class GpuContext:
         self._check(self.L.ufsecp_gpu_ext_device_props(self._ctx, ctypes.byref(sms), ctypes.byref(be),
                                                        ctypes.byref(bs)), "device_props")
         return {"sm_count": sms.value, "ecdsa_blocks_per_sm": be.value, "schnorr_blocks_per_sm": bs.value}
+
+    def set_variant(self, kind: int, variant: int) -> None:
+        self._check(self.L.ufsecp_gpu_ext_set_variant(self._ctx, kind, variant), "set_variant")
+
+    def get_variant(self, kind: int):
+        v, b = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.ufsecp_gpu_ext_get_variant(self._ctx, kind, ctypes.byref(v), ctypes.byref(b)),
+                    "get_variant")
+        return v.value, b.value
 
     def imad_peak(self) -> float:
         v = ctypes.c_double()

@@ -1,0 +1,114 @@
+"""Autotuner for the verify kernels.
+
+    python -m ultrafastsecp256k1_b200.autotune [--batch N] [--out PATH]
+
+For each signature kind (ECDSA, BIP-340) it times every verify-kernel variant
+(ufsecp_gpu_ext_set_variant; the variants differ in how much field / point
+arithmetic is inlined, i.e. instruction-cache footprint against call
+overhead) on a GPU-signed batch, checks that all variants return identical
+verdicts, and writes the winners to a tuning file of "key value" lines:
+
+    ultrafastsecp256k1_b200/tuning/<device name>_<SMs>sm.txt
+
+The C++ backend reads that file at context creation (or the file named by
+UFSECP_B200_TUNING).  Prints the measurements as JSON.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+
+import numpy as np
+
+import ultrafastsecp256k1_b200 as uf
+
+TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
+VARIANTS = 4
+
+
+def tuning_path(name: str, sms: int) -> str:
+    return os.path.join(TUNING_DIR, f"{re.sub(r'[^A-Za-z0-9]+', '_', name).strip('_')}_{sms}sm.txt")
+
+
+def signed_batch(ctx, torch, kind: int, n: int, seed: int):
+    rng = np.random.default_rng(seed)
+    sks = rng.integers(1, 255, (n, 32), dtype=np.uint8)
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    aux = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    d_m, d_k, d_a = dev(msgs), dev(sks), dev(aux)
+    ps = 33 if kind == 0 else 32
+    d_p = torch.empty(n * ps, dtype=torch.uint8, device="cuda")
+    d_s = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+    d_ok = torch.empty(n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ctx.sign_device(kind, d_m.data_ptr(), d_k.data_ptr(), d_a.data_ptr(), n, d_p.data_ptr(), d_s.data_ptr(),
+                    d_ok.data_ptr(), 0)
+    torch.cuda.synchronize()
+    torch.cuda.ExternalStream(ctx.stream()).synchronize()
+    # flip one bit in every 50th signature so the verdicts are not all 1
+    s = d_s.view(n, 64)
+    s[::50, 40] ^= 0x04
+    torch.cuda.synchronize()
+    return d_m, d_p, d_s
+
+
+def time_variant(ctx, torch, kind, bufs, n, reps=3):
+    d_m, d_p, d_s = bufs
+    out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    fn = ctx.ecdsa_verify_device if kind == 0 else ctx.schnorr_verify_device
+    fn(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), n, out.data_ptr(), st.cuda_stream)   # warm-up
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        fn(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), n, out.data_ptr(), st.cuda_stream)
+    b.record(st)
+    st.synchronize()
+    ms = a.elapsed_time(b) / reps
+    return n / (ms * 1e-3), out.cpu().numpy()
+
+
+def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = True) -> dict:
+    import torch
+    info = uf.device_info(0)
+    name = info.name.decode()
+    res = {"device": name, "sm_count": info.compute_units, "batch": batch, "kinds": {}}
+    with uf.GpuContext(0) as ctx:
+        for kind, label in ((0, "ecdsa"), (1, "schnorr")):
+            bufs = signed_batch(ctx, torch, kind, batch, seed=77 + kind)
+            rates, ref = {}, None
+            for v in range(VARIANTS):
+                ctx.set_variant(kind, v)
+                rate, verdicts = time_variant(ctx, torch, kind, bufs, batch)
+                if ref is None:
+                    ref = verdicts
+                elif not (verdicts == ref).all():
+                    raise RuntimeError(f"variant {v} disagrees with variant 0 on {label}")
+                rates[v] = rate
+            best = max(rates, key=rates.get)
+            res["kinds"][label] = {"sigs_per_s": {str(k): r for k, r in rates.items()}, "best": best,
+                                   "valid": int(ref.sum())}
+    if write:
+        path = out_path or tuning_path(name, info.compute_units)
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        with open(path, "w") as f:
+            f.write(f"ecdsa_variant {res['kinds']['ecdsa']['best']}\n")
+            f.write(f"schnorr_variant {res['kinds']['schnorr']['best']}\n")
+        res["tuning_file"] = path
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--batch", type=int, default=1 << 18)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--no-write", action="store_true")
+    a = ap.parse_args()
+    print(json.dumps(autotune(a.batch, a.out, not a.no_write), indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -36,8 +36,24 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+# kernels_verify.cu is compiled once per code-size variant (see csrc/common.cuh)
+VARIANTS = {
+    "kernels_verify.cu": [
+        ("v0", ["-DUF_VARIANT=0"]),
+        ("v1", ["-DUF_VARIANT=1", "-DUF_NOINLINE_POINT"]),
+        ("v2", ["-DUF_VARIANT=2", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD"]),
+        ("v3", ["-DUF_VARIANT=3", "-DUF_NOINLINE_FIELD"]),
+    ],
+}
+
+
 def _sources():
-    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    """(source, object suffix, extra flags) for every compile job."""
+    jobs = []
+    for src in sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp"))):
+        for suffix, flags in VARIANTS.get(os.path.basename(src), [("", [])]):
+            jobs.append((src, suffix, flags))
+    return jobs
 
 
 def _headers_mtime() -> float:
@@ -46,13 +62,14 @@ def _headers_mtime() -> float:
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 
-def _compile(src: str, force: bool, verbose: bool) -> str:
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+def _compile(job, force: bool, verbose: bool) -> str:
+    src, suffix, flags = job
+    obj = os.path.join(BUILD, os.path.basename(src) + (("." + suffix) if suffix else "") + ".o")
     if not force and os.path.exists(obj):
         newest = max(os.path.getmtime(src), _headers_mtime())
         if os.path.getmtime(obj) >= newest:
             return obj
-    cmd = [nvcc()] + ARCH + COMMON + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
     if src.endswith(".cu") and verbose:
         cmd += ["-Xptxas", "-v"]
     res = subprocess.run(cmd, capture_output=True, text=True)

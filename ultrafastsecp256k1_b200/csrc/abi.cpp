@@ -409,6 +409,19 @@ ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* sm_count, i
     return UFSECP_OK;
 }
 
+ufsecp_error_t ufsecp_gpu_ext_set_variant(ufsecp_gpu_ctx* ctx, int kind, int variant) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->set_variant(kind, variant);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_get_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out, int* blocks_per_sm_out) {
+    if (!ctx || !variant_out) return UFSECP_ERR_NULL_ARG;
+    if (kind < 0 || kind > 1) return UFSECP_ERR_BAD_INPUT;
+    *variant_out = ctx->backend->variant(kind);
+    if (blocks_per_sm_out) *blocks_per_sm_out = ctx->backend->blocks_per_sm(kind, *variant_out);
+    return UFSECP_OK;
+}
+
 ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) {
     if (!ctx || !ops_per_s) return UFSECP_ERR_NULL_ARG;
     return ctx->backend->imad_peak(ops_per_s);

@@ -1,7 +1,11 @@
 // CUDA backend implementation (see backend.h).
 #include "backend.h"
 
+#include <dlfcn.h>
+
 #include <algorithm>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "kernels.h"
@@ -11,7 +15,79 @@ namespace uf {
 namespace {
 // Items per host->device chunk: bounds device memory at ~130 B x 2^22 = 0.5 GB.
 constexpr size_t kChunk = size_t{1} << 22;
+
+const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
+                                                     launch_verify_v3};
+const verify_occupancy_fn kOccupancy[kVerifyVariants] = {verify_occupancy_v0, verify_occupancy_v1,
+                                                         verify_occupancy_v2, verify_occupancy_v3};
+
+int env_int(const char* name, int dflt) {
+    const char* v = getenv(name);
+    return (v && *v) ? atoi(v) : dflt;
+}
 }  // namespace
+
+cudaError_t Backend::launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
+                                   uint8_t* out, int collect, cudaStream_t st) {
+    const int v = variant_[kind & 1];
+    return kLaunchers[v](kind, m, p, s, n, d_gtab_, out, collect, grid_[v][kind & 1], st);
+}
+
+int Backend::set_variant(int kind, int v) {
+    if (kind < 0 || kind > 1 || v < 0 || v >= kVerifyVariants) return set_error(kErrBadInput, "bad variant");
+    variant_[kind] = v;
+    clear_error();
+    return kOk;
+}
+
+// Per-device tuning: a file of "key value" lines (ecdsa_variant,
+// schnorr_variant) written by ultrafastsecp256k1_b200.autotune.  It is the file
+// named by UFSECP_B200_TUNING, else tuning/<device name>_<SMs>sm.txt beside the
+// library's lib/ directory.  UFSECP_B200_VARIANT_ECDSA / _SCHNORR override
+// single entries.
+void Backend::load_tuning() {
+    std::string path_s;
+    const char* env = getenv("UFSECP_B200_TUNING");
+    if (env && *env) {
+        path_s = env;
+    } else {
+        Dl_info info;
+        if (dladdr((void*)&launch_verify_v0, &info) && info.dli_fname) {
+            std::string lib = info.dli_fname;
+            const size_t slash = lib.rfind('/');
+            const std::string dir = slash == std::string::npos ? std::string(".") : lib.substr(0, slash);
+            std::string name;
+            bool sep = false;
+            for (const char* c = dev_name_.c_str(); *c; ++c) {
+                const bool alnum = (*c >= 'a' && *c <= 'z') || (*c >= 'A' && *c <= 'Z') || (*c >= '0' && *c <= '9');
+                if (alnum) {
+                    if (sep && !name.empty()) name += '_';
+                    name += *c;
+                    sep = false;
+                } else {
+                    sep = true;
+                }
+            }
+            path_s = dir + "/../tuning/" + name + "_" + std::to_string(sms_) + "sm.txt";
+        }
+    }
+    const char* path = path_s.c_str();
+    if (*path) {
+        FILE* f = fopen(path, "r");
+        if (f) {
+            char key[64];
+            int val;
+            while (fscanf(f, "%63s %d", key, &val) == 2) {
+                if (!strcmp(key, "ecdsa_variant") && val >= 0 && val < kVerifyVariants) variant_[0] = val;
+                if (!strcmp(key, "schnorr_variant") && val >= 0 && val < kVerifyVariants) variant_[1] = val;
+            }
+            fclose(f);
+        }
+    }
+    const int ve = env_int("UFSECP_B200_VARIANT_ECDSA", -1), vs = env_int("UFSECP_B200_VARIANT_SCHNORR", -1);
+    if (ve >= 0 && ve < kVerifyVariants) variant_[0] = ve;
+    if (vs >= 0 && vs < kVerifyVariants) variant_[1] = vs;
+}
 
 cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap) return cudaSuccess;
@@ -81,13 +157,15 @@ int Backend::init(int device_index) {
     if ((e = cudaGetDeviceProperties(&prop, dev_)) != cudaSuccess) return cuda_error(e, "cudaGetDeviceProperties");
     if (prop.major < 10) return set_error(kErrGpuDevice, "this build targets sm_100a (B200)");
     sms_ = prop.multiProcessorCount;
+    dev_name_ = prop.name;
     if ((e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking)) != cudaSuccess)
         return cuda_error(e, "cudaStreamCreate");
     if ((e = cudaMalloc(&d_gtab_, kGTableBytes)) != cudaSuccess) return cuda_error(e, "cudaMalloc(gtab)");
     if ((e = launch_gtable_init(d_gtab_, stream_)) != cudaSuccess) return cuda_error(e, "gtable init launch");
     if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return cuda_error(e, "gtable init");
-    grid_ecdsa_ = std::max(1, verify_blocks_per_sm(0)) * sms_;
-    grid_schnorr_ = std::max(1, verify_blocks_per_sm(1)) * sms_;
+    for (int v = 0; v < kVerifyVariants; ++v)
+        for (int k = 0; k < 2; ++k) grid_[v][k] = std::max(1, kOccupancy[v](k)) * sms_;
+    load_tuning();
     (void)cudaGetLastError();
     ready_ = true;
     clear_error();
@@ -104,8 +182,7 @@ int Backend::verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pub
     cudaError_t e = cudaSetDevice(dev_);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
     cudaStream_t s = stream ? stream : stream_;
-    e = kind == 0 ? launch_ecdsa_verify(d_msgs, d_pubs, d_sigs, (uint32_t)count, d_gtab_, d_out, 0, grid_ecdsa_, s)
-                  : launch_schnorr_verify(d_msgs, d_pubs, d_sigs, (uint32_t)count, d_gtab_, d_out, 0, grid_schnorr_, s);
+    e = launch_verify(kind, d_msgs, d_pubs, d_sigs, (uint32_t)count, d_out, 0, s);
     if (e != cudaSuccess) return cuda_error(e, "verify launch");
     clear_error();
     return kOk;
@@ -135,8 +212,7 @@ int Backend::verify_host(int kind, const uint8_t* msgs, const uint8_t* pubs, con
             return cuda_error(e, "host->device copy");
         if (collect && (e = cudaMemcpyAsync(dout, out + off, m, cudaMemcpyHostToDevice, stream_)) != cudaSuccess)
             return cuda_error(e, "host->device copy");
-        e = kind == 0 ? launch_ecdsa_verify(dm, dp, ds, (uint32_t)m, d_gtab_, dout, collect, grid_ecdsa_, stream_)
-                      : launch_schnorr_verify(dm, dp, ds, (uint32_t)m, d_gtab_, dout, collect, grid_schnorr_, stream_);
+        e = launch_verify(kind, dm, dp, ds, (uint32_t)m, dout, collect, stream_);
         if (e != cudaSuccess) return cuda_error(e, "verify launch");
         if ((e = cudaMemcpyAsync(out + off, dout, m, cudaMemcpyDeviceToHost, stream_)) != cudaSuccess)
             return cuda_error(e, "device->host copy");

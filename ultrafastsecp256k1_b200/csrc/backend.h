@@ -58,7 +58,11 @@ public:
     int imad_peak(double* ops_per_s);
     int probe(int op, int blocks, int threads, int iters, float* ms);
 
-    int verify_grid(int kind) const { return kind == 0 ? grid_ecdsa_ : grid_schnorr_; }
+    // Kernel variant per signature kind (0 ECDSA, 1 BIP-340) and its grid.
+    int variant(int kind) const { return variant_[kind & 1]; }
+    int set_variant(int kind, int v);
+    int verify_grid(int kind) const { return grid_[variant_[kind & 1]][kind & 1]; }
+    int blocks_per_sm(int kind, int v) const { return sms_ ? grid_[v][kind & 1] / sms_ : 0; }
 
     int set_error(int code, const char* what);
     int cuda_error(cudaError_t e, const char* what);
@@ -68,7 +72,12 @@ private:
     bool ready_ = false;
     int dev_ = -1;
     int sms_ = 0;
-    int grid_ecdsa_ = 0, grid_schnorr_ = 0;
+    std::string dev_name_;
+    int grid_[4][2] = {};        // [variant][kind] resident-grid size
+    int variant_[2] = {1, 1};    // chosen variant per kind
+    cudaError_t launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
+                              uint8_t* out, int collect, cudaStream_t st);
+    void load_tuning();
     cudaStream_t stream_ = nullptr;
     void* d_gtab_ = nullptr;
     DevBuf msgs_, pubs_, sigs_, out_, scratch_;

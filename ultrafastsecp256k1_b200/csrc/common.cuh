@@ -16,6 +16,32 @@
 #define UF_HDI static inline
 #endif
 
+// Code-size control.  The verify kernel is long straight-line integer code;
+// when every field operation is inlined into every point operation the hot
+// loop no longer fits the instruction cache.  UF_FIELD_FN / UF_POINT_FN mark
+// the field multiply/square and the point double/add as out-of-line
+// subroutines in device code when the translation unit asks for it
+// (UF_NOINLINE_FIELD / UF_NOINLINE_POINT); UF_COLD marks large routines that
+// run once or twice per signature (inversion, square root) out of line always.
+#if defined(__CUDACC__)
+#define UF_NOINL __host__ __device__ __noinline__
+#define UF_COLD static UF_NOINL
+#if defined(UF_NOINLINE_FIELD)
+#define UF_FIELD_FN static UF_NOINL
+#else
+#define UF_FIELD_FN UF_HD
+#endif
+#if defined(UF_NOINLINE_POINT)
+#define UF_POINT_FN static UF_NOINL
+#else
+#define UF_POINT_FN UF_HD
+#endif
+#else
+#define UF_COLD static inline
+#define UF_FIELD_FN static inline
+#define UF_POINT_FN static inline
+#endif
+
 #if defined(__CUDA_ARCH__)
 #define UF_UNROLL _Pragma("unroll")
 #define UF_NOUNROLL _Pragma("unroll 1")

@@ -143,7 +143,7 @@ UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& 
     UF_NOUNROLL
     for (int i = kNWP - 1; i >= 0; --i) {
         if (i != kNWP - 1) {
-            UF_UNROLL
+            UF_NOUNROLL
             for (int j = 0; j < kWP; ++j) jac_dbl(R);
         }
         add_ptab(R, tab, dp1[i], sb.neg1, false, beta);

@@ -184,17 +184,26 @@ UF_HD void sqr256(uint32_t t[16], const uint32_t a[8]) {
     }
 }
 
-UF_HD void fe_mul(Fe& r, const Fe& a, const Fe& b) {
+// By-value cores, so that an out-of-line build (UF_NOINLINE_FIELD) passes
+// operands in registers rather than through the stack.
+UF_FIELD_FN Fe fe_mul_v(Fe a, Fe b) {
     uint32_t t[16];
+    Fe r;
     mul256(t, a.v, b.v);
     fe_reduce512(r, t);
+    return r;
 }
 
-UF_HD void fe_sqr(Fe& r, const Fe& a) {
+UF_FIELD_FN Fe fe_sqr_v(Fe a) {
     uint32_t t[16];
+    Fe r;
     sqr256(t, a.v);
     fe_reduce512(r, t);
+    return r;
 }
+
+UF_HD void fe_mul(Fe& r, const Fe& a, const Fe& b) { r = fe_mul_v(a, b); }
+UF_HD void fe_sqr(Fe& r, const Fe& a) { r = fe_sqr_v(a); }
 
 // r = a * m for a small m (< 2^22).
 UF_HD void fe_mul_small(Fe& r, const Fe& a, uint32_t m) {
@@ -264,7 +273,7 @@ UF_HD void fe_sqr_n(Fe& r, const Fe& a, int n) {
 // a^((p+1)/4): the square root when a is a square.  (p+1)/4 is, from the top,
 // 223 one-bits, a zero, 22 ones, four zeros, two ones, two zeros; the chain
 // builds x^(2^k - 1) blocks (253 squarings, 13 multiplications).
-UF_HDI void fe_sqrt_candidate(Fe& r, const Fe& a) {
+UF_COLD void fe_sqrt_candidate(Fe& r, const Fe& a) {
     Fe x2, x3, x6, x9, x11, x22, x44, x88, x176, x220, x223, t;
     fe_sqr(t, a);        fe_mul(x2, t, a);
     fe_sqr(t, x2);       fe_mul(x3, t, a);

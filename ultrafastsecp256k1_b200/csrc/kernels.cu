@@ -1,17 +1,6 @@
-// sm_100a kernels of the verify path.
-//
-// Per-signature verify (the plain form, one signature per thread): the
-// reference's ecdsa_verify_batch_kernel / schnorr_verify_batch_kernel
-// (src/cuda/src/secp256k1.cu:153, :232) re-designed for B200 -- see ecmult.cuh
-// for the scalar-multiplication design.  Memory layout per block:
-//   * dynamic shared memory holds each thread's 1P..8P table as
-//     [entry][quad][thread] uint4 (4 x 16 B per entry and coordinate pair), so a
-//     warp's data-dependent table reads are bank-conflict free (each thread owns
-//     its own bank column);
-//   * the 1..128 multiples of G and lambda*G (16 KB) stay in global memory and
-//     are read through the read-only L1 path;
-//   * Booth digits live in a small per-thread local array indexed uniformly
-//     across the warp (coalesced, L1 resident).
+// Support kernels of the verify path: generator-table set-up, the arithmetic
+// probes used by the tests, and the IMAD issue-rate probe.  The verify kernels
+// themselves are in kernels_verify.cu.
 #include "kernels.h"
 #include "verify.cuh"
 #include "dev_tables.cuh"
@@ -47,71 +36,6 @@ __global__ void k_gtable_init(uint4* out) {
 cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s) {
     k_gtable_init<<<1, 256, 0, s>>>(reinterpret_cast<uint4*>(d_gtab));
     return cudaGetLastError();
-}
-
-// ------------------------------------------------------------ plain verify --
-template <bool kEcdsa>
-__global__ void __launch_bounds__(kVerifyThreads)
-k_verify(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs, const uint8_t* __restrict__ sigs,
-         uint32_t n, const uint4* __restrict__ gt, uint8_t* __restrict__ out, int collect) {
-    extern __shared__ uint4 smem_tab[];
-    const SmemTab tab{smem_tab + threadIdx.x, blockDim.x};
-    const GlobalGT g{gt};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t mw[8], sw[16];
-        load_words8(mw, msgs + 32ull * i);
-        load_words8(sw, sigs + 64ull * i);
-        load_words8(sw + 8, sigs + 64ull * i + 32);
-        bool ok;
-        if (kEcdsa) {
-            ok = ecdsa_verify_one(mw, pubs + 33ull * i, sw, tab, g);
-        } else {
-            uint32_t pw[8];
-            load_words8(pw, pubs + 32ull * i);
-            ok = schnorr_verify_one(mw, pw, sw, tab, g);
-        }
-        if (collect) {
-            if (ok) out[i] = 0;
-        } else {
-            out[i] = ok ? 1 : 0;
-        }
-    }
-}
-
-template <bool kEcdsa>
-static cudaError_t launch_verify(const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs, uint32_t n,
-                                 const void* d_gtab, uint8_t* out, int collect, int grid, cudaStream_t s) {
-    if (n == 0) return cudaSuccess;
-    // the shared-memory opt-in was set per device by verify_blocks_per_sm() at context creation
-    const size_t smem = kVerifyThreads * kVerifySmemPerThread;
-    const int need = (int)((n + kVerifyThreads - 1) / kVerifyThreads);
-    if (grid <= 0 || grid > need) grid = need;
-    k_verify<kEcdsa><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, reinterpret_cast<const uint4*>(d_gtab),
-                                                        out, collect);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_ecdsa_verify(const uint8_t* msgs, const uint8_t* pubs33, const uint8_t* sigs, uint32_t n,
-                                const void* d_gtab, uint8_t* out, int collect, int grid, cudaStream_t s) {
-    return launch_verify<true>(msgs, pubs33, sigs, n, d_gtab, out, collect, grid, s);
-}
-
-cudaError_t launch_schnorr_verify(const uint8_t* msgs, const uint8_t* xonly32, const uint8_t* sigs, uint32_t n,
-                                  const void* d_gtab, uint8_t* out, int collect, int grid, cudaStream_t s) {
-    return launch_verify<false>(msgs, xonly32, sigs, n, d_gtab, out, collect, grid, s);
-}
-
-int verify_blocks_per_sm(int kind) {
-    int blocks = 0;
-    const size_t smem = kVerifyThreads * kVerifySmemPerThread;
-    if (kind == 0) {
-        cudaFuncSetAttribute(k_verify<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_verify<true>, kVerifyThreads, smem);
-    } else {
-        cudaFuncSetAttribute(k_verify<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_verify<false>, kVerifyThreads, smem);
-    }
-    return blocks;
 }
 
 // ---------------------------------------------------------- diagnostics --

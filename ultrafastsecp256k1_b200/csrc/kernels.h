@@ -17,25 +17,34 @@ constexpr size_t kVerifySmemPerThread = 8 * 64;
 
 cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s);
 
-// One signature per thread, grid-stride.  Inputs: msgs 32 B, pubs 33 B
-// (ECDSA, SEC1 compressed) or 32 B (BIP-340 x-only), sigs 64 B, all
+// One signature per thread, grid-stride.  kind 0 = ECDSA (pubs: 33-byte SEC1
+// compressed), 1 = BIP-340 (pubs: 32-byte x-only).  msgs 32 B, sigs 64 B, all
 // contiguous; msgs / x-only pubs / sigs must be 16-byte aligned.  out[i] = 1
 // for a valid signature, 0 otherwise.  With collect != 0 a valid signature
-// writes 0 and an invalid one leaves out[i] untouched.
-cudaError_t launch_ecdsa_verify(const uint8_t* msgs, const uint8_t* pubs33, const uint8_t* sigs,
-                                uint32_t n, const void* d_gtab, uint8_t* out, int collect,
-                                int grid, cudaStream_t s);
-cudaError_t launch_schnorr_verify(const uint8_t* msgs, const uint8_t* xonly32, const uint8_t* sigs,
-                                  uint32_t n, const void* d_gtab, uint8_t* out, int collect,
-                                  int grid, cudaStream_t s);
+// writes 0 and an invalid one leaves out[i] untouched.  Variants 0..3 are the
+// same kernel built with different code-size choices (kernels_verify.cu).
+constexpr int kVerifyVariants = 4;
+typedef cudaError_t (*verify_launcher)(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs,
+                                       uint32_t n, const void* d_gtab, uint8_t* out, int collect, int grid,
+                                       cudaStream_t s);
+typedef int (*verify_occupancy_fn)(int kind);
+cudaError_t launch_verify_v0(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
+cudaError_t launch_verify_v1(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
+cudaError_t launch_verify_v2(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
+cudaError_t launch_verify_v3(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
+int verify_occupancy_v0(int kind);
+int verify_occupancy_v1(int kind);
+int verify_occupancy_v2(int kind);
+int verify_occupancy_v3(int kind);
 
 // Batch signer (workload generator): kind 0 = ECDSA (pubs 33 B), 1 = BIP-340
 // (pubs 32 B x-only, auxs 32 B aux_rand).  ok[i] = 0 for an invalid key.
 cudaError_t launch_sign(int kind, const uint8_t* msgs, const uint8_t* sks, const uint8_t* auxs, uint32_t n,
                         const void* d_gtab, uint8_t* pubs, uint8_t* sigs, uint8_t* ok, int grid, cudaStream_t s);
-
-// Blocks per SM the verify kernels reach (occupancy query).
-int verify_blocks_per_sm(int kind);
 
 // Building-block probes for the tests (op codes in ufsecp_gpu_ext.h).
 cudaError_t launch_diag(uint32_t op, const uint8_t* in, uint32_t n, uint8_t* out,

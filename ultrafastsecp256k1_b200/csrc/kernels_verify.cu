@@ -1,0 +1,91 @@
+// Per-signature verify kernels (the plain form: one signature per thread).
+//
+// The reference's ecdsa_verify_batch_kernel / schnorr_verify_batch_kernel
+// (src/cuda/src/secp256k1.cu:153, :232) re-designed for B200; ecmult.cuh has the
+// scalar-multiplication design.  Memory layout per block:
+//   * dynamic shared memory holds each thread's 1P..8P table as
+//     [entry][quad][thread] uint4, so a warp's data-dependent table reads are
+//     bank-conflict free (each thread owns its own bank column);
+//   * the 1..128 multiples of G and lambda*G (16 KB) stay in global memory and
+//     are read through the read-only L1 path;
+//   * Booth digits live in a small per-thread local array indexed uniformly
+//     across the warp (coalesced, L1 resident).
+//
+// This file is compiled several times (UF_VARIANT 0..3) with different
+// code-size choices (UF_NOINLINE_POINT / UF_NOINLINE_FIELD, see common.cuh);
+// the backend picks a variant per signature kind (tuned per device).
+#include "kernels.h"
+#include "verify.cuh"
+#include "dev_tables.cuh"
+
+#ifndef UF_VARIANT
+#define UF_VARIANT 0
+#endif
+#define UF_CAT2(a, b) a##b
+#define UF_CAT(a, b) UF_CAT2(a, b)
+
+namespace uf {
+namespace UF_CAT(vk, UF_VARIANT) {
+
+template <bool kEcdsa>
+__global__ void __launch_bounds__(kVerifyThreads)
+k_verify(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs, const uint8_t* __restrict__ sigs,
+         uint32_t n, const uint4* __restrict__ gt, uint8_t* __restrict__ out, int collect) {
+    extern __shared__ uint4 smem_tab[];
+    const SmemTab tab{smem_tab + threadIdx.x, blockDim.x};
+    const GlobalGT g{gt};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t mw[8], sw[16];
+        load_words8(mw, msgs + 32ull * i);
+        load_words8(sw, sigs + 64ull * i);
+        load_words8(sw + 8, sigs + 64ull * i + 32);
+        bool ok;
+        if (kEcdsa) {
+            ok = ecdsa_verify_one(mw, pubs + 33ull * i, sw, tab, g);
+        } else {
+            uint32_t pw[8];
+            load_words8(pw, pubs + 32ull * i);
+            ok = schnorr_verify_one(mw, pw, sw, tab, g);
+        }
+        if (collect) {
+            if (ok) out[i] = 0;
+        } else {
+            out[i] = ok ? 1 : 0;
+        }
+    }
+}
+
+}  // namespace vkN
+
+cudaError_t UF_CAT(launch_verify_v, UF_VARIANT)(int kind, const uint8_t* msgs, const uint8_t* pubs,
+                                                const uint8_t* sigs, uint32_t n, const void* d_gtab, uint8_t* out,
+                                                int collect, int grid, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    // the shared-memory opt-in was set per device by verify_occupancy_v*() at context creation
+    const size_t smem = kVerifyThreads * kVerifySmemPerThread;
+    const int need = (int)((n + kVerifyThreads - 1) / kVerifyThreads);
+    if (grid <= 0 || grid > need) grid = need;
+    const uint4* gt = reinterpret_cast<const uint4*>(d_gtab);
+    if (kind == 0)
+        UF_CAT(vk, UF_VARIANT)::k_verify<true><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+    else
+        UF_CAT(vk, UF_VARIANT)::k_verify<false><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+    return cudaGetLastError();
+}
+
+int UF_CAT(verify_occupancy_v, UF_VARIANT)(int kind) {
+    int blocks = 0;
+    const size_t smem = kVerifyThreads * kVerifySmemPerThread;
+    if (kind == 0) {
+        auto f = UF_CAT(vk, UF_VARIANT)::k_verify<true>;
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, kVerifyThreads, smem);
+    } else {
+        auto f = UF_CAT(vk, UF_VARIANT)::k_verify<false>;
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, kVerifyThreads, smem);
+    }
+    return blocks;
+}
+
+}  // namespace uf

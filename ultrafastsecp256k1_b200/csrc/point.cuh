@@ -27,8 +27,8 @@ UF_HD void jac_from_aff(Jac& a, const Fe& x, const Fe& y) {
 }
 
 // dbl-2009-l.  Y = 0 cannot occur on secp256k1 (no 2-torsion).
-UF_HD void jac_dbl(Jac& a) {
-    if (a.inf) return;
+UF_POINT_FN Jac jac_dbl_v(Jac a) {
+    if (a.inf) return a;
     Fe A, B, C, D, E, t;
     fe_mul(t, a.Y, a.Z);
     fe_dbl(a.Z, t);             // Z3 = 2 Y Z
@@ -51,11 +51,14 @@ UF_HD void jac_dbl(Jac& a) {
     fe_dbl(C, C);
     fe_dbl(C, C);
     fe_sub(a.Y, a.Y, C);        // Y3 = E (D - X3) - 8C
+    return a;
 }
 
+UF_HD void jac_dbl(Jac& a) { a = jac_dbl_v(a); }
+
 // a += (x2, y2) affine (madd-2007-bl), exact in all cases.
-UF_HD void jac_add_aff(Jac& a, const Fe& x2, const Fe& y2) {
-    if (a.inf) { jac_from_aff(a, x2, y2); return; }
+UF_POINT_FN Jac jac_add_aff_v(Jac a, Fe x2, Fe y2) {
+    if (a.inf) { jac_from_aff(a, x2, y2); return a; }
     Fe Z1Z1, U2, S2, H, r, t;
     fe_sqr(Z1Z1, a.Z);
     fe_mul(U2, x2, Z1Z1);
@@ -66,7 +69,7 @@ UF_HD void jac_add_aff(Jac& a, const Fe& x2, const Fe& y2) {
     if (fe_is_zero(H)) {
         if (fe_is_zero(r)) jac_dbl(a);      // same point
         else a.inf = true;                  // opposite points
-        return;
+        return a;
     }
     Fe HH, I, J, V;
     fe_sqr(HH, H);
@@ -91,7 +94,10 @@ UF_HD void jac_add_aff(Jac& a, const Fe& x2, const Fe& y2) {
     fe_mul(J, a.Y, J);
     fe_dbl(J, J);
     fe_sub(a.Y, t, J);
+    return a;
 }
+
+UF_HD void jac_add_aff(Jac& a, const Fe& x2, const Fe& y2) { a = jac_add_aff_v(a, x2, y2); }
 
 // General Jacobian + Jacobian (used off the hot path: table set-up, tests).
 UF_HDI void jac_add(Jac& a, const Jac& b) {

@@ -190,7 +190,7 @@ UF_HD void from_s30_mod(uint32_t out[8], const int32_t in[9], bool negate, const
 }
 
 // out = x^-1 mod M for 0 < x < M (x = 0 gives 0).
-UF_HDI void modinv_var(uint32_t out[8], const uint32_t x[8], const ModInfo& mi) {
+UF_COLD void modinv_var(uint32_t out[8], const uint32_t x[8], const ModInfo& mi) {
     int32_t f[9], g[9], d[9], e[9], T[4];
     UF_UNROLL
     for (int i = 0; i < 9; ++i) { f[i] = mi.m30[i]; d[i] = 0; e[i] = 0; }

@@ -276,3 +276,25 @@ def test_abi_gating_with_context(gpu_ctx):
     assert gpu_ctx.is_ready()
     info = uf.device_info(0)
     assert info.compute_units > 0 and info.global_mem_bytes > 0
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_every_kernel_variant_matches_oracle(gpu_ctx, oracle, variant):
+    """The code-size variants (ufsecp_gpu_ext_set_variant) compute identical verdicts."""
+    _, wy, e = load_golden()
+    m, p, s = ecdsa_corpus(oracle, 700, seed=60 + variant, tamper=0.2)
+    mx, x, sx = schnorr_corpus(oracle, 700, seed=70 + variant, tamper=0.2)
+    old = (gpu_ctx.get_variant(0)[0], gpu_ctx.get_variant(1)[0])
+    try:
+        gpu_ctx.set_variant(0, variant)
+        gpu_ctx.set_variant(1, variant)
+        assert (gpu_ctx.ecdsa_verify_batch(m, p, s) == oracle.ecdsa_verify_batch(m, p, s)).all()
+        assert (gpu_ctx.schnorr_verify_batch(mx, x, sx) == oracle.schnorr_verify_batch(mx, x, sx)).all()
+        assert (gpu_ctx.ecdsa_verify_batch(wy["msgs"], wy["pubs"], wy["sigs"]) == wy["ref_valid"]).all()
+        assert (gpu_ctx.ecdsa_verify_batch(e["ecdsa_msgs"], e["ecdsa_pubs"], e["ecdsa_sigs"])
+                == e["ecdsa_ref_valid"]).all()
+        assert (gpu_ctx.schnorr_verify_batch(e["schnorr_msgs"], e["schnorr_pubs"], e["schnorr_sigs"])
+                == e["schnorr_ref_valid"]).all()
+    finally:
+        gpu_ctx.set_variant(0, old[0])
+        gpu_ctx.set_variant(1, old[1])

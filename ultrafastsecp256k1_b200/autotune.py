@@ -25,7 +25,7 @@ import numpy as np
 import ultrafastsecp256k1_b200 as uf
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
-VARIANTS = 4
+VARIANTS = 6
 
 
 def tuning_path(name: str, sms: int) -> str:

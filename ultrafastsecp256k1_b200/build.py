@@ -43,6 +43,8 @@ VARIANTS = {
         ("v1", ["-DUF_VARIANT=1", "-DUF_NOINLINE_POINT"]),
         ("v2", ["-DUF_VARIANT=2", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD"]),
         ("v3", ["-DUF_VARIANT=3", "-DUF_NOINLINE_FIELD"]),
+        ("v4", ["-DUF_VARIANT=4", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]),
+        ("v5", ["-DUF_VARIANT=5", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]),
     ],
 }
 

@@ -17,9 +17,10 @@ namespace {
 constexpr size_t kChunk = size_t{1} << 22;
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
-                                                     launch_verify_v3};
+                                                     launch_verify_v3, launch_verify_v4, launch_verify_v5};
 const verify_occupancy_fn kOccupancy[kVerifyVariants] = {verify_occupancy_v0, verify_occupancy_v1,
-                                                         verify_occupancy_v2, verify_occupancy_v3};
+                                                         verify_occupancy_v2, verify_occupancy_v3,
+                                                         verify_occupancy_v4, verify_occupancy_v5};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);

@@ -73,8 +73,8 @@ private:
     int dev_ = -1;
     int sms_ = 0;
     std::string dev_name_;
-    int grid_[4][2] = {};        // [variant][kind] resident-grid size
-    int variant_[2] = {1, 1};    // chosen variant per kind
+    int grid_[6][2] = {};        // [variant][kind] resident-grid size
+    int variant_[2] = {2, 2};    // chosen variant per kind (2: out-of-line field and point ops)
     cudaError_t launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
                               uint8_t* out, int collect, cudaStream_t st);
     void load_tuning();

@@ -12,6 +12,7 @@
 //  * add/sub fold their carry/borrow with K as well (at most twice).
 #pragma once
 #include "common.cuh"
+#include "fe_ptx.cuh"
 
 namespace uf {
 
@@ -95,21 +96,10 @@ UF_HD void fe_neg(Fe& r, const Fe& a) {
 
 UF_HD void fe_dbl(Fe& r, const Fe& a) { fe_add(r, a, a); }
 
-// Reduce a 512-bit product t[0..15] to a weakly reduced field element.
-UF_HD void fe_reduce512(Fe& r, const uint32_t t[16]) {
-    uint32_t s[8];
-    uint64_t c = (uint64_t)t[8] * 977u + t[0];
-    s[0] = lo32(c);
-    c >>= 32;
-    UF_UNROLL
-    for (int j = 1; j < 8; ++j) {
-        c += (uint64_t)t[8 + j] * 977u + t[j] + t[7 + j];
-        s[j] = lo32(c);
-        c >>= 32;
-    }
-    const uint64_t s8 = c + t[15];          // < 2^45: weight 2^256
+// s[0..7] + top * 2^256 (top < 2^45) -> weakly reduced r (second, small fold).
+UF_HD void fe_fold_top(Fe& r, uint32_t s[8], uint64_t s8) {
     const uint64_t m = s8 * 977u;           // < 2^55
-    c = (uint64_t)s[0] + lo32(m);
+    uint64_t c = (uint64_t)s[0] + lo32(m);
     s[0] = lo32(c);
     c >>= 32;
     c += (uint64_t)s[1] + hi32(m) + lo32(s8);
@@ -127,6 +117,26 @@ UF_HD void fe_reduce512(Fe& r, const uint32_t t[16]) {
     fe_add_k(s, (uint32_t)c);
     UF_UNROLL
     for (int j = 0; j < 8; ++j) r.v[j] = s[j];
+}
+
+// Reduce a 512-bit product t[0..15] to a weakly reduced field element.
+UF_HD void fe_reduce512(Fe& r, const uint32_t t[16]) {
+    uint32_t s[8];
+#if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
+    const uint64_t s8 = fold_977_ptx(s, t);
+#else
+    uint64_t c = (uint64_t)t[8] * 977u + t[0];
+    s[0] = lo32(c);
+    c >>= 32;
+    UF_UNROLL
+    for (int j = 1; j < 8; ++j) {
+        c += (uint64_t)t[8 + j] * 977u + t[j] + t[7 + j];
+        s[j] = lo32(c);
+        c >>= 32;
+    }
+    const uint64_t s8 = c + t[15];          // < 2^45: weight 2^256
+#endif
+    fe_fold_top(r, s, s8);
 }
 
 // 256x256 -> 512 schoolbook product (operand scanning, 64-bit accumulators:
@@ -186,10 +196,16 @@ UF_HD void sqr256(uint32_t t[16], const uint32_t a[8]) {
 
 // By-value cores, so that an out-of-line build (UF_NOINLINE_FIELD) passes
 // operands in registers rather than through the stack.
+// UF_PTX_MUL selects the PTX carry-chain product of fe_ptx.cuh on the device
+// (the square then uses the same full product).
 UF_FIELD_FN Fe fe_mul_v(Fe a, Fe b) {
     uint32_t t[16];
     Fe r;
+#if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
+    mul256_ptx(t, a.v, b.v);
+#else
     mul256(t, a.v, b.v);
+#endif
     fe_reduce512(r, t);
     return r;
 }
@@ -197,7 +213,11 @@ UF_FIELD_FN Fe fe_mul_v(Fe a, Fe b) {
 UF_FIELD_FN Fe fe_sqr_v(Fe a) {
     uint32_t t[16];
     Fe r;
+#if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
+    mul256_ptx(t, a.v, a.v);
+#else
     sqr256(t, a.v);
+#endif
     fe_reduce512(r, t);
     return r;
 }

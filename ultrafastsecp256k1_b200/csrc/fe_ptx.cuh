@@ -1,0 +1,119 @@
+// 256 x 256 -> 512-bit product with PTX carry chains (device only).
+//
+// Operand scanning, one row per limb b[i] of the multiplier.  Within a row the
+// products a[j]*b[i] are split by the parity of j, because lo(a[j] b[i]) lands
+// on limb i+j and hi(a[j] b[i]) on i+j+1: the even products (j = 0,2,4,6) then
+// touch limbs i..i+7 exactly once each and form ONE unbroken carry chain
+//   mad.lo.cc, madc.hi.cc, madc.lo.cc, ..., madc.hi.cc, addc
+// and the odd products (j = 1,3,5,7) form a second chain over limbs i+1..i+8.
+// That is 16 multiply-adds and 1 add per row, 8 rows.  Carry bounds: after
+// rows 0..i the accumulator holds a * (b mod 2^(32(i+1))) < 2^(32(i+9)), so
+// limb i+8 is zero before row i's even chain deposits its carry there, and the
+// odd chain of row i never carries out of limb i+8.
+//
+// The reference's GPU field multiply is also an 8x32 mad.lo.cc / madc.hi.cc
+// product (src/cuda/include/secp256k1_32_hybrid_final.cuh:15-103, a column-wise
+// Comba arrangement); this is the row-wise even/odd arrangement instead.
+#pragma once
+#include "common.cuh"
+
+#if defined(__CUDA_ARCH__)
+namespace uf {
+
+#define UF_ROW_EVEN(T0, T1, T2, T3, T4, T5, T6, T7, T8, BI)                                      \
+    asm("mad.lo.cc.u32 %0, %9, %13, %0;\n\t"                                                     \
+        "madc.hi.cc.u32 %1, %9, %13, %1;\n\t"                                                    \
+        "madc.lo.cc.u32 %2, %10, %13, %2;\n\t"                                                   \
+        "madc.hi.cc.u32 %3, %10, %13, %3;\n\t"                                                   \
+        "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"                                                   \
+        "madc.hi.cc.u32 %5, %11, %13, %5;\n\t"                                                   \
+        "madc.lo.cc.u32 %6, %12, %13, %6;\n\t"                                                   \
+        "madc.hi.cc.u32 %7, %12, %13, %7;\n\t"                                                   \
+        "addc.u32 %8, %8, 0;"                                                                    \
+        : "+r"(T0), "+r"(T1), "+r"(T2), "+r"(T3), "+r"(T4), "+r"(T5), "+r"(T6), "+r"(T7), "+r"(T8) \
+        : "r"(a[0]), "r"(a[2]), "r"(a[4]), "r"(a[6]), "r"(BI))
+
+#define UF_ROW_ODD(T1, T2, T3, T4, T5, T6, T7, T8, BI)                                           \
+    asm("mad.lo.cc.u32 %0, %8, %12, %0;\n\t"                                                     \
+        "madc.hi.cc.u32 %1, %8, %12, %1;\n\t"                                                    \
+        "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                    \
+        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                    \
+        "madc.lo.cc.u32 %4, %10, %12, %4;\n\t"                                                   \
+        "madc.hi.cc.u32 %5, %10, %12, %5;\n\t"                                                   \
+        "madc.lo.cc.u32 %6, %11, %12, %6;\n\t"                                                   \
+        "madc.hi.u32 %7, %11, %12, %7;"                                                          \
+        : "+r"(T1), "+r"(T2), "+r"(T3), "+r"(T4), "+r"(T5), "+r"(T6), "+r"(T7), "+r"(T8)          \
+        : "r"(a[1]), "r"(a[3]), "r"(a[5]), "r"(a[7]), "r"(BI))
+
+__device__ __forceinline__ void mul256_ptx(uint32_t t[16], const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0, t9 = 0, t10 = 0, t11 = 0,
+             t12 = 0, t13 = 0, t14 = 0, t15 = 0;
+    UF_ROW_EVEN(t0, t1, t2, t3, t4, t5, t6, t7, t8, b[0]);
+    UF_ROW_ODD(t1, t2, t3, t4, t5, t6, t7, t8, b[0]);
+    UF_ROW_EVEN(t1, t2, t3, t4, t5, t6, t7, t8, t9, b[1]);
+    UF_ROW_ODD(t2, t3, t4, t5, t6, t7, t8, t9, b[1]);
+    UF_ROW_EVEN(t2, t3, t4, t5, t6, t7, t8, t9, t10, b[2]);
+    UF_ROW_ODD(t3, t4, t5, t6, t7, t8, t9, t10, b[2]);
+    UF_ROW_EVEN(t3, t4, t5, t6, t7, t8, t9, t10, t11, b[3]);
+    UF_ROW_ODD(t4, t5, t6, t7, t8, t9, t10, t11, b[3]);
+    UF_ROW_EVEN(t4, t5, t6, t7, t8, t9, t10, t11, t12, b[4]);
+    UF_ROW_ODD(t5, t6, t7, t8, t9, t10, t11, t12, b[4]);
+    UF_ROW_EVEN(t5, t6, t7, t8, t9, t10, t11, t12, t13, b[5]);
+    UF_ROW_ODD(t6, t7, t8, t9, t10, t11, t12, t13, b[5]);
+    UF_ROW_EVEN(t6, t7, t8, t9, t10, t11, t12, t13, t14, b[6]);
+    UF_ROW_ODD(t7, t8, t9, t10, t11, t12, t13, t14, b[6]);
+    UF_ROW_EVEN(t7, t8, t9, t10, t11, t12, t13, t14, t15, b[7]);
+    UF_ROW_ODD(t8, t9, t10, t11, t12, t13, t14, t15, b[7]);
+    t[0] = t0; t[1] = t1; t[2] = t2; t[3] = t3; t[4] = t4; t[5] = t5; t[6] = t6; t[7] = t7;
+    t[8] = t8; t[9] = t9; t[10] = t10; t[11] = t11; t[12] = t12; t[13] = t13; t[14] = t14; t[15] = t15;
+}
+
+#undef UF_ROW_EVEN
+#undef UF_ROW_ODD
+
+// First fold of the reduction mod p for the 512-bit t = H*2^256 + L:
+// s[0..7] + top*2^256 = L + 977*H + (H << 32), with top < 2^32 + 978.
+// Order matters for the carry bounds: L + 977*H < 2^266 fits limbs 0..8, then
+// adding H << 32 can carry once more into a 33rd top bit.
+__device__ __forceinline__ uint64_t fold_977_ptx(uint32_t s[8], const uint32_t t[16]) {
+    uint32_t s0 = t[0], s1 = t[1], s2 = t[2], s3 = t[3], s4 = t[4], s5 = t[5], s6 = t[6], s7 = t[7], s8 = 0, s9;
+    // + 977*H, even then odd limbs of H (each one carry chain)
+    asm("mad.lo.cc.u32 %0, %9, 977, %0;\n\t"
+        "madc.hi.cc.u32 %1, %9, 977, %1;\n\t"
+        "madc.lo.cc.u32 %2, %10, 977, %2;\n\t"
+        "madc.hi.cc.u32 %3, %10, 977, %3;\n\t"
+        "madc.lo.cc.u32 %4, %11, 977, %4;\n\t"
+        "madc.hi.cc.u32 %5, %11, 977, %5;\n\t"
+        "madc.lo.cc.u32 %6, %12, 977, %6;\n\t"
+        "madc.hi.cc.u32 %7, %12, 977, %7;\n\t"
+        "addc.u32 %8, %8, 0;"
+        : "+r"(s0), "+r"(s1), "+r"(s2), "+r"(s3), "+r"(s4), "+r"(s5), "+r"(s6), "+r"(s7), "+r"(s8)
+        : "r"(t[8]), "r"(t[10]), "r"(t[12]), "r"(t[14]));
+    asm("mad.lo.cc.u32 %0, %8, 977, %0;\n\t"
+        "madc.hi.cc.u32 %1, %8, 977, %1;\n\t"
+        "madc.lo.cc.u32 %2, %9, 977, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, 977, %3;\n\t"
+        "madc.lo.cc.u32 %4, %10, 977, %4;\n\t"
+        "madc.hi.cc.u32 %5, %10, 977, %5;\n\t"
+        "madc.lo.cc.u32 %6, %11, 977, %6;\n\t"
+        "madc.hi.u32 %7, %11, 977, %7;"
+        : "+r"(s1), "+r"(s2), "+r"(s3), "+r"(s4), "+r"(s5), "+r"(s6), "+r"(s7), "+r"(s8)
+        : "r"(t[9]), "r"(t[11]), "r"(t[13]), "r"(t[15]));
+    // + (H << 32)
+    asm("add.cc.u32 %0, %0, %9;\n\t"
+        "addc.cc.u32 %1, %1, %10;\n\t"
+        "addc.cc.u32 %2, %2, %11;\n\t"
+        "addc.cc.u32 %3, %3, %12;\n\t"
+        "addc.cc.u32 %4, %4, %13;\n\t"
+        "addc.cc.u32 %5, %5, %14;\n\t"
+        "addc.cc.u32 %6, %6, %15;\n\t"
+        "addc.cc.u32 %7, %7, %16;\n\t"
+        "addc.u32 %8, 0, 0;"
+        : "+r"(s1), "+r"(s2), "+r"(s3), "+r"(s4), "+r"(s5), "+r"(s6), "+r"(s7), "+r"(s8), "=r"(s9)
+        : "r"(t[8]), "r"(t[9]), "r"(t[10]), "r"(t[11]), "r"(t[12]), "r"(t[13]), "r"(t[14]), "r"(t[15]));
+    s[0] = s0; s[1] = s1; s[2] = s2; s[3] = s3; s[4] = s4; s[5] = s5; s[6] = s6; s[7] = s7;
+    return ((uint64_t)s9 << 32) | s8;
+}
+
+}  // namespace uf
+#endif

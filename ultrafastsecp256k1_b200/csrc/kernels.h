@@ -21,9 +21,9 @@ cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s);
 // compressed), 1 = BIP-340 (pubs: 32-byte x-only).  msgs 32 B, sigs 64 B, all
 // contiguous; msgs / x-only pubs / sigs must be 16-byte aligned.  out[i] = 1
 // for a valid signature, 0 otherwise.  With collect != 0 a valid signature
-// writes 0 and an invalid one leaves out[i] untouched.  Variants 0..3 are the
+// writes 0 and an invalid one leaves out[i] untouched.  Variants 0..5 are the
 // same kernel built with different code-size choices (kernels_verify.cu).
-constexpr int kVerifyVariants = 4;
+constexpr int kVerifyVariants = 6;
 typedef cudaError_t (*verify_launcher)(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs,
                                        uint32_t n, const void* d_gtab, uint8_t* out, int collect, int grid,
                                        cudaStream_t s);
@@ -36,10 +36,16 @@ cudaError_t launch_verify_v2(int, const uint8_t*, const uint8_t*, const uint8_t*
                              int, int, cudaStream_t);
 cudaError_t launch_verify_v3(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
                              int, int, cudaStream_t);
+cudaError_t launch_verify_v4(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
+cudaError_t launch_verify_v5(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
 int verify_occupancy_v0(int kind);
 int verify_occupancy_v1(int kind);
 int verify_occupancy_v2(int kind);
 int verify_occupancy_v3(int kind);
+int verify_occupancy_v4(int kind);
+int verify_occupancy_v5(int kind);
 
 // Batch signer (workload generator): kind 0 = ECDSA (pubs 33 B), 1 = BIP-340
 // (pubs 32 B x-only, auxs 32 B aux_rand).  ok[i] = 0 for an invalid key.

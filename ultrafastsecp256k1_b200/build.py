@@ -36,17 +36,17 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-# kernels_verify.cu is compiled once per code-size variant (see csrc/common.cuh)
-VARIANTS = {
-    "kernels_verify.cu": [
-        ("v0", ["-DUF_VARIANT=0"]),
+# kernels_verify.cu (and its building-block probe) is compiled once per
+# code-size variant (see csrc/common.cuh)
+_VARIANT_FLAGS = [
+    ("v0", ["-DUF_VARIANT=0"]),
         ("v1", ["-DUF_VARIANT=1", "-DUF_NOINLINE_POINT"]),
         ("v2", ["-DUF_VARIANT=2", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD"]),
         ("v3", ["-DUF_VARIANT=3", "-DUF_NOINLINE_FIELD"]),
         ("v4", ["-DUF_VARIANT=4", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]),
         ("v5", ["-DUF_VARIANT=5", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]),
-    ],
-}
+]
+VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS, "kernels_probe.cu": _VARIANT_FLAGS}
 
 
 def _sources():

@@ -291,6 +291,10 @@ int Backend::probe(int op, int blocks, int threads, int iters, float* ms) {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
+    // the probe copy built like the BIP-340 verify kernel's current variant
+    static const probe_launcher kProbes[kVerifyVariants] = {launch_probe_v0, launch_probe_v1, launch_probe_v2,
+                                                            launch_probe_v3, launch_probe_v4, launch_probe_v5};
+    const probe_launcher launch_probe = kProbes[variant_[1]];
     e = launch_probe(op, blocks, threads, 1, (uint32_t*)scratch_.p, stream_);   // warm-up
     if (e == cudaSuccess) {
         cudaEventRecord(a, stream_);

@@ -13,6 +13,7 @@
 #pragma once
 #include "common.cuh"
 #include "fe_ptx.cuh"
+#include "fe_ptx_sqr.cuh"
 
 namespace uf {
 
@@ -65,6 +66,13 @@ UF_HD uint32_t fe_sub_k(uint32_t v[8], uint32_t c) {
 }
 
 UF_HD void fe_add(Fe& r, const Fe& a, const Fe& b) {
+#if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
+    uint32_t tp[8];
+    fe_add_ptx(tp, a.v, b.v);
+    UF_UNROLL
+    for (int i = 0; i < 8; ++i) r.v[i] = tp[i];
+    return;
+#endif
     uint64_t t = 0;
     UF_UNROLL
     for (int i = 0; i < 8; ++i) {
@@ -77,6 +85,13 @@ UF_HD void fe_add(Fe& r, const Fe& a, const Fe& b) {
 }
 
 UF_HD void fe_sub(Fe& r, const Fe& a, const Fe& b) {
+#if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
+    uint32_t tp[8];
+    fe_sub_ptx(tp, a.v, b.v);
+    UF_UNROLL
+    for (int i = 0; i < 8; ++i) r.v[i] = tp[i];
+    return;
+#endif
     uint32_t br = 0;
     UF_UNROLL
     for (int i = 0; i < 8; ++i) {
@@ -196,8 +211,8 @@ UF_HD void sqr256(uint32_t t[16], const uint32_t a[8]) {
 
 // By-value cores, so that an out-of-line build (UF_NOINLINE_FIELD) passes
 // operands in registers rather than through the stack.
-// UF_PTX_MUL selects the PTX carry-chain product of fe_ptx.cuh on the device
-// (the square then uses the same full product).
+// UF_PTX_MUL selects the PTX carry-chain product / square of fe_ptx.cuh and
+// fe_ptx_sqr.cuh on the device (and the PTX add / sub above).
 UF_FIELD_FN Fe fe_mul_v(Fe a, Fe b) {
     uint32_t t[16];
     Fe r;
@@ -214,7 +229,7 @@ UF_FIELD_FN Fe fe_sqr_v(Fe a) {
     uint32_t t[16];
     Fe r;
 #if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
-    mul256_ptx(t, a.v, a.v);
+    sqr256_ptx(t, a.v);
 #else
     sqr256(t, a.v);
 #endif

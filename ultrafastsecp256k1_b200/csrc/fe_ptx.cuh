@@ -115,5 +115,92 @@ __device__ __forceinline__ uint64_t fold_977_ptx(uint32_t s[8], const uint32_t t
     return ((uint64_t)s9 << 32) | s8;
 }
 
+// r = a + b mod p (weakly reduced in and out).  The carry out of the 256-bit
+// add is folded back as +K (K = 2^32 + 977); that fold can itself carry only
+// when the result is below K, which takes a further +K (practically never
+// taken, kept exact behind a branch).
+__device__ __forceinline__ void fe_add_ptx(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t c;
+    asm("add.cc.u32 %0, %9, %17;\n\t"
+        "addc.cc.u32 %1, %10, %18;\n\t"
+        "addc.cc.u32 %2, %11, %19;\n\t"
+        "addc.cc.u32 %3, %12, %20;\n\t"
+        "addc.cc.u32 %4, %13, %21;\n\t"
+        "addc.cc.u32 %5, %14, %22;\n\t"
+        "addc.cc.u32 %6, %15, %23;\n\t"
+        "addc.cc.u32 %7, %16, %24;\n\t"
+        "addc.u32 %8, 0, 0;"
+        : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]), "=&r"(r[7]),
+          "=&r"(c)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+          "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+    asm("mad.lo.cc.u32 %0, %9, 977, %0;\n\t"
+        "addc.cc.u32 %1, %1, %9;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\t"
+        "addc.cc.u32 %3, %3, 0;\n\t"
+        "addc.cc.u32 %4, %4, 0;\n\t"
+        "addc.cc.u32 %5, %5, 0;\n\t"
+        "addc.cc.u32 %6, %6, 0;\n\t"
+        "addc.cc.u32 %7, %7, 0;\n\t"
+        "addc.u32 %8, 0, 0;"
+        : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(c)
+        : "r"(c));
+    if (__builtin_expect(c != 0, 0)) {
+        asm("add.cc.u32 %0, %0, 977;\n\t"
+            "addc.cc.u32 %1, %1, 1;\n\t"
+            "addc.cc.u32 %2, %2, 0;\n\t"
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.cc.u32 %4, %4, 0;\n\t"
+            "addc.cc.u32 %5, %5, 0;\n\t"
+            "addc.cc.u32 %6, %6, 0;\n\t"
+            "addc.u32 %7, %7, 0;"
+            : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+    }
+}
+
+// r = a - b mod p (weakly reduced in and out).  A borrow out of the 256-bit
+// subtraction is folded as -K (adds p); a second borrow, possible only when
+// b > p and a is tiny, takes one more -K behind a branch.
+__device__ __forceinline__ void fe_sub_ptx(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t br;
+    asm("sub.cc.u32 %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32 %8, 0, 0;"
+        : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]), "=&r"(r[7]),
+          "=&r"(br)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+          "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+    // br is 0 or 0xFFFFFFFF; subtract K & br
+    const uint32_t k0 = br & 977u, k1 = br & 1u;
+    asm("sub.cc.u32 %0, %0, %9;\n\t"
+        "subc.cc.u32 %1, %1, %10;\n\t"
+        "subc.cc.u32 %2, %2, 0;\n\t"
+        "subc.cc.u32 %3, %3, 0;\n\t"
+        "subc.cc.u32 %4, %4, 0;\n\t"
+        "subc.cc.u32 %5, %5, 0;\n\t"
+        "subc.cc.u32 %6, %6, 0;\n\t"
+        "subc.cc.u32 %7, %7, 0;\n\t"
+        "subc.u32 %8, 0, 0;"
+        : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(br)
+        : "r"(k0), "r"(k1));
+    if (__builtin_expect(br != 0, 0)) {
+        asm("sub.cc.u32 %0, %0, 977;\n\t"
+            "subc.cc.u32 %1, %1, 1;\n\t"
+            "subc.cc.u32 %2, %2, 0;\n\t"
+            "subc.cc.u32 %3, %3, 0;\n\t"
+            "subc.cc.u32 %4, %4, 0;\n\t"
+            "subc.cc.u32 %5, %5, 0;\n\t"
+            "subc.cc.u32 %6, %6, 0;\n\t"
+            "subc.u32 %7, %7, 0;"
+            : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+    }
+}
+
 }  // namespace uf
 #endif

@@ -60,7 +60,14 @@ cudaError_t launch_diag(uint32_t op, const uint8_t* in, uint32_t n, uint8_t* out
 // 16 independent 32-bit IMADs.  Returns a checksum so the work is not elided.
 cudaError_t launch_imad_peak(uint32_t* d_sink, int blocks, int threads, int iters, cudaStream_t s);
 
-// Building-block throughput probe (op codes in ufsecp_gpu_ext.h).
-cudaError_t launch_probe(int op, int blocks, int threads, int iters, uint32_t* sink, cudaStream_t s);
+// Building-block throughput probe (op codes in ufsecp_gpu_ext.h), one per
+// verify-kernel variant.
+typedef cudaError_t (*probe_launcher)(int op, int blocks, int threads, int iters, uint32_t* sink, cudaStream_t s);
+cudaError_t launch_probe_v0(int, int, int, int, uint32_t*, cudaStream_t);
+cudaError_t launch_probe_v1(int, int, int, int, uint32_t*, cudaStream_t);
+cudaError_t launch_probe_v2(int, int, int, int, uint32_t*, cudaStream_t);
+cudaError_t launch_probe_v3(int, int, int, int, uint32_t*, cudaStream_t);
+cudaError_t launch_probe_v4(int, int, int, int, uint32_t*, cudaStream_t);
+cudaError_t launch_probe_v5(int, int, int, int, uint32_t*, cudaStream_t);
 
 }  // namespace uf

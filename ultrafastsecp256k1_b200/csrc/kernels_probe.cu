@@ -1,4 +1,5 @@
-// Throughput probes of the verify path's building blocks (field mul / sqr,
+// Throughput probes of the verify path's building blocks, one copy per
+// verify-kernel variant (the same field / point code generation) (field mul / sqr,
 // inversions, sqrt, point doubling and mixed add, GLV split, the challenge
 // hash).  Each thread runs `iters` rounds on values held in registers; the
 // host times the launch with CUDA events and reports operations per second,
@@ -6,7 +7,14 @@
 #include "kernels.h"
 #include "verify.cuh"
 
+#ifndef UF_VARIANT
+#define UF_VARIANT 0
+#endif
+#define UF_CAT2(a, b) a##b
+#define UF_CAT(a, b) UF_CAT2(a, b)
+
 namespace uf {
+namespace UF_CAT(pk, UF_VARIANT) {
 
 __device__ __forceinline__ void seed_fe(Fe& a, uint32_t s) {
     for (int i = 0; i < 8; ++i) {
@@ -78,8 +86,12 @@ __global__ void k_probe(int op, int iters, uint32_t* sink) {
     if (acc == 0x9E3779B9u) sink[0] = acc;   // keeps the work observable
 }
 
-cudaError_t launch_probe(int op, int blocks, int threads, int iters, uint32_t* sink, cudaStream_t s) {
-    k_probe<<<blocks, threads, 0, s>>>(op, iters, sink);
+}  // namespace pkN
+
+// Compiled once per verify-kernel variant (same code-size flags), see build.py.
+cudaError_t UF_CAT(launch_probe_v, UF_VARIANT)(int op, int blocks, int threads, int iters, uint32_t* sink,
+                                               cudaStream_t s) {
+    UF_CAT(pk, UF_VARIANT)::k_probe<<<blocks, threads, 0, s>>>(op, iters, sink);
     return cudaGetLastError();
 }
 

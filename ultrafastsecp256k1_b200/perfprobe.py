@@ -1,6 +1,6 @@
 """Building-block throughput on the current GPU.
 
-    python -m ultrafastsecp256k1_b200.perfprobe
+    python -m ultrafastsecp256k1_b200.perfprobe [variant ...]
 
 Prints, per operation of the verify path, the device-wide rate (ops / s) and
 the cost of one operation in field-multiplication equivalents, next to the
@@ -18,11 +18,23 @@ ITERS = {1: 2048, 2: 2048, 3: 16, 4: 4, 5: 512, 6: 512, 7: 16, 8: 64, 9: 128}
 
 
 def main():
+    variants = [int(v) for v in sys.argv[1:]] or [None]
     with uf.GpuContext(0) as ctx:
         props = ctx.device_props()
         sms = props["sm_count"]
         imad = ctx.imad_peak()
-        out = {"sm_count": sms, "imad_ops_per_s": imad, "ops": {}}
+        result = {"sm_count": sms, "imad_ops_per_s": imad, "variants": {}}
+        for variant in variants:
+            if variant is not None:
+                ctx.set_variant(1, variant)
+            result["variants"][str(ctx.get_variant(1)[0])] = measure(ctx, sms, imad)
+        json.dump(result, sys.stdout, indent=1)
+        print()
+
+
+def measure(ctx, sms, imad):
+    if True:
+        out = {"ops": {}}
         mul_rate = None
         for op, (name, per_iter) in OPS.items():
             best = None
@@ -38,8 +50,7 @@ def main():
             out["ops"][name] = {"ops_per_s": rate, "threads": threads, "blocks_per_sm": bps,
                                 "fe_mul_equiv": mul_rate / rate if mul_rate else None,
                                 "imad_per_op_if_bound": imad / rate}
-        json.dump(out, sys.stdout, indent=1)
-        print()
+        return out
 
 
 if __name__ == "__main__":

@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the mixed-batch / RLC / serving sections")
     return ap.parse_args()
 
 
@@ -336,8 +337,11 @@ def run_ours(args):
 
     # ---- secondary: plain ECDSA on 4096 signatures (one launch) -----------
     ecdsa_rate = None
+    mixed = None
     if rank == 0:
         ecdsa_rate = ecdsa_4096_rate(ctx, torch)
+        if not args.no_secondary:
+            mixed = bench_mixed(ctx, torch)
 
     # ---- CPU baseline (rank 0, one GPU only) --------------------------------
     cpu = None
@@ -386,7 +390,7 @@ def run_ours(args):
             "clocks": clocks,
             "gpu_launches": args.steps,
             "verdict_agreement": agree / n,
-            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate},
+            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate, "mixed_batches": mixed},
         }
         print(json.dumps(line))
     del d_msgs, d_xs, d_sigs, d_out
@@ -394,6 +398,95 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def mixed_workload(ctx, torch, n_batches=2000, seed=3, pool=100_000):
+    """Mixed batches: sizes log-uniform in [1, 8192], 70% BIP-340 / 30% ECDSA inside
+    each batch, keys drawn Zipf(s=1.1) from a seeded pool, 0.5% one-bit tampering.
+    Signed on the GPU.  Returns per-batch (kind-split) host arrays."""
+    rng = np.random.default_rng(seed)
+    sizes = np.clip(np.exp(rng.uniform(0, np.log(8192), n_batches)).astype(np.int64), 1, 8192)
+    total = int(sizes.sum())
+    pool_sk = rng.integers(1, 255, (pool, 32), dtype=np.uint8)
+    w = 1.0 / np.arange(1, pool + 1) ** 1.1
+    key_idx = rng.choice(pool, size=total, p=w / w.sum())
+    kinds = (rng.random(total) < 0.7).astype(np.uint8)          # 1 = BIP-340
+    msgs = rng.integers(0, 256, (total, 32), dtype=np.uint8)
+    aux = rng.integers(0, 256, (total, 32), dtype=np.uint8)
+    sks = pool_sk[key_idx]
+    out = {}
+    for kind, ps in ((0, 33), (1, 32)):
+        sel = np.nonzero(kinds == kind)[0]
+        n = sel.size
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        d_m, d_k, d_a = dev(msgs[sel]), dev(sks[sel]), dev(aux[sel])
+        d_p = torch.empty(n * ps, dtype=torch.uint8, device="cuda")
+        d_s = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+        d_ok = torch.empty(n, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        ctx.sign_device(kind, d_m.data_ptr(), d_k.data_ptr(), d_a.data_ptr(), n, d_p.data_ptr(), d_s.data_ptr(),
+                        d_ok.data_ptr(), 0)
+        torch.cuda.ExternalStream(ctx.stream()).synchronize()
+        sigs = d_s.cpu().numpy().reshape(n, 64)
+        expect = np.ones(n, np.uint8)
+        bad = rng.choice(n, size=max(1, n // 200), replace=False)
+        for i in bad:
+            bit = int(rng.integers(0, 512))
+            sigs[i, bit // 8] ^= 1 << (bit % 8)
+        expect[bad] = 0
+        out[kind] = (sel, msgs[sel], d_p.cpu().numpy().reshape(n, ps), sigs, expect)
+    # split back into batches (each batch: its ECDSA items and its BIP-340 items)
+    bounds = np.concatenate([[0], np.cumsum(sizes)])
+    pos = {0: np.searchsorted(out[0][0], bounds), 1: np.searchsorted(out[1][0], bounds)}
+    batches = []
+    for b in range(n_batches):
+        parts = []
+        for kind in (0, 1):
+            lo, hi = pos[kind][b], pos[kind][b + 1]
+            sel, m, p, s, ex = out[kind]
+            parts.append((kind, m[lo:hi], p[lo:hi], s[lo:hi], ex[lo:hi]))
+        batches.append(parts)
+    return batches, total
+
+
+def bench_mixed(ctx, torch):
+    """Per-batch plain ABI calls against one-launch batched jobs, same batches."""
+    import time as _t
+    batches, total = mixed_workload(ctx, torch)
+    # plain: the reference-style synchronous call per batch and kind
+    agree = 0
+    t0 = _t.perf_counter()
+    for parts in batches:
+        for kind, m, p, s, ex in parts:
+            if len(m) == 0:
+                continue
+            v = ctx.ecdsa_verify_batch(m, p, s) if kind == 0 else ctx.schnorr_verify_batch(m, p, s)
+            agree += int((v == ex).sum())
+    t_plain = _t.perf_counter() - t0
+    # batched: groups of consecutive batches packed into one persistent-queue launch
+    group_items = 1 << 18
+    agree_b = 0
+    t0 = _t.perf_counter()
+    i = 0
+    while i < len(batches):
+        jobs, exps, n = [], [], 0
+        while i < len(batches) and (n == 0 or n < group_items):
+            for kind, m, p, s, ex in batches[i]:
+                jobs.append((kind, m, p, s))
+                exps.append(ex)
+                n += len(m)
+            i += 1
+        outs = ctx.verify_jobs(jobs)
+        agree_b += sum(int((o == ex).sum()) for o, ex in zip(outs, exps))
+    t_batched = _t.perf_counter() - t0
+    return {"workload": "2000 mixed batches, sizes log-uniform [1, 8192], 70/30 BIP-340/ECDSA, Zipf(1.1) keys "
+                        "from a 100k pool, 0.5% invalid",
+            "signatures": total,
+            "plain_sigs_per_s": total / t_plain, "batched_sigs_per_s": total / t_batched,
+            "batched_over_plain": t_plain / t_batched,
+            "plain": "one ufsecp_gpu_{ecdsa,schnorr}_verify_batch call per batch and kind (host buffers, wall clock)",
+            "batched": f"ufsecp_gpu_ext_verify_jobs over groups of >= {group_items} signatures (host buffers, wall clock)",
+            "verdict_agreement": {"plain": agree / total, "batched": agree_b / total}}
 
 
 def ecdsa_4096_rate(ctx, torch):

@@ -27,6 +27,30 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_device(ufsecp_gpu_ctx* c
                                                                const uint8_t* d_pubkeys_x32, const uint8_t* d_sigs64,
                                                                size_t count, uint8_t* d_out_results, void* stream);
 
+/* Mixed ECDSA / BIP-340 batches in one launch.  Each job is one caller batch
+ * with the layouts of ufsecp_gpu_ecdsa_verify_batch (kind 0: 33-byte
+ * compressed keys) or ufsecp_gpu_schnorr_verify_batch (kind 1: 32-byte x-only
+ * keys), host buffers.  All jobs are packed into pinned staging and verified
+ * by one persistent work-queue kernel (warps claim 32-item chunks from a
+ * device queue head); layouts up to 65,536 items per kind replay a CUDA graph
+ * captured per capacity bucket.  Synchronous, like the reference calls; the
+ * verdicts equal those of the per-kind calls item for item.  Gating as the
+ * reference ABI: NULL ctx -> NULL_ARG, no jobs -> OK, every out buffer is
+ * cleared first, NULL buffers of a non-empty job -> NULL_ARG, kind > 1 or a
+ * total above 2^26 -> BAD_INPUT. */
+typedef struct {
+    uint32_t kind;                /* 0 = ECDSA, 1 = BIP-340 */
+    uint32_t reserved;            /* 0 */
+    size_t count;
+    const uint8_t* msg_hashes32;  /* count * 32 */
+    const uint8_t* pubkeys;       /* count * 33 (ECDSA) or count * 32 (BIP-340) */
+    const uint8_t* sigs64;        /* count * 64 */
+    uint8_t* out_results;         /* count bytes: 1 valid, 0 invalid */
+} ufsecp_gpu_ext_job_t;
+
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
+                                                     size_t n_jobs);
+
 /* Batch signing for synthetic workloads (device pointers, asynchronous on
  * `stream`): kind 0 = ECDSA, RFC 6979 nonce, low-S compact r||s, 33-byte
  * compressed pubkeys out; kind 1 = BIP-340 with aux_rand (d_aux32), 32-byte

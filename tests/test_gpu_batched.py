@@ -1,0 +1,92 @@
+"""Mixed ECDSA / BIP-340 batches through ufsecp_gpu_ext_verify_jobs (one
+persistent work-queue launch per call, CUDA graphs per capacity bucket):
+verdicts must equal the per-kind plain calls and the oracle item for item."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import ultrafastsecp256k1_b200 as uf
+from conftest import ecdsa_corpus, schnorr_corpus
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def corpora(oracle):
+    e = ecdsa_corpus(oracle, 6000, seed=81, tamper=0.05)
+    s = schnorr_corpus(oracle, 6000, seed=82, tamper=0.05)
+    return e, s, oracle.ecdsa_verify_batch(*e), oracle.schnorr_verify_batch(*s)
+
+
+def _slice(c, lo, hi):
+    return tuple(x[lo:hi] for x in c)
+
+
+def test_mixed_uneven_batches(gpu_ctx, corpora):
+    (e, s, we, ws) = corpora
+    rng = np.random.default_rng(5)
+    jobs, want = [], []
+    pe = ps = 0
+    for k in range(60):
+        kind = int(rng.random() < 0.3) ^ 1          # ~70% BIP-340
+        size = int(np.exp(rng.uniform(0, np.log(300))))
+        if k % 17 == 0:
+            size = 0
+        if kind == 0:
+            size = min(size, 6000 - pe)
+            jobs.append((0,) + _slice(e, pe, pe + size))
+            want.append(we[pe:pe + size])
+            pe += size
+        else:
+            size = min(size, 6000 - ps)
+            jobs.append((1,) + _slice(s, ps, ps + size))
+            want.append(ws[ps:ps + size])
+            ps += size
+    got = gpu_ctx.verify_jobs(jobs)
+    assert len(got) == len(jobs)
+    for g, w in zip(got, want):
+        assert (g == w).all()
+
+
+def test_graph_buckets_replay(gpu_ctx, corpora):
+    """Repeated calls hitting the same and different capacity buckets stay exact."""
+    (e, s, we, ws) = corpora
+    for n_e, n_s in [(1, 1), (255, 0), (0, 257), (300, 900), (300, 900), (2000, 3000), (5, 5999), (6000, 6000)]:
+        jobs = [(0,) + _slice(e, 0, n_e), (1,) + _slice(s, 0, n_s)]
+        ge, gs = gpu_ctx.verify_jobs(jobs)
+        assert (ge == we[:n_e]).all() and (gs == ws[:n_s]).all()
+
+
+def test_direct_path_large(gpu_ctx, oracle):
+    """Above the graph capacity (65,536 per kind) the same sequence runs directly."""
+    base = 4096
+    m, x, s = schnorr_corpus(oracle, base, seed=83, tamper=0.1)
+    w = oracle.schnorr_verify_batch(m, x, s)
+    reps = 20
+    big = (1, np.tile(m, (reps, 1)), np.tile(x, (reps, 1)), np.tile(s, (reps, 1)))
+    me, pe, se = ecdsa_corpus(oracle, 777, seed=84, tamper=0.1)
+    we = oracle.ecdsa_verify_batch(me, pe, se)
+    gs, ge = gpu_ctx.verify_jobs([big, (0, me, pe, se)])
+    assert (gs == np.tile(w, reps)).all() and (ge == we).all()
+
+
+def test_same_verdicts_as_plain_calls(gpu_ctx, corpora):
+    (e, s, we, ws) = corpora
+    ge, gs = gpu_ctx.verify_jobs([(0,) + e, (1,) + s])
+    assert (ge == gpu_ctx.ecdsa_verify_batch(*e)).all()
+    assert (gs == gpu_ctx.schnorr_verify_batch(*s)).all()
+
+
+def test_jobs_gating(gpu_ctx):
+    L = uf.load_library()
+    h = gpu_ctx.handle
+    assert L.ufsecp_gpu_ext_verify_jobs(None, None, 1) == uf.UFSECP_ERR_NULL_ARG
+    assert L.ufsecp_gpu_ext_verify_jobs(h, None, 0) == uf.UFSECP_OK
+    out = np.full(4, 7, np.uint8)
+    j = (uf.Job * 1)(uf.Job(0, 0, 4, None, None, None, out.ctypes.data))
+    assert L.ufsecp_gpu_ext_verify_jobs(h, j, 1) == uf.UFSECP_ERR_NULL_ARG
+    assert (out == 0).all()                      # cleared before the NULL check
+    buf = np.zeros(64 * 4, np.uint8)
+    j = (uf.Job * 1)(uf.Job(2, 0, 4, buf.ctypes.data, buf.ctypes.data, buf.ctypes.data, out.ctypes.data))
+    assert L.ufsecp_gpu_ext_verify_jobs(h, j, 1) == uf.UFSECP_ERR_BAD_INPUT

@@ -45,6 +45,12 @@ class UfsecpError(RuntimeError):
         super().__init__(f"{where}: ufsecp error {code}{' (' + msg + ')' if msg else ''}")
 
 
+class Job(ctypes.Structure):
+    """ufsecp_gpu_ext_job_t: one caller batch of a mixed ufsecp_gpu_ext_verify_jobs call."""
+    _fields_ = [("kind", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("count", ctypes.c_size_t),
+                ("msg_hashes32", _vp), ("pubkeys", _vp), ("sigs64", _vp), ("out_results", _vp)]
+
+
 class DeviceInfo(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 128), ("global_mem_bytes", ctypes.c_uint64),
                 ("compute_units", ctypes.c_uint32), ("max_clock_mhz", ctypes.c_uint32),
@@ -71,6 +77,7 @@ _SIGS = {
     "ufsecp_gpu_schnorr_verify_collect": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_ecdsa_verify_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp]),
     "ufsecp_gpu_ext_schnorr_verify_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp]),
+    "ufsecp_gpu_ext_verify_jobs": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_size_t]),
     "ufsecp_gpu_ext_sign_device": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp,
                                                   _vp]),
     "ufsecp_gpu_ext_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
@@ -223,6 +230,23 @@ class GpuContext:
                             msg_hashes32, pubkeys_x32, 32, sigs64, count=kb.size, out=kb)
 
     # ---- ufsecp_gpu_ext.h -------------------------------------------------------
+    def verify_jobs(self, jobs):
+        """ufsecp_gpu_ext_verify_jobs: jobs = [(kind, msgs, pubs, sigs), ...] with kind 0
+        ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys); returns one verdict array per job."""
+        keep, arr, outs = [], (Job * max(1, len(jobs)))(), []
+        for k, (kind, msgs, pubs, sigs) in enumerate(jobs):
+            m = np.ascontiguousarray(np.asarray(msgs, np.uint8)).reshape(-1)
+            n = m.size // 32
+            p = _buf(pubs, (33 if kind == 0 else 32) * n, "pubkeys")
+            s = _buf(sigs, 64 * n, "sigs64")
+            o = np.zeros(n, np.uint8)
+            keep += [m, p, s]
+            outs.append(o)
+            arr[k] = Job(kind, 0, n, _ptr(m) if n else None, _ptr(p) if n else None, _ptr(s) if n else None,
+                         _ptr(o) if n else None)
+        self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, arr, len(jobs)), "verify_jobs")
+        return outs
+
     def ecdsa_verify_device(self, d_msgs: int, d_pubs33: int, d_sigs: int, count: int, d_out: int,
                             stream: int = 0) -> None:
         """Device pointers in / out, enqueued on `stream` (0 = context stream)."""

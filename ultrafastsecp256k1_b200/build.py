@@ -46,7 +46,11 @@ _VARIANT_FLAGS = [
         ("v4", ["-DUF_VARIANT=4", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]),
         ("v5", ["-DUF_VARIANT=5", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]),
 ]
-VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS, "kernels_probe.cu": _VARIANT_FLAGS}
+# the batched / served kernels are built once, with the code generation that
+# measured fastest for the per-signature kernel on B200 (variant 4)
+_BEST_FLAGS = ["-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]
+VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS, "kernels_probe.cu": _VARIANT_FLAGS,
+            "kernels_queue.cu": [("", _BEST_FLAGS)]}
 
 
 def _sources():

@@ -12,7 +12,10 @@
 #include <memory>
 #include <new>
 
+#include <vector>
+
 #include "backend.h"
+#include "batch.h"
 #include "ufsecp/ufsecp_gpu.h"
 #include "ufsecp/ufsecp_gpu_ext.h"
 
@@ -379,6 +382,38 @@ ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_device(ufsecp_gpu_ctx* ctx, const u
     if (!d_msg_hashes32 || !d_pubkeys_x32 || !d_sigs64 || !d_out_results) return UFSECP_ERR_NULL_ARG;
     return ctx->backend->verify_device(1, d_msg_hashes32, d_pubkeys_x32, d_sigs64, count, d_out_results,
                                        (cudaStream_t)stream);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs, size_t n_jobs) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n_jobs == 0) return UFSECP_OK;
+    if (!jobs) return UFSECP_ERR_NULL_ARG;
+    size_t total = 0;
+    for (size_t j = 0; j < n_jobs; ++j) {
+        if (jobs[j].out_results) clear_out(jobs[j].out_results, jobs[j].count, 1);
+        total += jobs[j].count;
+    }
+    for (size_t j = 0; j < n_jobs; ++j) {
+        const ufsecp_gpu_ext_job_t& J = jobs[j];
+        if (J.count == 0) continue;
+        if (!J.msg_hashes32 || !J.pubkeys || !J.sigs64 || !J.out_results) return UFSECP_ERR_NULL_ARG;
+        if (J.kind > 1) return UFSECP_ERR_BAD_INPUT;
+    }
+    if (total > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    try {
+        std::vector<uf::VerifyJob> v(n_jobs);
+        for (size_t j = 0; j < n_jobs; ++j)
+            v[j] = uf::VerifyJob{(int)jobs[j].kind, jobs[j].count, jobs[j].msg_hashes32, jobs[j].pubkeys,
+                                 jobs[j].sigs64, jobs[j].out_results};
+        const int rc = ctx->backend->verify_jobs(v.data(), n_jobs);
+        if (rc != UFSECP_OK)
+            for (size_t j = 0; j < n_jobs; ++j) clear_out(jobs[j].out_results, jobs[j].count, 1);
+        return rc;
+    } catch (const std::bad_alloc&) {
+        return UFSECP_ERR_GPU_MEMORY;
+    } catch (...) {
+        return UFSECP_ERR_INTERNAL;
+    }
 }
 
 ufsecp_error_t ufsecp_gpu_ext_sign_device(ufsecp_gpu_ctx* ctx, uint32_t kind, const uint8_t* d_msgs32,

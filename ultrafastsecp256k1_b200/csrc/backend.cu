@@ -8,6 +8,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "batch.h"
 #include "kernels.h"
 
 namespace uf {
@@ -112,7 +113,10 @@ void DevBuf::release() {
     cap = 0;
 }
 
+Backend::Backend() = default;
+
 Backend::~Backend() {
+    batch_.reset();
     if (dev_ >= 0) {
         cudaSetDevice(dev_);
         if (stream_) cudaStreamSynchronize(stream_);
@@ -166,6 +170,7 @@ int Backend::init(int device_index) {
     if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return cuda_error(e, "gtable init");
     for (int v = 0; v < kVerifyVariants; ++v)
         for (int k = 0; k < 2; ++k) grid_[v][k] = std::max(1, kOccupancy[v](k)) * sms_;
+    queue_grid_ = std::max(1, verify_queue_occupancy()) * sms_;
     load_tuning();
     (void)cudaGetLastError();
     ready_ = true;
@@ -235,6 +240,20 @@ int Backend::sign_device(int kind, const uint8_t* d_msgs, const uint8_t* d_sks, 
     if (e != cudaSuccess) return cuda_error(e, "sign launch");
     clear_error();
     return kOk;
+}
+
+int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
+    if (!ready_) return set_error(kErrGpuDevice, "context not ready");
+    if (!batch_) {
+        auto slot = std::make_unique<BatchSlot>();
+        const int rc = slot->init(this);
+        if (rc != kOk) return rc;
+        batch_ = std::move(slot);
+    }
+    int rc = batch_->enqueue(jobs, n_jobs);
+    if (rc == kOk) rc = batch_->finish(jobs, n_jobs);
+    if (rc == kOk) clear_error();
+    return rc;
 }
 
 int Backend::diag(uint32_t op, const uint8_t* in, size_t n, uint8_t* out, size_t in_sz, size_t out_sz) {

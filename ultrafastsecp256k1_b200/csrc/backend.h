@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <memory>
 #include <string>
 
 namespace uf {
@@ -29,9 +30,12 @@ struct DevBuf {
     void release();
 };
 
+struct VerifyJob;
+class BatchSlot;
+
 class Backend {
 public:
-    Backend() = default;
+    Backend();
     ~Backend();
     Backend(const Backend&) = delete;
     Backend& operator=(const Backend&) = delete;
@@ -54,6 +58,10 @@ public:
     // Batch signing (workload generator), device buffers, asynchronous.
     int sign_device(int kind, const uint8_t* d_msgs, const uint8_t* d_sks, const uint8_t* d_auxs, size_t count,
                     uint8_t* d_pubs, uint8_t* d_sigs, uint8_t* d_ok, cudaStream_t stream);
+    // Mixed ECDSA / BIP-340 jobs (host buffers) in one persistent-queue launch;
+    // synchronous.
+    int verify_jobs(const VerifyJob* jobs, size_t n_jobs);
+    int queue_grid() const { return queue_grid_; }
     int diag(uint32_t op, const uint8_t* in, size_t n, uint8_t* out, size_t in_sz, size_t out_sz);
     int imad_peak(double* ops_per_s);
     int probe(int op, int blocks, int threads, int iters, float* ms);
@@ -74,13 +82,15 @@ private:
     int sms_ = 0;
     std::string dev_name_;
     int grid_[6][2] = {};        // [variant][kind] resident-grid size
-    int variant_[2] = {2, 2};    // chosen variant per kind (2: out-of-line field and point ops)
+    int variant_[2] = {4, 4};    // chosen variant per kind (4: out-of-line field / point ops, PTX chains)
     cudaError_t launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
                               uint8_t* out, int collect, cudaStream_t st);
     void load_tuning();
     cudaStream_t stream_ = nullptr;
     void* d_gtab_ = nullptr;
     DevBuf msgs_, pubs_, sigs_, out_, scratch_;
+    int queue_grid_ = 0;
+    std::unique_ptr<BatchSlot> batch_;   // slot of the synchronous mixed-batch call
     int last_err_ = kOk;
     std::string last_msg_ = "OK";
 };

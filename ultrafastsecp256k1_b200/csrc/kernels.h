@@ -47,6 +47,45 @@ int verify_occupancy_v3(int kind);
 int verify_occupancy_v4(int kind);
 int verify_occupancy_v5(int kind);
 
+// Mixed-batch staging layout shared by host (pinned) and device buffers:
+//   [header 256 B: counts n_e, n_s][e_msgs cap_e*32][s_msgs cap_s*32]
+//   [e_sigs cap_e*64][s_sigs cap_s*64][s_pubs cap_s*32][e_pubs cap_e*33]
+//   [e_out cap_e][s_out cap_s]
+// Every region starts 256-byte aligned.  in_bytes covers header + inputs (one
+// host->device copy), out_bytes the verdicts (one device->host copy).
+struct QueueLayout {
+    uint32_t cap_e = 0, cap_s = 0;
+    size_t e_msgs, s_msgs, e_sigs, s_sigs, s_pubs, e_pubs, e_out, s_out, in_bytes, out_bytes, total;
+    static size_t up(size_t x) { return (x + 255) & ~size_t{255}; }
+    QueueLayout() = default;
+    QueueLayout(uint32_t ce, uint32_t cs) : cap_e(ce), cap_s(cs) {
+        e_msgs = 256;
+        s_msgs = up(e_msgs + (size_t)ce * 32);
+        e_sigs = up(s_msgs + (size_t)cs * 32);
+        s_sigs = up(e_sigs + (size_t)ce * 64);
+        s_pubs = up(s_sigs + (size_t)cs * 64);
+        e_pubs = up(s_pubs + (size_t)cs * 32);
+        e_out = up(e_pubs + (size_t)ce * 33);
+        s_out = up(e_out + (size_t)ce);
+        total = up(s_out + (size_t)cs);
+        in_bytes = e_out;
+        out_bytes = total - e_out;
+    }
+};
+
+struct QueueArgs {
+    const uint32_t* counts;  // device header: n_e, n_s
+    uint32_t cap_e, cap_s;   // region capacities: the kernel never reads past them
+    const uint8_t *e_msgs, *e_pubs, *e_sigs, *s_msgs, *s_pubs, *s_sigs;
+    uint8_t *e_out, *s_out;
+};
+
+// Zeroes the queue head, then launches the persistent queue kernel (`grid`
+// resident blocks) over the items described by `a` (kernels_queue.cu).
+cudaError_t launch_verify_queue(const QueueArgs& a, const void* d_gtab, unsigned int* d_head, int grid,
+                                cudaStream_t s);
+int verify_queue_occupancy();
+
 // Batch signer (workload generator): kind 0 = ECDSA (pubs 33 B), 1 = BIP-340
 // (pubs 32 B x-only, auxs 32 B aux_rand).  ok[i] = 0 for an invalid key.
 cudaError_t launch_sign(int kind, const uint8_t* msgs, const uint8_t* sks, const uint8_t* auxs, uint32_t n,

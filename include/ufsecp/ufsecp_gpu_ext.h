@@ -51,6 +51,25 @@ typedef struct {
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
                                                      size_t n_jobs);
 
+/* Allocation-free variant of ufsecp_gpu_ext_verify_jobs, for callers that
+ * cannot call cudaMalloc (GPU memory owned by another allocator or framework,
+ * a fixed device-memory budget, or a policy that the verifier must not
+ * allocate).  No counterpart in the reference.  The jobs' buffers are DEVICE
+ * (device-accessible) memory the caller owns: msgs / signatures / x-only keys
+ * 16-byte aligned, outputs one byte per item.  The call allocates nothing: the
+ * work-queue kernel's scratch (queue head and job table) is a static device
+ * array of the library, at most UFSECP_GPU_EXT_NOALLOC_MAX_JOBS jobs per call
+ * (more -> UFSECP_ERR_BAD_INPUT with an explanatory last_error_msg).  The
+ * first call on a device looks up that array's device address; make it before
+ * any stream capture.  The call returns after enqueueing the kernel on
+ * `stream` (NULL = the context's stream); the verdicts are ready when the
+ * stream reaches that point.  All calls share the array and the queue head is
+ * reset by every call, so calls whose work overlaps on the GPU race: serialise
+ * them (one stream, or wait for the previous call). */
+#define UFSECP_GPU_EXT_NOALLOC_MAX_JOBS 1024
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs_noalloc(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
+                                                             size_t n_jobs, void* stream);
+
 /* Batch signing for synthetic workloads (device pointers, asynchronous on
  * `stream`): kind 0 = ECDSA, RFC 6979 nonce, low-S compact r||s, 33-byte
  * compressed pubkeys out; kind 1 = BIP-340 with aux_rand (d_aux32), 32-byte

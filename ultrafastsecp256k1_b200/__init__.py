@@ -78,6 +78,7 @@ _SIGS = {
     "ufsecp_gpu_ext_ecdsa_verify_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp]),
     "ufsecp_gpu_ext_schnorr_verify_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp]),
     "ufsecp_gpu_ext_verify_jobs": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_size_t]),
+    "ufsecp_gpu_ext_verify_jobs_noalloc": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_sign_device": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp, _vp,
                                                   _vp]),
     "ufsecp_gpu_ext_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),

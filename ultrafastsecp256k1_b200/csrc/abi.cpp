@@ -416,6 +416,42 @@ ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_
     }
 }
 
+ufsecp_error_t ufsecp_gpu_ext_verify_jobs_noalloc(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
+                                                  size_t n_jobs, void* stream) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n_jobs == 0) return UFSECP_OK;
+    if (!jobs) return UFSECP_ERR_NULL_ARG;
+    uf::Backend& be = *ctx->backend;
+    if (n_jobs > uf::kNoAllocJobLimit)
+        return be.set_error(UFSECP_ERR_BAD_INPUT,
+                            "more than 1024 jobs: the allocation-free path's static scratch holds 1024 job descriptors");
+    size_t total = 0;
+    for (size_t j = 0; j < n_jobs; ++j) {
+        const ufsecp_gpu_ext_job_t& J = jobs[j];
+        if (J.kind > 1) return be.set_error(UFSECP_ERR_BAD_INPUT, "job kind must be 0 (ECDSA) or 1 (BIP-340)");
+        if (J.count == 0) continue;
+        if (!J.msg_hashes32 || !J.pubkeys || !J.sigs64 || !J.out_results) return UFSECP_ERR_NULL_ARG;
+        if (((uintptr_t)J.msg_hashes32 | (uintptr_t)J.sigs64 | (J.kind == 1 ? (uintptr_t)J.pubkeys : 0)) & 15u)
+            return be.set_error(UFSECP_ERR_BAD_INPUT, "device inputs must be 16-byte aligned");
+        total += J.count;
+    }
+    if (total > kMaxBatch) return be.set_error(UFSECP_ERR_BAD_INPUT, "more than 2^26 items");
+    if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
+    uf::NoAllocJobDesc desc[uf::kNoAllocJobLimit];
+    for (size_t j = 0; j < n_jobs; ++j)
+        desc[j] = uf::NoAllocJobDesc{jobs[j].kind, jobs[j].count, jobs[j].msg_hashes32, jobs[j].pubkeys,
+                                     jobs[j].sigs64, jobs[j].out_results};
+    cudaError_t e = cudaSetDevice(be.device());
+    int limit = 0;
+    if (e == cudaSuccess)
+        e = uf::verify_jobs_noalloc(be.device(), desc, n_jobs, be.gtab(),
+                                    stream ? (cudaStream_t)stream : be.stream(), &limit);
+    if (limit) return be.set_error(UFSECP_ERR_BAD_INPUT, "job limits of the allocation-free path exceeded");
+    if (e != cudaSuccess) return be.cuda_error(e, "allocation-free verify");
+    be.clear_error();
+    return UFSECP_OK;
+}
+
 ufsecp_error_t ufsecp_gpu_ext_sign_device(ufsecp_gpu_ctx* ctx, uint32_t kind, const uint8_t* d_msgs32,
                                           const uint8_t* d_privkeys32, const uint8_t* d_aux32, size_t count,
                                           uint8_t* d_pubkeys_out, uint8_t* d_sigs64_out, uint8_t* d_ok, void* stream) {

@@ -86,6 +86,21 @@ cudaError_t launch_verify_queue(const QueueArgs& a, const void* d_gtab, unsigned
                                 cudaStream_t s);
 int verify_queue_occupancy();
 
+// Allocation-free mixed verification (kernels_noalloc.cu): jobs hold
+// device-accessible buffers; the queue head and the job table live in a
+// static device array of the library, nothing is allocated.
+struct NoAllocJobDesc {
+    uint32_t kind;
+    size_t count;
+    const uint8_t* msgs;
+    const uint8_t* pubs;
+    const uint8_t* sigs;
+    uint8_t* out;
+};
+constexpr size_t kNoAllocJobLimit = 1024;
+cudaError_t verify_jobs_noalloc(int device, const NoAllocJobDesc* jobs, size_t n_jobs, const void* d_gtab,
+                                cudaStream_t s, int* limit_hit);
+
 // Batch signer (workload generator): kind 0 = ECDSA (pubs 33 B), 1 = BIP-340
 // (pubs 32 B x-only, auxs 32 B aux_rand).  ok[i] = 0 for an invalid key.
 cudaError_t launch_sign(int kind, const uint8_t* msgs, const uint8_t* sks, const uint8_t* auxs, uint32_t n,

@@ -154,9 +154,10 @@ def tamper(rng, xs, sigs, expect):
     expect[idx] = 0
 
 
-def make_schnorr_batch(ctx, torch, n: int, seed: int):
+def make_schnorr_batch(ctx, torch, n: int, seed: int, invalid: bool = True):
     """Seeded BIP-340 batch, signed on the GPU; returns device tensors, host
-    copies and the verdict every item must get (by construction)."""
+    copies and the verdict every item must get (by construction).  invalid=False
+    leaves every signature valid."""
     rng = np.random.default_rng(seed)
     sks = rng.integers(0, 256, (n, 32), dtype=np.uint8)
     # keys uniform in [1, n-1]: redraw the (astronomically rare) values outside
@@ -179,7 +180,8 @@ def make_schnorr_batch(ctx, torch, n: int, seed: int):
     xs = d_xs.cpu().numpy().reshape(n, 32)
     sigs = d_sigs.cpu().numpy().reshape(n, 64)
     expect = np.ones(n, np.uint8)
-    tamper(rng, xs, sigs, expect)
+    if invalid:
+        tamper(rng, xs, sigs, expect)
     d_xs = dev(xs)
     d_sigs = dev(sigs)
     d_out = torch.zeros(n, dtype=torch.uint8, device="cuda")
@@ -338,10 +340,12 @@ def run_ours(args):
     # ---- secondary: plain ECDSA on 4096 signatures (one launch) -----------
     ecdsa_rate = None
     mixed = None
+    rlc = None
     if rank == 0:
         ecdsa_rate = ecdsa_4096_rate(ctx, torch)
         if not args.no_secondary:
             mixed = bench_mixed(ctx, torch)
+            rlc = bench_rlc(ctx, torch)
 
     # ---- CPU baseline (rank 0, one GPU only) --------------------------------
     cpu = None
@@ -390,7 +394,7 @@ def run_ours(args):
             "clocks": clocks,
             "gpu_launches": args.steps,
             "verdict_agreement": agree / n,
-            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate, "mixed_batches": mixed},
+            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate, "mixed_batches": mixed, "rlc_batch_verify": rlc},
         }
         print(json.dumps(line))
     del d_msgs, d_xs, d_sigs, d_out
@@ -487,6 +491,61 @@ def bench_mixed(ctx, torch):
             "plain": "one ufsecp_gpu_{ecdsa,schnorr}_verify_batch call per batch and kind (host buffers, wall clock)",
             "batched": f"ufsecp_gpu_ext_verify_jobs over groups of >= {group_items} signatures (host buffers, wall clock)",
             "verdict_agreement": {"plain": agree / total, "batched": agree_b / total}}
+
+
+def bench_rlc(ctx, torch, n: int = 1 << 20, reps: int = 3):
+    """RLC batch verify (BIP-340) against the plain kernel on the same n valid
+    signatures cut into batches of 64 / 512 / 4096 / 16384, with 0 or 1 invalid
+    signature per batch (one flipped bit of s).  Device-resident inputs; each
+    RLC call is synchronous (it reads every round's result on the host), so it
+    is timed by wall clock around the call, after one untimed call."""
+    (d_m, d_x, d_s, d_out), (msgs, xs, sigs), _ = make_schnorr_batch(ctx, torch, n, seed=64, invalid=False)
+    st = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        ctx.schnorr_verify_device(d_m.data_ptr(), d_x.data_ptr(), d_s.data_ptr(), n, d_out.data_ptr(), st.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        ctx.schnorr_verify_device(d_m.data_ptr(), d_x.data_ptr(), d_s.data_ptr(), n, d_out.data_ptr(), st.cuda_stream)
+    b.record(st)
+    torch.cuda.synchronize()
+    plain = n * reps / (a.elapsed_time(b) * 1e-3)
+    rng = np.random.default_rng(65)
+    rows = []
+    for bs in (64, 512, 4096, 16384):
+        for bad in (0, 1):
+            expect = np.ones(n, np.uint8)
+            d_sig = d_s
+            if bad:
+                s_bad = sigs.copy()
+                for start in range(0, n, bs):
+                    i = start + int(rng.integers(0, min(bs, n - start)))
+                    bit = int(rng.integers(0, 256))
+                    s_bad[i, 32 + bit // 8] ^= 1 << (bit % 8)
+                    expect[i] = 0
+                d_sig = torch.from_numpy(s_bad).cuda()
+            torch.cuda.synchronize()
+            seed = rng.bytes(32)
+            ctx.schnorr_verify_rlc_device(d_m.data_ptr(), d_x.data_ptr(), d_sig.data_ptr(), n, d_out.data_ptr(),
+                                          batch_size=bs, seed32=seed, stream=st.cuda_stream)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                ctx.schnorr_verify_rlc_device(d_m.data_ptr(), d_x.data_ptr(), d_sig.data_ptr(), n, d_out.data_ptr(),
+                                              batch_size=bs, seed32=seed, stream=st.cuda_stream)
+            dt = (time.perf_counter() - t0) / reps
+            stats = ctx.rlc_stats()
+            agree = float((d_out.cpu().numpy() == expect).mean())
+            rows.append({"batch": bs, "invalid_per_batch": bad, "sigs_per_s": n / dt, "ms_per_call": dt * 1e3,
+                         "over_plain": n / dt / plain, "window_bits": stats["window_bits"],
+                         "msm_rounds": stats["rounds"], "leaf_items": stats["leaf_items"],
+                         "verdict_agreement": agree})
+            del d_sig
+    return {"workload": f"{n} valid BIP-340 signatures in batches of 64/512/4096/16384, 0 or 1 invalid per batch",
+            "plain_sigs_per_s": plain,
+            "plain": "ufsecp_gpu_ext_schnorr_verify_device, one launch over all items, CUDA events",
+            "rlc": "ufsecp_gpu_ext_schnorr_verify_rlc_device (device buffers, wall clock per call)",
+            "rows": rows}
 
 
 def ecdsa_4096_rate(ctx, torch):

@@ -70,6 +70,53 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const 
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs_noalloc(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
                                                              size_t n_jobs, void* stream);
 
+/* BIP-340 batch verification by random linear combination (RLC).
+ * Counterpart of the reference's CPU batch verify (schnorr_batch_verify,
+ * src/cpu/src/batch_verify.cpp:324-424) with per-item verdicts: the items are
+ * cut into batches of batch_size (0 = one batch, the last batch ragged); every
+ * batch is checked by ONE multi-scalar multiplication
+ *     sum a_i R_i + sum (a_i e_i) P_i - (sum a_i s_i) G == infinity
+ * with 128-bit weights a_i = SHA-256(seed32 || le32 i)[0:16] (never 0);
+ * failing batches are bisected and small failing pieces verified one by one,
+ * so out_results[i] equals ufsecp_gpu_schnorr_verify_batch's verdict for every
+ * item (a false accept needs a 2^-128 event).  out_batch_ok (may be NULL)
+ * receives one byte per batch: 1 when all its items are valid.  window_bits:
+ * 0 = chosen per batch length, else 4..16 (Pippenger window).  seed32 should
+ * be unpredictable to whoever produced the signatures.  Up to 2^24 items per
+ * call.  Host buffers, synchronous; the _device form takes 16-byte aligned
+ * device buffers and runs on `stream` (NULL = the context's stream), returning
+ * when the verdicts are written (it reads each round's result on the host). */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32,
+                                                            const uint8_t* pubkeys_x32, const uint8_t* sigs64,
+                                                            size_t count, size_t batch_size, const uint8_t* seed32,
+                                                            int window_bits, uint8_t* out_results,
+                                                            uint8_t* out_batch_ok);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
+                                                                   const uint8_t* d_pubkeys_x32,
+                                                                   const uint8_t* d_sigs64, size_t count,
+                                                                   size_t batch_size, const uint8_t* seed32,
+                                                                   int window_bits, uint8_t* d_out_results,
+                                                                   uint8_t* out_batch_ok, void* stream);
+/* Counters of the context's last RLC call: out[0] MSM rounds (the first check
+ * plus one per bisection level), out[1] segments checked, out[2] items
+ * verified one by one, out[3] window bits of the first round. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_stats(ufsecp_gpu_ctx* ctx, uint64_t out[4]);
+
+/* The reference's batch API on the GPU, same rows, gating and results:
+ * ufsecp_schnorr_batch_verify (src/cpu/src/impl/ufsecp_taproot.cpp:703) and
+ * ufsecp_schnorr_batch_identify_invalid (:849).  Rows are [x-only key 32 |
+ * msg 32 | sig 64] = 128 bytes, n <= 2^20.  The first row (in index order)
+ * with x >= p returns UFSECP_ERR_BAD_PUBKEY, with r >= p or s outside [1, n-1]
+ * UFSECP_ERR_BAD_SIG.  batch_verify returns UFSECP_OK when every row is valid
+ * and UFSECP_ERR_VERIFY_FAIL otherwise; identify_invalid writes the indices
+ * of the invalid rows, ascending (at most *invalid_count of them), and sets
+ * *invalid_count to their total.  One RLC batch of all rows with a fresh
+ * random seed, bisected on failure. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_verify(ufsecp_gpu_ctx* ctx, const uint8_t* entries, size_t n);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_identify_invalid(ufsecp_gpu_ctx* ctx, const uint8_t* entries,
+                                                                        size_t n, size_t* invalid_out,
+                                                                        size_t* invalid_count);
+
 /* Batch signing for synthetic workloads (device pointers, asynchronous on
  * `stream`): kind 0 = ECDSA, RFC 6979 nonce, low-S compact r||s, 33-byte
  * compressed pubkeys out; kind 1 = BIP-340 with aux_rand (d_aux32), 32-byte

@@ -173,6 +173,10 @@ class RefLib:
         L.ufsecp_pubkey_xonly.argtypes = [ctypes.c_void_p, _u8p, _u8p]
         L.ufsecp_schnorr_batch_verify.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t]
         L.ufsecp_schnorr_batch_verify.restype = ctypes.c_int
+        L.ufsecp_schnorr_batch_identify_invalid.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t,
+                                                           ctypes.POINTER(ctypes.c_size_t),
+                                                           ctypes.POINTER(ctypes.c_size_t)]
+        L.ufsecp_schnorr_batch_identify_invalid.restype = ctypes.c_int
         L.ufsecp_set_cache_dir.argtypes = [ctypes.c_char_p]
         L.ufsecp_set_cache_dir(_CACHE_DIR.encode())
         self._tls = threading.local()
@@ -251,6 +255,16 @@ class RefLib:
         """ufsecp_schnorr_batch_verify over 128-byte rows pk|msg|sig (RLC form)."""
         rows = _as_u8(rows128)
         return self.L.ufsecp_schnorr_batch_verify(self.ctx(), _ptr(rows), rows.size // 128)
+
+    def schnorr_batch_identify_invalid_rows(self, rows128: np.ndarray, capacity: int | None = None):
+        """ufsecp_schnorr_batch_identify_invalid: (code, indices, total invalid)."""
+        rows = _as_u8(rows128)
+        n = rows.size // 128
+        cap = n if capacity is None else capacity
+        buf = (ctypes.c_size_t * max(cap, 1))()
+        cnt = ctypes.c_size_t(cap)
+        rc = self.L.ufsecp_schnorr_batch_identify_invalid(self.ctx(), _ptr(rows), n, buf, ctypes.byref(cnt))
+        return rc, [buf[i] for i in range(min(cap, cnt.value))], cnt.value
 
 
 class RefDriver:

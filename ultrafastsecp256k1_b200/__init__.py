@@ -22,7 +22,10 @@ LIB_PATH = os.path.join(PKG, "lib", "libufsecp_gpu.so")
 
 UFSECP_OK = 0
 UFSECP_ERR_NULL_ARG = 1
+UFSECP_ERR_BAD_PUBKEY = 3
+UFSECP_ERR_BAD_SIG = 4
 UFSECP_ERR_BAD_INPUT = 5
+UFSECP_ERR_VERIFY_FAIL = 6
 UFSECP_ERR_INTERNAL = 9
 UFSECP_ERR_GPU_UNAVAILABLE = 100
 UFSECP_ERR_GPU_DEVICE = 101
@@ -91,6 +94,15 @@ _SIGS = {
     "ufsecp_gpu_ext_diag": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_probe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_float)]),
+    "ufsecp_gpu_ext_schnorr_verify_rlc": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp,
+                                                         ctypes.c_int, _vp, _vp]),
+    "ufsecp_gpu_ext_schnorr_verify_rlc_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t,
+                                                                _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "ufsecp_gpu_ext_schnorr_batch_verify": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
+    "ufsecp_gpu_ext_schnorr_batch_identify_invalid": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t,
+                                                                     ctypes.POINTER(ctypes.c_size_t),
+                                                                     ctypes.POINTER(ctypes.c_size_t)]),
 }
 
 
@@ -247,6 +259,59 @@ class GpuContext:
                          _ptr(o) if n else None)
         self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, arr, len(jobs)), "verify_jobs")
         return outs
+
+    def schnorr_verify_rlc(self, msg_hashes32, pubkeys_x32, sigs64, batch_size: int = 0, seed32=None,
+                           window_bits: int = 0):
+        """ufsecp_gpu_ext_schnorr_verify_rlc: RLC batch verify with bisection.
+        Returns (per-item verdicts, per-batch all-valid flags)."""
+        n = np.asarray(msg_hashes32, np.uint8).size // 32 if not isinstance(msg_hashes32, (bytes, bytearray)) \
+            else len(msg_hashes32) // 32
+        m = _buf(msg_hashes32, 32 * n, "msg_hashes32")
+        p = _buf(pubkeys_x32, 32 * n, "pubkeys_x32")
+        s = _buf(sigs64, 64 * n, "sigs64")
+        seed = _buf(seed32 if seed32 is not None else os.urandom(32), 32, "seed32")
+        out = np.zeros(n, np.uint8)
+        nb = 1 if batch_size == 0 or batch_size >= n else -(-n // batch_size)
+        bok = np.zeros(max(nb, 1), np.uint8)
+        rc = self.L.ufsecp_gpu_ext_schnorr_verify_rlc(self._ctx, _ptr(m), _ptr(p), _ptr(s), n, batch_size,
+                                                      _ptr(seed), window_bits, _ptr(out), _ptr(bok))
+        self._check(rc, "schnorr_verify_rlc")
+        return out, bok[:nb]
+
+    def schnorr_verify_rlc_device(self, d_msgs: int, d_xonly: int, d_sigs: int, count: int, d_out: int,
+                                  batch_size: int = 0, seed32=None, window_bits: int = 0, stream: int = 0):
+        """Device-buffer RLC verify; returns the per-batch all-valid flags."""
+        seed = _buf(seed32 if seed32 is not None else os.urandom(32), 32, "seed32")
+        nb = 1 if batch_size == 0 or batch_size >= count else -(-count // batch_size)
+        bok = np.zeros(max(nb, 1), np.uint8)
+        rc = self.L.ufsecp_gpu_ext_schnorr_verify_rlc_device(self._ctx, d_msgs, d_xonly, d_sigs, count, batch_size,
+                                                             _ptr(seed), window_bits, d_out, _ptr(bok),
+                                                             stream or None)
+        self._check(rc, "schnorr_verify_rlc_device")
+        return bok[:nb]
+
+    def rlc_stats(self) -> dict:
+        v = (ctypes.c_uint64 * 4)()
+        self._check(self.L.ufsecp_gpu_ext_rlc_stats(self._ctx, v), "rlc_stats")
+        return {"rounds": v[0], "segments": v[1], "leaf_items": v[2], "window_bits": v[3]}
+
+    def schnorr_batch_verify(self, entries) -> int:
+        """ufsecp_gpu_ext_schnorr_batch_verify on rows [x 32 | msg 32 | sig 64]; returns the
+        reference's code (0 all valid, 6 VERIFY_FAIL, 3 BAD_PUBKEY, 4 BAD_SIG, ...)."""
+        e = np.ascontiguousarray(np.asarray(entries, np.uint8)).reshape(-1)
+        return self.L.ufsecp_gpu_ext_schnorr_batch_verify(self._ctx, _ptr(e) if e.size else None, e.size // 128)
+
+    def schnorr_batch_identify_invalid(self, entries, capacity: int = None):
+        """Returns (code, invalid indices, total invalid)."""
+        e = np.ascontiguousarray(np.asarray(entries, np.uint8)).reshape(-1)
+        n = e.size // 128
+        cap = n if capacity is None else capacity
+        buf = (ctypes.c_size_t * max(cap, 1))()
+        cnt = ctypes.c_size_t(cap)
+        rc = self.L.ufsecp_gpu_ext_schnorr_batch_identify_invalid(self._ctx, _ptr(e) if e.size else None, n, buf,
+                                                                  ctypes.byref(cnt))
+        got = min(cnt.value, cap)
+        return rc, [buf[i] for i in range(got)], cnt.value
 
     def ecdsa_verify_device(self, d_msgs: int, d_pubs33: int, d_sigs: int, count: int, d_out: int,
                             stream: int = 0) -> None:

@@ -11,11 +11,14 @@
 #include <limits>
 #include <memory>
 #include <new>
+#include <random>
+#include <algorithm>
 
 #include <vector>
 
 #include "backend.h"
 #include "batch.h"
+#include "rlc.h"
 #include "ufsecp/ufsecp_gpu.h"
 #include "ufsecp/ufsecp_gpu_ext.h"
 
@@ -23,6 +26,7 @@ struct ufsecp_gpu_ctx {
     std::unique_ptr<uf::Backend> backend;
     uint32_t backend_id;
     uint32_t device_index;
+    uf::RlcStats rlc_stats;      // of the last RLC call
 };
 
 namespace {
@@ -512,6 +516,159 @@ ufsecp_error_t ufsecp_gpu_ext_diag(ufsecp_gpu_ctx* ctx, uint32_t op, const uint8
     static const int out_sz[11] = {0, 32, 32, 32, 33, 32, 32, 34, 64, 65, 32};
     if (op < 1 || op > 10 || n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
     return ctx->backend->diag(op, in, n, out, (size_t)in_sz[op], (size_t)out_sz[op]);
+}
+
+}  // extern "C"
+
+// ---- RLC batch verification ------------------------------------------------
+
+namespace {
+
+constexpr size_t kMaxRlcItems = size_t{1} << 24;
+constexpr size_t kMaxRefBatch = size_t{1} << 20;   // the reference batch API's cap
+
+void fresh_seed(uint8_t seed[32]) {
+    std::random_device rd;
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t v = rd();
+        memcpy(seed + 4 * k, &v, 4);
+    }
+}
+
+template <class F>
+ufsecp_error_t guarded(F&& run) {
+    try {
+        return run();
+    } catch (const std::bad_alloc&) {
+        return UFSECP_ERR_GPU_MEMORY;
+    } catch (...) {
+        return UFSECP_ERR_INTERNAL;
+    }
+}
+
+// Shared body of the two reference-shaped batch calls: gate + verdicts.
+ufsecp_error_t rows_verdicts(ufsecp_gpu_ctx* ctx, const uint8_t* entries, size_t n, std::vector<uint8_t>& verdicts) {
+    uf::Backend& be = *ctx->backend;
+    if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
+    cudaError_t e = cudaSetDevice(be.device());
+    if (e != cudaSuccess) return be.cuda_error(e, "cudaSetDevice");
+    uint8_t seed[32];
+    fresh_seed(seed);
+    verdicts.assign(n, 0);
+    int gate = 0;
+    uint32_t where = 0;
+    ctx->rlc_stats = uf::RlcStats{};
+    const int rc = be.rlc().verify_entries(entries, (uint32_t)n, seed, verdicts.data(), &gate, &where,
+                                           &ctx->rlc_stats);
+    if (rc != UFSECP_OK) return rc;
+    if (gate == UFSECP_ERR_BAD_PUBKEY) return be.set_error(gate, "non-canonical pubkey (x>=p) in batch");
+    if (gate == UFSECP_ERR_BAD_SIG) return be.set_error(gate, "invalid Schnorr sig in batch");
+    be.clear_error();
+    return UFSECP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32,
+                                                 const uint8_t* pubkeys_x32, const uint8_t* sigs64, size_t count,
+                                                 size_t batch_size, const uint8_t* seed32, int window_bits,
+                                                 uint8_t* out_results, uint8_t* out_batch_ok) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (count > kMaxRlcItems) return ctx->backend->set_error(UFSECP_ERR_BAD_INPUT, "RLC: more than 2^24 items");
+    clear_out(out_results, count, 1);
+    const size_t n_batches = batch_size == 0 || batch_size >= count ? 1 : (count + batch_size - 1) / batch_size;
+    clear_out(out_batch_ok, n_batches, 1);
+    if (!msg_hashes32 || !pubkeys_x32 || !sigs64 || !seed32 || !out_results) return UFSECP_ERR_NULL_ARG;
+    return guarded([&]() -> ufsecp_error_t {
+        uf::Backend& be = *ctx->backend;
+        if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
+        cudaError_t e = cudaSetDevice(be.device());
+        if (e != cudaSuccess) return be.cuda_error(e, "cudaSetDevice");
+        ctx->rlc_stats = uf::RlcStats{};
+        const int rc = be.rlc().verify_host(msg_hashes32, pubkeys_x32, sigs64, (uint32_t)count,
+                                            (uint32_t)std::min(batch_size, count), seed32, window_bits, out_results,
+                                            out_batch_ok, &ctx->rlc_stats);
+        if (rc != UFSECP_OK) {
+            clear_out(out_results, count, 1);
+            clear_out(out_batch_ok, n_batches, 1);
+            return rc;
+        }
+        be.clear_error();
+        return UFSECP_OK;
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
+                                                        const uint8_t* d_pubkeys_x32, const uint8_t* d_sigs64,
+                                                        size_t count, size_t batch_size, const uint8_t* seed32,
+                                                        int window_bits, uint8_t* d_out_results,
+                                                        uint8_t* out_batch_ok, void* stream) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (count > kMaxRlcItems) return ctx->backend->set_error(UFSECP_ERR_BAD_INPUT, "RLC: more than 2^24 items");
+    if (!d_msg_hashes32 || !d_pubkeys_x32 || !d_sigs64 || !seed32 || !d_out_results) return UFSECP_ERR_NULL_ARG;
+    return guarded([&]() -> ufsecp_error_t {
+        uf::Backend& be = *ctx->backend;
+        if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
+        cudaError_t e = cudaSetDevice(be.device());
+        if (e != cudaSuccess) return be.cuda_error(e, "cudaSetDevice");
+        ctx->rlc_stats = uf::RlcStats{};
+        const int rc = be.rlc().verify(d_msg_hashes32, d_pubkeys_x32, d_sigs64, (uint32_t)count,
+                                       (uint32_t)std::min(batch_size, count), seed32, window_bits, d_out_results,
+                                       out_batch_ok, stream ? (cudaStream_t)stream : be.stream(), &ctx->rlc_stats);
+        if (rc != UFSECP_OK) return rc;
+        be.clear_error();
+        return UFSECP_OK;
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_rlc_stats(ufsecp_gpu_ctx* ctx, uint64_t out[4]) {
+    if (!ctx || !out) return UFSECP_ERR_NULL_ARG;
+    out[0] = ctx->rlc_stats.rounds;
+    out[1] = ctx->rlc_stats.segments;
+    out[2] = ctx->rlc_stats.leaf_items;
+    out[3] = (uint64_t)ctx->rlc_stats.window_bits;
+    return UFSECP_OK;
+}
+
+ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_verify(ufsecp_gpu_ctx* ctx, const uint8_t* entries, size_t n) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (!entries) return UFSECP_ERR_NULL_ARG;
+    if (n > kMaxRefBatch) return ctx->backend->set_error(UFSECP_ERR_BAD_INPUT, "batch count too large");
+    return guarded([&]() -> ufsecp_error_t {
+        std::vector<uint8_t> v;
+        const ufsecp_error_t rc = rows_verdicts(ctx, entries, n, v);
+        if (rc != UFSECP_OK) return rc;
+        for (size_t i = 0; i < n; ++i)
+            if (!v[i]) return ctx->backend->set_error(UFSECP_ERR_VERIFY_FAIL, "batch verify failed");
+        return UFSECP_OK;
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_identify_invalid(ufsecp_gpu_ctx* ctx, const uint8_t* entries, size_t n,
+                                                             size_t* invalid_out, size_t* invalid_count) {
+    if (!ctx || !entries || !invalid_out || !invalid_count) return UFSECP_ERR_NULL_ARG;
+    if (n > kMaxRefBatch) return ctx->backend->set_error(UFSECP_ERR_BAD_INPUT, "batch count too large");
+    return guarded([&]() -> ufsecp_error_t {
+        const size_t cap = *invalid_count;
+        std::vector<uint8_t> v;
+        if (n) {
+            const ufsecp_error_t rc = rows_verdicts(ctx, entries, n, v);
+            if (rc != UFSECP_OK) return rc;
+        }
+        size_t total = 0;
+        for (size_t i = 0; i < n; ++i) {
+            if (v[i]) continue;
+            if (total < cap) invalid_out[total] = i;
+            ++total;
+        }
+        *invalid_count = total;
+        return UFSECP_OK;
+    });
 }
 
 }  // extern "C"

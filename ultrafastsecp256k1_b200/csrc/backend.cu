@@ -10,6 +10,7 @@
 
 #include "batch.h"
 #include "kernels.h"
+#include "rlc.h"
 
 namespace uf {
 
@@ -115,8 +116,15 @@ void DevBuf::release() {
 
 Backend::Backend() = default;
 
+RlcVerifier& Backend::rlc() {
+    if (!rlc_) rlc_.reset(new RlcVerifier(this));
+    return *rlc_;
+}
+
 Backend::~Backend() {
     batch_.reset();
+    if (dev_ >= 0) cudaSetDevice(dev_);
+    rlc_.reset();
     if (dev_ >= 0) {
         cudaSetDevice(dev_);
         if (stream_) cudaStreamSynchronize(stream_);

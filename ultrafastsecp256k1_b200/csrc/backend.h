@@ -32,6 +32,7 @@ struct DevBuf {
 
 struct VerifyJob;
 class BatchSlot;
+class RlcVerifier;
 
 class Backend {
 public:
@@ -61,6 +62,8 @@ public:
     // Mixed ECDSA / BIP-340 jobs (host buffers) in one persistent-queue launch;
     // synchronous.
     int verify_jobs(const VerifyJob* jobs, size_t n_jobs);
+    // RLC batch verifier of BIP-340 signatures (created on first use).
+    RlcVerifier& rlc();
     int queue_grid() const { return queue_grid_; }
     int diag(uint32_t op, const uint8_t* in, size_t n, uint8_t* out, size_t in_sz, size_t out_sz);
     int imad_peak(double* ops_per_s);
@@ -91,6 +94,7 @@ private:
     DevBuf msgs_, pubs_, sigs_, out_, scratch_;
     int queue_grid_ = 0;
     std::unique_ptr<BatchSlot> batch_;   // slot of the synchronous mixed-batch call
+    std::unique_ptr<RlcVerifier> rlc_;
     int last_err_ = kOk;
     std::string last_msg_ = "OK";
 };

@@ -1,0 +1,705 @@
+// RLC batch verification: device kernels and the host round loop (rlc.h).
+//
+// Memory per call of n items: items 192 B (three affine points), magnitudes
+// 48 B, t_i = a_i s_i 32 B, parse flag 1 B.  Per round of S segments with
+// c-bit windows (W = ceil(129 / c) windows, B = 2^(c-1) buckets per window):
+// one 4-byte entry per non-zero digit (at most (3 len + 2) W per segment),
+// counters and offsets over the K = S W B bucket keys, a Jacobian sum (112 B)
+// per bucket and per chunk of kChunk entries, two per bucket sub-range and one
+// per window.
+#include "rlc.h"
+
+#include <string.h>
+
+#include <algorithm>
+
+#include <cub/device/device_scan.cuh>
+
+#include "dev_tables.cuh"
+#include "kernels.h"
+#include "sign.cuh"
+#include "verify.cuh"
+
+namespace uf {
+
+namespace {
+
+struct RlcItem {
+    uint4 pt[3][4];     // affine R, +-P, +-lambda P (x then y, 8 words each)
+};
+
+struct RlcSeed {
+    uint8_t b[32];
+};
+
+constexpr int kSub = 8;          // buckets per running-sum sub-range
+
+__device__ __forceinline__ void store_aff(uint4* q, const Fe& x, const Fe& y) {
+    q[0] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    q[1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+    q[2] = make_uint4(y.v[0], y.v[1], y.v[2], y.v[3]);
+    q[3] = make_uint4(y.v[4], y.v[5], y.v[6], y.v[7]);
+}
+
+__device__ __forceinline__ void load_aff(const uint4* q, Fe& x, Fe& y) {
+    const uint4 a = q[0], b = q[1], c = q[2], d = q[3];
+    x.v[0] = a.x; x.v[1] = a.y; x.v[2] = a.z; x.v[3] = a.w;
+    x.v[4] = b.x; x.v[5] = b.y; x.v[6] = b.z; x.v[7] = b.w;
+    y.v[0] = c.x; y.v[1] = c.y; y.v[2] = c.z; y.v[3] = c.w;
+    y.v[4] = d.x; y.v[5] = d.y; y.v[6] = d.z; y.v[7] = d.w;
+}
+
+// Jacobian point in global memory: X, Y, Z and the infinity flag (7 x uint4).
+constexpr int kJacQ = 7;
+
+__device__ __forceinline__ void store_jac(uint4* q, const Jac& P) {
+    store_aff(q, P.X, P.Y);
+    q[4] = make_uint4(P.Z.v[0], P.Z.v[1], P.Z.v[2], P.Z.v[3]);
+    q[5] = make_uint4(P.Z.v[4], P.Z.v[5], P.Z.v[6], P.Z.v[7]);
+    q[6] = make_uint4(P.inf ? 1u : 0u, 0u, 0u, 0u);
+}
+
+__device__ __forceinline__ void load_jac(const uint4* q, Jac& P) {
+    load_aff(q, P.X, P.Y);
+    const uint4 a = q[4], b = q[5];
+    P.Z.v[0] = a.x; P.Z.v[1] = a.y; P.Z.v[2] = a.z; P.Z.v[3] = a.w;
+    P.Z.v[4] = b.x; P.Z.v[5] = b.y; P.Z.v[6] = b.z; P.Z.v[7] = b.w;
+    P.inf = q[6].x != 0;
+}
+
+// Signed digit of window w (c bits) of a magnitude m < 2^128 (the recoding of
+// booth_recode in ecmult.cuh with a run-time window width).
+__device__ __forceinline__ int booth_digit(const uint4 m, int w, int c) {
+    const uint32_t k[6] = {m.x, m.y, m.z, m.w, 0u, 0u};
+    const int pos = c * w - 1;
+    const uint32_t mask = (1u << (c + 1)) - 1u;
+    uint32_t raw;
+    if (pos < 0) {
+        raw = (k[0] << 1) & mask;
+    } else {
+        const int li = pos >> 5, off = pos & 31;
+        const uint64_t v = ((uint64_t)k[li + 1] << 32) | k[li];
+        raw = (uint32_t)(v >> off) & mask;
+    }
+    return (int)(raw & 1u) + (int)((raw >> 1) & ((1u << (c - 1)) - 1u)) - (int)((raw >> c) << (c - 1));
+}
+
+// Point pidx of the round: 3 per item, then G / lambda G per segment.
+__device__ __forceinline__ void load_point(uint32_t pidx, const RlcItem* __restrict__ items, uint32_t n3,
+                                           const uint4* __restrict__ gt, Fe& x, Fe& y) {
+    if (pidx < n3) {
+        load_aff(items[pidx / 3u].pt[pidx % 3u], x, y);
+    } else {
+        const GlobalGT G{gt};
+        G.load(((pidx - n3) & 1u) ? kGTab : 0, x, y);
+    }
+}
+
+// ---------------------------------------------------------------- prep --
+// Per item: strict parse (r < p, 0 < s < n, x(P) < p), lift_x of P and R,
+// challenge e, weight a, the three points with their 128-bit magnitudes (GLV
+// signs folded into y) and t = a s mod n.  Items that fail to parse get zero
+// magnitudes and t = 0, so they drop out of the equation; their verdict is 0.
+__global__ void __launch_bounds__(128)
+k_rlc_prep(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ xs, const uint8_t* __restrict__ sigs,
+           uint32_t n, RlcSeed seed, RlcItem* __restrict__ items, uint4* __restrict__ mags,
+           uint32_t* __restrict__ tsc, uint8_t* __restrict__ okb, uint8_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t mw[8], pw[8], sw[16];
+    load_words8(mw, msgs + 32ull * i);
+    load_words8(pw, xs + 32ull * i);
+    load_words8(sw, sigs + 64ull * i);
+    load_words8(sw + 8, sigs + 64ull * i + 32);
+    uint32_t r[8];
+    Sc s;
+    Fe px, py, rx, ry;
+    words_be_to_limbs(r, sw);
+    words_be_to_limbs(s.v, sw + 8);
+    words_be_to_limbs(px.v, pw);
+    bool ok = limbs_lt_p(r) && !sc_is_zero(s) && limbs_lt_n(s.v) && limbs_lt_p(px.v);
+    if (ok) ok = lift_x_parity(py, px, false);
+    if (ok) {
+        for (int k = 0; k < 8; ++k) rx.v[k] = r[k];
+        ok = lift_x_parity(ry, rx, false);
+    }
+    okb[i] = ok ? 1 : 0;
+    out[i] = ok ? 1 : 0;
+    if (!ok) {
+        const uint4 z = make_uint4(0, 0, 0, 0);
+        mags[3ull * i] = z;
+        mags[3ull * i + 1] = z;
+        mags[3ull * i + 2] = z;
+        for (int k = 0; k < 8; ++k) tsc[8ull * i + k] = 0;
+        return;
+    }
+    // the challenge takes the byte strings as big-endian words
+    uint32_t rbe[8], pbe[8], mbe[8], h[8];
+    for (int k = 0; k < 8; ++k) { rbe[k] = bswap32(sw[k]); pbe[k] = bswap32(pw[k]); mbe[k] = bswap32(mw[k]); }
+    bip340_challenge(h, rbe, pbe, mbe);
+    Sc e;
+    for (int k = 0; k < 8; ++k) e.v[k] = h[7 - k];
+    sc_reduce_once(e);
+    // a = SHA-256(seed || le32 i), first 16 bytes as a big-endian integer
+    uint8_t buf[36];
+    for (int k = 0; k < 32; ++k) buf[k] = seed.b[k];
+    for (int k = 0; k < 4; ++k) buf[32 + k] = (uint8_t)(i >> (8 * k));
+    uint32_t ah[8];
+    sha256_iv(ah);
+    sha256_tail(ah, buf, 36, 0);
+    Sc a;
+    a.v[0] = ah[3]; a.v[1] = ah[2]; a.v[2] = ah[1]; a.v[3] = ah[0];
+    for (int k = 4; k < 8; ++k) a.v[k] = 0;
+    if ((a.v[0] | a.v[1] | a.v[2] | a.v[3]) == 0) a.v[0] = 1;
+    Sc ae, t;
+    sc_mul(ae, a, e);
+    sc_mul(t, a, s);
+    GlvSplit g;
+    glv_split(g, ae);
+    Fe beta, yn, lx;
+    fe_beta(beta);
+    store_aff(items[i].pt[0], rx, ry);
+    yn = py;
+    if (g.neg1) { fe_neg(yn, py); fe_normalize(yn); }
+    store_aff(items[i].pt[1], px, yn);
+    yn = py;
+    if (g.neg2) { fe_neg(yn, py); fe_normalize(yn); }
+    fe_mul(lx, px, beta);
+    fe_normalize(lx);
+    store_aff(items[i].pt[2], lx, yn);
+    mags[3ull * i] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
+    mags[3ull * i + 1] = make_uint4(g.k1[0], g.k1[1], g.k1[2], g.k1[3]);
+    mags[3ull * i + 2] = make_uint4(g.k2[0], g.k2[1], g.k2[2], g.k2[3]);
+    for (int k = 0; k < 8; ++k) tsc[8ull * i + k] = t.v[k];
+}
+
+// Round geometry in device memory: seg[2s], seg[2s+1] = first item, length of
+// segment s; pwf[s] = first (point, window) index of segment s, pwf[S] = total.
+struct RoundGeo {
+    const uint32_t* seg;
+    const uint32_t* pwf;
+    uint32_t n_seg;
+    uint32_t n3;             // 3 * items of the call: index of the first generator point
+    int c, W, B, S;          // window bits, windows, buckets per window, sub-ranges per window
+};
+
+// largest k < n with a[k] <= t (a non-decreasing, a[0] = 0 <= t)
+__device__ __forceinline__ uint32_t upper_index(const uint32_t* __restrict__ a, uint32_t n, uint32_t t) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(a + mid) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per segment: sum of t_i and count of unparsed items; then the magnitudes of
+// the two generator points from the GLV split of -sum t_i.
+__global__ void __launch_bounds__(256)
+k_rlc_tsum(RoundGeo g, const uint32_t* __restrict__ tsc, const uint8_t* __restrict__ okb,
+           uint4* __restrict__ segmag, uint8_t* __restrict__ segneg, uint32_t* __restrict__ segbad) {
+    __shared__ uint32_t red[8][256];
+    __shared__ uint32_t bad;
+    const uint32_t s = blockIdx.x, tid = threadIdx.x;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    const uint32_t i0 = g.seg[2 * s], len = g.seg[2 * s + 1];
+    Sc acc;
+    for (int k = 0; k < 8; ++k) acc.v[k] = 0;
+    uint32_t nbad = 0;
+    for (uint32_t i = i0 + tid; i < i0 + len; i += blockDim.x) {
+        Sc t;
+        const uint4* q = reinterpret_cast<const uint4*>(tsc + 8ull * i);
+        const uint4 lo = q[0], hi = q[1];
+        t.v[0] = lo.x; t.v[1] = lo.y; t.v[2] = lo.z; t.v[3] = lo.w;
+        t.v[4] = hi.x; t.v[5] = hi.y; t.v[6] = hi.z; t.v[7] = hi.w;
+        sc_add(acc, acc, t);
+        nbad += okb[i] ? 0u : 1u;
+    }
+    if (nbad) atomicAdd(&bad, nbad);
+    for (int k = 0; k < 8; ++k) red[k][tid] = acc.v[k];
+    __syncthreads();
+    for (uint32_t st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (tid < st) {
+            Sc a, b;
+            for (int k = 0; k < 8; ++k) { a.v[k] = red[k][tid]; b.v[k] = red[k][tid + st]; }
+            sc_add(a, a, b);
+            for (int k = 0; k < 8; ++k) red[k][tid] = a.v[k];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        Sc sum;
+        for (int k = 0; k < 8; ++k) sum.v[k] = red[k][0];
+        sc_neg(sum, sum);
+        GlvSplit gs;
+        glv_split(gs, sum);
+        segmag[2 * s] = make_uint4(gs.k1[0], gs.k1[1], gs.k1[2], gs.k1[3]);
+        segmag[2 * s + 1] = make_uint4(gs.k2[0], gs.k2[1], gs.k2[2], gs.k2[3]);
+        segneg[2 * s] = gs.neg1 ? 1 : 0;
+        segneg[2 * s + 1] = gs.neg2 ? 1 : 0;
+        segbad[s] = bad;
+    }
+}
+
+// One thread per (point, window): pass 0 counts the non-zero digits of every
+// bucket key, pass 1 writes entry = point index | sign << 31 at the bucket's
+// cursor.  Key = (segment * W + window) * B + |digit| - 1.
+__global__ void __launch_bounds__(256)
+k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint4* __restrict__ segmag,
+             const uint8_t* __restrict__ segneg, uint32_t total, uint32_t* __restrict__ counts,
+             uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries, int pass) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const uint32_t s = upper_index(g.pwf, g.n_seg, t);
+    const uint32_t local = t - g.pwf[s];
+    const uint32_t p = local / (uint32_t)g.W, w = local - p * (uint32_t)g.W;
+    const uint32_t len = g.seg[2 * s + 1];
+    uint32_t pidx;
+    uint4 m;
+    bool neg = false;
+    if (p < 3u * len) {
+        pidx = 3u * g.seg[2 * s] + p;
+        m = mags[pidx];
+    } else {
+        const uint32_t j = 2u * s + (p - 3u * len);
+        pidx = g.n3 + j;
+        m = segmag[j];
+        neg = segneg[j] != 0;
+    }
+    const int d = booth_digit(m, (int)w, g.c);
+    if (d == 0) return;
+    const uint32_t key = (s * (uint32_t)g.W + w) * (uint32_t)g.B + (uint32_t)((d < 0 ? -d : d) - 1);
+    if (pass == 0) {
+        atomicAdd(&counts[key], 1u);
+    } else {
+        const uint32_t pos = atomicAdd(&cursor[key], 1u);
+        entries[pos] = pidx | (((d < 0) != neg) ? 0x80000000u : 0u);
+    }
+}
+
+// chunks per key, for the chunk scan; nch[K] = 0
+__global__ void k_rlc_nchunks(const uint32_t* __restrict__ counts, uint32_t K, uint32_t* __restrict__ nch) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) nch[k] = (counts[k] + RlcVerifier::kChunk - 1) / RlcVerifier::kChunk;
+    else if (k == K) nch[k] = 0;
+}
+
+// One thread per chunk of at most kChunk entries of one bucket.  A bucket
+// with a single chunk is written straight to its bucket slot.
+__global__ void __launch_bounds__(128)
+k_rlc_chunks(const uint32_t* __restrict__ coff, uint32_t K, const uint32_t* __restrict__ offsets,
+             const uint32_t* __restrict__ entries, const RlcItem* __restrict__ items, uint32_t n3,
+             const uint4* __restrict__ gt, uint4* __restrict__ partials, uint4* __restrict__ buckets) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= coff[K]) return;
+    const uint32_t key = upper_index(coff, K, t);
+    const uint32_t j = t - coff[key];
+    const uint32_t e0 = offsets[key] + j * RlcVerifier::kChunk;
+    const uint32_t e1 = min(e0 + RlcVerifier::kChunk, offsets[key + 1]);
+    Jac acc;
+    jac_set_inf(acc);
+    for (uint32_t e = e0; e < e1; ++e) {
+        const uint32_t v = entries[e];
+        Fe x, y;
+        load_point(v & 0x7FFFFFFFu, items, n3, gt, x, y);
+        if (v >> 31) fe_neg(y, y);
+        jac_add_aff(acc, x, y);
+    }
+    if (coff[key + 1] - coff[key] == 1) store_jac(buckets + kJacQ * (uint64_t)key, acc);
+    else store_jac(partials + kJacQ * (uint64_t)t, acc);
+}
+
+// Buckets with 0 or >= 2 chunks: infinity, or the sum of their partials.
+__global__ void __launch_bounds__(128)
+k_rlc_bucket_fin(const uint32_t* __restrict__ coff, uint32_t K, const uint4* __restrict__ partials,
+                 uint4* __restrict__ buckets) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    const uint32_t c0 = coff[k], c1 = coff[k + 1];
+    if (c1 - c0 == 1) return;
+    Jac acc, p;
+    jac_set_inf(acc);
+    for (uint32_t c = c0; c < c1; ++c) {
+        load_jac(partials + kJacQ * (uint64_t)c, p);
+        jac_add(acc, p);
+    }
+    store_jac(buckets + kJacQ * (uint64_t)k, acc);
+}
+
+// One thread per (segment, window, sub-range j of m buckets):
+// T_j = sum_b bucket_b, U_j = sum_b (b - j m + 1) bucket_b by running sums.
+__global__ void __launch_bounds__(128)
+k_rlc_wpart(RoundGeo g, const uint4* __restrict__ buckets, uint4* __restrict__ wu, uint4* __restrict__ wt) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.n_seg * (uint32_t)(g.W * g.S)) return;
+    const uint32_t sw = q / (uint32_t)g.S, j = q - sw * (uint32_t)g.S;
+    const int m = g.B / g.S;
+    const uint4* base = buckets + kJacQ * ((uint64_t)sw * g.B + (uint64_t)j * m);
+    Jac run, tot, b;
+    jac_set_inf(run);
+    jac_set_inf(tot);
+    for (int k = m - 1; k >= 0; --k) {
+        load_jac(base + kJacQ * k, b);
+        jac_add(run, b);
+        jac_add(tot, run);
+    }
+    store_jac(wu + kJacQ * (uint64_t)q, tot);
+    store_jac(wt + kJacQ * (uint64_t)q, run);
+}
+
+// One thread per (segment, window): window sum = sum_j U_j + m sum_j j T_j.
+__global__ void __launch_bounds__(128)
+k_rlc_wcomb(RoundGeo g, const uint4* __restrict__ wu, const uint4* __restrict__ wt, uint4* __restrict__ wins) {
+    const uint32_t sw = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sw >= g.n_seg * (uint32_t)g.W) return;
+    const uint64_t q0 = (uint64_t)sw * g.S;
+    Jac acc, run, jt, p;
+    jac_set_inf(acc);
+    jac_set_inf(run);
+    jac_set_inf(jt);
+    for (int j = g.S - 1; j >= 1; --j) {
+        load_jac(wt + kJacQ * (q0 + j), p);
+        jac_add(run, p);
+        jac_add(jt, run);
+    }
+    for (int m = g.B / g.S; m > 1; m >>= 1) jac_dbl(jt);
+    for (int j = 0; j < g.S; ++j) {
+        load_jac(wu + kJacQ * (q0 + j), p);
+        jac_add(acc, p);
+    }
+    jac_add(acc, jt);
+    store_jac(wins + kJacQ * (uint64_t)sw, acc);
+}
+
+// One thread per segment: Horner over the windows; ok = 1 if the sum is
+// infinity, | 2 if the segment holds an item that failed to parse.
+__global__ void __launch_bounds__(64)
+k_rlc_finish(RoundGeo g, const uint4* __restrict__ wins, const uint32_t* __restrict__ segbad,
+             uint8_t* __restrict__ segok) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.n_seg) return;
+    const uint4* base = wins + kJacQ * (uint64_t)s * g.W;
+    Jac acc, w;
+    load_jac(base + kJacQ * (g.W - 1), acc);
+    for (int k = g.W - 2; k >= 0; --k) {
+        for (int d = 0; d < g.c; ++d) jac_dbl(acc);
+        load_jac(base + kJacQ * k, w);
+        jac_add(acc, w);
+    }
+    segok[s] = (uint8_t)((acc.inf ? 1 : 0) | (segbad[s] ? 2 : 0));
+}
+
+__global__ void k_rlc_gather(const uint32_t* __restrict__ idx, uint32_t m, const uint8_t* __restrict__ msgs,
+                             const uint8_t* __restrict__ xs, const uint8_t* __restrict__ sigs, uint8_t* __restrict__ gm,
+                             uint8_t* __restrict__ gx, uint8_t* __restrict__ gs) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const uint64_t i = idx[k];
+    const uint4* a = reinterpret_cast<const uint4*>(msgs + 32 * i);
+    const uint4* b = reinterpret_cast<const uint4*>(xs + 32 * i);
+    const uint4* c = reinterpret_cast<const uint4*>(sigs + 64 * i);
+    uint4* ga = reinterpret_cast<uint4*>(gm + 32ull * k);
+    uint4* gb = reinterpret_cast<uint4*>(gx + 32ull * k);
+    uint4* gc = reinterpret_cast<uint4*>(gs + 64ull * k);
+    ga[0] = a[0]; ga[1] = a[1];
+    gb[0] = b[0]; gb[1] = b[1];
+    gc[0] = c[0]; gc[1] = c[1]; gc[2] = c[2]; gc[3] = c[3];
+}
+
+__global__ void k_rlc_scatter(const uint32_t* __restrict__ idx, uint32_t m, const uint8_t* __restrict__ v,
+                              uint8_t* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) out[idx[k]] = v[k];
+}
+
+// Rows [x 32 | msg 32 | sig 64] -> three arrays, and the reference's parse
+// gate: *first = min over failing rows of (row << 2 | code - 3), code 3 for
+// x >= p, 4 for r >= p or s outside [1, n-1] (the x test comes first).
+__global__ void k_rlc_rows(const uint8_t* __restrict__ rows, uint32_t n, uint8_t* __restrict__ gm,
+                           uint8_t* __restrict__ gx, uint8_t* __restrict__ gs, uint32_t* __restrict__ first) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4* q = reinterpret_cast<const uint4*>(rows + 128ull * i);
+    uint4 v[8];
+    for (int k = 0; k < 8; ++k) v[k] = q[k];
+    uint4* a = reinterpret_cast<uint4*>(gx + 32ull * i);
+    uint4* b = reinterpret_cast<uint4*>(gm + 32ull * i);
+    uint4* c = reinterpret_cast<uint4*>(gs + 64ull * i);
+    a[0] = v[0]; a[1] = v[1];
+    b[0] = v[2]; b[1] = v[3];
+    c[0] = v[4]; c[1] = v[5]; c[2] = v[6]; c[3] = v[7];
+    const uint8_t* row = rows + 128ull * i;
+    uint32_t w[8], lim[8];
+    be32_to_limbs(w, row);
+    uint32_t code = 0;
+    if (!limbs_lt_p(w)) {
+        code = 3;
+    } else {
+        be32_to_limbs(w, row + 64);
+        be32_to_limbs(lim, row + 96);
+        if (!limbs_lt_p(w) || is_zero256(lim) || !limbs_lt_n(lim)) code = 4;
+    }
+    if (code) atomicMin(first, (i << 2) | (code - 3));
+}
+
+inline unsigned grid_for(uint64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace
+
+int rlc_window_bits(uint32_t len) {
+    // cost in mixed-addition units: one per non-zero digit, about 1.5 per
+    // Jacobian addition of the bucket reduction, 0.7 per Horner doubling
+    int best = 4;
+    double best_cost = 1e300;
+    for (int c = 4; c <= 16; ++c) {
+        const int W = (129 + c - 1) / c, B = 1 << (c - 1);
+        const double cost = (3.0 * len + 2.0) * W + 1.5 * 2.0 * W * B * (1.0 + 1.0 / kSub) + 0.7 * (W - 1) * c;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+RlcVerifier::~RlcVerifier() {
+    for (DevBuf* b : {&items_, &mags_, &tsc_, &okb_, &segs_, &segmag_, &segneg_, &segbad_, &counts_, &offsets_,
+                      &cursor_, &nch_, &coff_, &entries_, &partials_, &buckets_, &wu_, &wt_, &wins_, &segok_,
+                      &scan_tmp_, &leaf_idx_, &leaf_m_, &leaf_x_, &leaf_s_, &leaf_out_, &in_m_, &in_x_, &in_s_,
+                      &in_out_, &in_rows_, &gate_})
+        b->release();
+}
+
+int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok) {
+    const uint32_t n_seg = (uint32_t)(seg.size() / 2);
+    const int W = (129 + c - 1) / c, B = 1 << (c - 1), S = B >= kSub ? B / kSub : 1;
+    std::vector<uint32_t> host(3 * (size_t)n_seg + 1);
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n_seg; ++k) {
+        host[2 * k] = seg[2 * k];
+        host[2 * k + 1] = seg[2 * k + 1];
+        host[2 * n_seg + k] = (uint32_t)total;
+        total += (3ull * seg[2 * k + 1] + 2) * (uint64_t)W;
+        if (total >= 0x7FFFFFFFull) return be_->set_error(kErrBadInput, "RLC round too large");
+    }
+    host[3 * (size_t)n_seg] = (uint32_t)total;
+    const uint64_t K = (uint64_t)n_seg * W * B;
+    if (K >= 0x7FFFFFFFull) return be_->set_error(kErrBadInput, "RLC round too large");
+    const uint64_t chunk_cap = total / kChunk + K + 1;
+    size_t scan_bytes = 0;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                                  (int)(K + 1), s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC scan size");
+    if ((e = segs_.ensure(host.size() * 4)) != cudaSuccess || (e = segmag_.ensure(32ull * n_seg)) != cudaSuccess ||
+        (e = segneg_.ensure(2ull * n_seg)) != cudaSuccess || (e = segbad_.ensure(4ull * n_seg)) != cudaSuccess ||
+        (e = counts_.ensure((K + 1) * 4)) != cudaSuccess || (e = offsets_.ensure((K + 1) * 4)) != cudaSuccess ||
+        (e = cursor_.ensure((K + 1) * 4)) != cudaSuccess || (e = nch_.ensure((K + 1) * 4)) != cudaSuccess ||
+        (e = coff_.ensure((K + 1) * 4)) != cudaSuccess ||
+        (e = entries_.ensure(std::max<uint64_t>(total, 1) * 4)) != cudaSuccess ||
+        (e = partials_.ensure(chunk_cap * 112)) != cudaSuccess || (e = buckets_.ensure(K * 112)) != cudaSuccess ||
+        (e = wu_.ensure((uint64_t)n_seg * W * S * 112)) != cudaSuccess ||
+        (e = wt_.ensure((uint64_t)n_seg * W * S * 112)) != cudaSuccess ||
+        (e = wins_.ensure((uint64_t)n_seg * W * 112)) != cudaSuccess || (e = segok_.ensure(n_seg)) != cudaSuccess ||
+        (e = scan_tmp_.ensure(std::max<size_t>(scan_bytes, 16))) != cudaSuccess)
+        return be_->cuda_error(e, "RLC round buffers");
+    uint32_t* d_seg = (uint32_t*)segs_.p;
+    const RoundGeo g{d_seg, d_seg + 2 * n_seg, n_seg, 3u * n_, c, W, B, S};
+    uint32_t* counts = (uint32_t*)counts_.p;
+    uint32_t* offsets = (uint32_t*)offsets_.p;
+    uint32_t* cursor = (uint32_t*)cursor_.p;
+    uint32_t* nch = (uint32_t*)nch_.p;
+    uint32_t* coff = (uint32_t*)coff_.p;
+    const uint4* mags = (const uint4*)mags_.p;
+    // `host` is pageable: the copy is staged before cudaMemcpyAsync returns
+    e = cudaMemcpyAsync(d_seg, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, (K + 1) * 4, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC round set-up");
+    k_rlc_tsum<<<n_seg, 256, 0, s>>>(g, (const uint32_t*)tsc_.p, (const uint8_t*)okb_.p, (uint4*)segmag_.p,
+                                     (uint8_t*)segneg_.p, (uint32_t*)segbad_.p);
+    k_rlc_digits<<<grid_for(total, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
+                                                     (uint32_t)total, counts, nullptr, nullptr, 0);
+    size_t tb = scan_tmp_.cap;
+    e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, counts, offsets, (int)(K + 1), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cursor, offsets, K * 4, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC scan");
+    k_rlc_digits<<<grid_for(total, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
+                                                     (uint32_t)total, nullptr, cursor, (uint32_t*)entries_.p, 1);
+    k_rlc_nchunks<<<grid_for(K + 1, 256), 256, 0, s>>>(counts, (uint32_t)K, nch);
+    tb = scan_tmp_.cap;
+    e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, nch, coff, (int)(K + 1), s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC chunk scan");
+    k_rlc_chunks<<<grid_for(chunk_cap, 128), 128, 0, s>>>(coff, (uint32_t)K, offsets, (const uint32_t*)entries_.p,
+                                                          (const RlcItem*)items_.p, 3u * n_,
+                                                          (const uint4*)be_->gtab(), (uint4*)partials_.p,
+                                                          (uint4*)buckets_.p);
+    k_rlc_bucket_fin<<<grid_for(K, 128), 128, 0, s>>>(coff, (uint32_t)K, (const uint4*)partials_.p,
+                                                      (uint4*)buckets_.p);
+    k_rlc_wpart<<<grid_for((uint64_t)n_seg * W * S, 128), 128, 0, s>>>(g, (const uint4*)buckets_.p, (uint4*)wu_.p,
+                                                                       (uint4*)wt_.p);
+    k_rlc_wcomb<<<grid_for((uint64_t)n_seg * W, 128), 128, 0, s>>>(g, (const uint4*)wu_.p, (const uint4*)wt_.p,
+                                                                  (uint4*)wins_.p);
+    k_rlc_finish<<<grid_for(n_seg, 64), 64, 0, s>>>(g, (const uint4*)wins_.p, (const uint32_t*)segbad_.p,
+                                                   (uint8_t*)segok_.p);
+    e = cudaGetLastError();
+    ok.resize(n_seg);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ok.data(), segok_.p, n_seg, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC round");
+    return kOk;
+}
+
+int RlcVerifier::verify_leaves(const std::vector<uint32_t>& leaves, const uint8_t* d_msgs, const uint8_t* d_xs,
+                               const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats) {
+    std::vector<uint32_t> idx;
+    for (size_t k = 0; k < leaves.size(); k += 2)
+        for (uint32_t i = 0; i < leaves[k + 1]; ++i) idx.push_back(leaves[k] + i);
+    const uint32_t m = (uint32_t)idx.size();
+    if (m == 0) return kOk;
+    cudaError_t e;
+    if ((e = leaf_idx_.ensure(4ull * m)) != cudaSuccess || (e = leaf_m_.ensure(32ull * m)) != cudaSuccess ||
+        (e = leaf_x_.ensure(32ull * m)) != cudaSuccess || (e = leaf_s_.ensure(64ull * m)) != cudaSuccess ||
+        (e = leaf_out_.ensure(m)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC leaf buffers");
+    e = cudaMemcpyAsync(leaf_idx_.p, idx.data(), 4ull * m, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC leaf indices");
+    k_rlc_gather<<<grid_for(m, 256), 256, 0, s>>>((const uint32_t*)leaf_idx_.p, m, d_msgs, d_xs, d_sigs,
+                                                 (uint8_t*)leaf_m_.p, (uint8_t*)leaf_x_.p, (uint8_t*)leaf_s_.p);
+    if ((e = cudaGetLastError()) != cudaSuccess) return be_->cuda_error(e, "RLC gather");
+    const int rc = be_->verify_device(1, (const uint8_t*)leaf_m_.p, (const uint8_t*)leaf_x_.p,
+                                      (const uint8_t*)leaf_s_.p, m, (uint8_t*)leaf_out_.p, s);
+    if (rc != kOk) return rc;
+    k_rlc_scatter<<<grid_for(m, 256), 256, 0, s>>>((const uint32_t*)leaf_idx_.p, m, (const uint8_t*)leaf_out_.p,
+                                                  d_out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return be_->cuda_error(e, "RLC scatter");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return be_->cuda_error(e, "RLC leaves");
+    if (stats) stats->leaf_items += m;
+    return kOk;
+}
+
+int RlcVerifier::verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_t* d_sigs, uint32_t n,
+                        uint32_t batch_size, const uint8_t seed[32], int window_bits, uint8_t* d_out,
+                        uint8_t* h_batch_ok, cudaStream_t s, RlcStats* stats) {
+    if (n == 0) return kOk;
+    if (n > kMaxItems) return be_->set_error(kErrBadInput, "RLC: more than 2^24 items in one call");
+    if (window_bits != 0 && (window_bits < 4 || window_bits > 16))
+        return be_->set_error(kErrBadInput, "RLC: window_bits must be 0 or 4..16");
+    if (((uintptr_t)d_msgs | (uintptr_t)d_xs | (uintptr_t)d_sigs) & 15u)
+        return be_->set_error(kErrBadInput, "device inputs must be 16-byte aligned");
+    if (batch_size == 0 || batch_size > n) batch_size = n;
+    n_ = n;
+    cudaError_t e;
+    if ((e = items_.ensure((uint64_t)n * sizeof(RlcItem))) != cudaSuccess ||
+        (e = mags_.ensure((uint64_t)n * 48)) != cudaSuccess || (e = tsc_.ensure((uint64_t)n * 32)) != cudaSuccess ||
+        (e = okb_.ensure(n)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC item buffers");
+    RlcSeed sd;
+    memcpy(sd.b, seed, 32);
+    k_rlc_prep<<<grid_for(n, 128), 128, 0, s>>>(d_msgs, d_xs, d_sigs, n, sd, (RlcItem*)items_.p, (uint4*)mags_.p,
+                                                (uint32_t*)tsc_.p, (uint8_t*)okb_.p, d_out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return be_->cuda_error(e, "RLC prep");
+    std::vector<uint32_t> seg, next, leaves;
+    for (uint32_t b = 0; b < n; b += batch_size) {
+        seg.push_back(b);
+        seg.push_back(std::min(batch_size, n - b));
+    }
+    int round = 0;
+    while (!seg.empty()) {
+        uint32_t maxlen = 0;
+        for (size_t k = 1; k < seg.size(); k += 2) maxlen = std::max(maxlen, seg[k]);
+        const int c = window_bits > 0 ? window_bits : rlc_window_bits(maxlen);
+        const int rc = run_round(seg, c, s, ok_host_);
+        if (rc != kOk) return rc;
+        if (stats) {
+            stats->rounds++;
+            stats->segments += seg.size() / 2;
+            if (round == 0) stats->window_bits = c;
+        }
+        if (round == 0 && h_batch_ok)
+            for (size_t k = 0; k < ok_host_.size(); ++k) h_batch_ok[k] = ok_host_[k] == 1 ? 1 : 0;
+        size_t n_fail = 0;
+        for (size_t k = 0; k < ok_host_.size(); ++k) n_fail += (ok_host_[k] & 1) ? 0 : 1;
+        // dense failures (most segments of a bisection level fail): stop splitting
+        const bool dense = round > 0 && n_fail >= 8 && 4 * n_fail > 3 * ok_host_.size();
+        next.clear();
+        for (size_t k = 0; k < ok_host_.size(); ++k) {
+            if (ok_host_[k] & 1) continue;
+            const uint32_t st = seg[2 * k], len = seg[2 * k + 1];
+            if (dense || len <= kLeaf) {
+                leaves.push_back(st);
+                leaves.push_back(len);
+            } else {
+                const uint32_t h = len / 2;
+                next.push_back(st);
+                next.push_back(h);
+                next.push_back(st + h);
+                next.push_back(len - h);
+            }
+        }
+        seg.swap(next);
+        ++round;
+    }
+    return verify_leaves(leaves, d_msgs, d_xs, d_sigs, d_out, s, stats);
+}
+
+int RlcVerifier::verify_host(const uint8_t* msgs, const uint8_t* xs, const uint8_t* sigs, uint32_t n,
+                             uint32_t batch_size, const uint8_t seed[32], int window_bits, uint8_t* out,
+                             uint8_t* h_batch_ok, RlcStats* stats) {
+    if (n == 0) return kOk;
+    if (n > kMaxItems) return be_->set_error(kErrBadInput, "RLC: more than 2^24 items in one call");
+    const cudaStream_t s = be_->stream();
+    cudaError_t e;
+    if ((e = in_m_.ensure(32ull * n)) != cudaSuccess || (e = in_x_.ensure(32ull * n)) != cudaSuccess ||
+        (e = in_s_.ensure(64ull * n)) != cudaSuccess || (e = in_out_.ensure(n)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC staging buffers");
+    e = cudaMemcpyAsync(in_m_.p, msgs, 32ull * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in_x_.p, xs, 32ull * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in_s_.p, sigs, 64ull * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC copy in");
+    const int rc = verify((const uint8_t*)in_m_.p, (const uint8_t*)in_x_.p, (const uint8_t*)in_s_.p, n, batch_size,
+                          seed, window_bits, (uint8_t*)in_out_.p, h_batch_ok, s, stats);
+    if (rc != kOk) return rc;
+    e = cudaMemcpyAsync(out, in_out_.p, n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC copy out");
+    return kOk;
+}
+
+int RlcVerifier::verify_entries(const uint8_t* rows, uint32_t n, const uint8_t seed[32], uint8_t* h_out,
+                                int* gate_code, uint32_t* gate_index, RlcStats* stats) {
+    *gate_code = 0;
+    *gate_index = 0;
+    if (n == 0) return kOk;
+    if (n > kMaxItems) return be_->set_error(kErrBadInput, "RLC: more than 2^24 items in one call");
+    const cudaStream_t s = be_->stream();
+    cudaError_t e;
+    if ((e = in_rows_.ensure(128ull * n)) != cudaSuccess || (e = in_m_.ensure(32ull * n)) != cudaSuccess ||
+        (e = in_x_.ensure(32ull * n)) != cudaSuccess || (e = in_s_.ensure(64ull * n)) != cudaSuccess ||
+        (e = in_out_.ensure(n)) != cudaSuccess || (e = gate_.ensure(4)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC staging buffers");
+    uint32_t first = 0xFFFFFFFFu;
+    e = cudaMemcpyAsync(in_rows_.p, rows, 128ull * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(gate_.p, 0xFF, 4, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC copy in");
+    k_rlc_rows<<<grid_for(n, 256), 256, 0, s>>>((const uint8_t*)in_rows_.p, n, (uint8_t*)in_m_.p, (uint8_t*)in_x_.p,
+                                               (uint8_t*)in_s_.p, (uint32_t*)gate_.p);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&first, gate_.p, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC row gate");
+    if (first != 0xFFFFFFFFu) {
+        *gate_code = 3 + (int)(first & 3u);
+        *gate_index = first >> 2;
+        return kOk;
+    }
+    const int rc = verify((const uint8_t*)in_m_.p, (const uint8_t*)in_x_.p, (const uint8_t*)in_s_.p, n, n, seed, 0,
+                          (uint8_t*)in_out_.p, nullptr, s, stats);
+    if (rc != kOk) return rc;
+    e = cudaMemcpyAsync(h_out, in_out_.p, n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC copy out");
+    return kOk;
+}
+
+}  // namespace uf

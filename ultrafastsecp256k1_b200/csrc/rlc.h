@@ -1,0 +1,104 @@
+// BIP-340 batch verification by random linear combination (RLC) on the GPU,
+// with bisection down to per-signature verdicts.
+//
+// Role in the reference: the CPU batch verify schnorr_batch_verify_impl
+// (src/cpu/src/batch_verify.cpp:324-424: strict parse, lift_x of R and P,
+// challenge e, weights a_i = SHA-256(batch_seed || le32 i) (batch_weight :272),
+// one multi-scalar multiplication checked against infinity, Pippenger in
+// src/cpu/src/pippenger.cpp:73) behind ufsecp_schnorr_batch_verify and
+// ufsecp_schnorr_batch_identify_invalid (src/cpu/src/impl/ufsecp_taproot.cpp:703,
+// :849), which re-verifies every item one by one when the batch fails.  Here:
+//
+//  * item i gets the weight a_i = first 16 bytes of SHA-256(seed || le32 i)
+//    (never 0) and the batch equation
+//        sum_i a_i R_i + sum_i (a_i e_i) P_i - (sum_i a_i s_i) G == infinity
+//    is ONE Pippenger multi-scalar multiplication over 3 points per item
+//    (R_i with a_i; P_i and lambda P_i with the two GLV halves of a_i e_i) plus
+//    2 points per segment (G and lambda G with the GLV halves of
+//    -sum a_i s_i), every scalar below 2^128;
+//  * signed c-bit windows: a counting sort places every (point, window) with a
+//    non-zero digit into bucket (segment, window, |digit|); each bucket is
+//    summed in chunks of kChunk points, each window reduced by running sums
+//    over sub-ranges of buckets, windows combined by Horner's rule;
+//  * a failing segment is split in halves and both are checked again (the
+//    per-item data is computed once); segments of at most kLeaf items, or all
+//    failing segments once most of a round fails, are verified per signature by
+//    the plain kernel.  Verdicts equal the per-signature verify item by item
+//    (a false accept needs a 2^-128 event per failing segment).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "backend.h"
+
+namespace uf {
+
+struct RlcStats {
+    uint64_t rounds = 0;          // MSM rounds (the first check and each bisection level)
+    uint64_t segments = 0;        // segments checked by MSM, all rounds
+    uint64_t leaf_items = 0;      // items verified one by one after bisection
+    int window_bits = 0;          // window of the first round
+};
+
+class RlcVerifier {
+public:
+    static constexpr uint32_t kLeaf = 32;      // segments this small are verified per signature
+    static constexpr uint32_t kChunk = 16;     // bucket points summed by one thread
+    static constexpr uint32_t kMaxItems = 1u << 24;
+
+    explicit RlcVerifier(Backend* be) : be_(be) {}
+    ~RlcVerifier();
+
+    // Device-resident BIP-340 items (32-byte messages, 32-byte x-only keys,
+    // 64-byte signatures, 16-byte aligned); batch_size items per batch, the
+    // last batch ragged (0 = one batch).  window_bits 0 = chosen by segment
+    // length, else 4..16.  Writes d_out[i] = 1 / 0 and, if h_batch_ok is not
+    // null, one byte per batch: 1 when every item of the batch is valid.
+    // Synchronous on `s`.
+    int verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_t* d_sigs, uint32_t n, uint32_t batch_size,
+               const uint8_t seed[32], int window_bits, uint8_t* d_out, uint8_t* h_batch_ok, cudaStream_t s,
+               RlcStats* stats);
+
+    // Host buffers: copies the items in, runs verify() and copies the verdicts
+    // back on the backend's stream.
+    int verify_host(const uint8_t* msgs, const uint8_t* xs, const uint8_t* sigs, uint32_t n, uint32_t batch_size,
+                    const uint8_t seed[32], int window_bits, uint8_t* out, uint8_t* h_batch_ok, RlcStats* stats);
+
+    // Rows of the reference batch API, [x(P) 32 | message 32 | signature 64]
+    // (ufsecp_schnorr_batch_verify, src/cpu/src/impl/ufsecp_taproot.cpp:703).
+    // Rows are gated in index order as the reference does: the first row with
+    // x(P) >= p sets *gate_code = 3 (BAD_PUBKEY), one with r >= p or s outside
+    // [1, n-1] sets 4 (BAD_SIG), and *gate_index to that row; then nothing is
+    // verified.  Otherwise *gate_code = 0 and h_out[i] = 1 / 0 per row, all rows
+    // in one RLC batch.
+    int verify_entries(const uint8_t* entries, uint32_t n, const uint8_t seed[32], uint8_t* h_out, int* gate_code,
+                       uint32_t* gate_index, RlcStats* stats);
+
+private:
+    // One MSM check of every segment (start, length pairs); ok[k] bit 0 = the
+    // equation holds, bit 1 = the segment holds an item that failed to parse.
+    int run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok);
+    int verify_leaves(const std::vector<uint32_t>& leaves, const uint8_t* d_msgs, const uint8_t* d_xs,
+                      const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats);
+
+    Backend* be_;
+    uint32_t n_ = 0;
+    // per item
+    DevBuf items_, mags_, tsc_, okb_;
+    // per round
+    DevBuf segs_, segmag_, segneg_, segbad_, counts_, offsets_, cursor_, nch_, coff_, entries_, partials_,
+        buckets_, wu_, wt_, wins_, segok_, scan_tmp_;
+    // leaves
+    DevBuf leaf_idx_, leaf_m_, leaf_x_, leaf_s_, leaf_out_;
+    // host-buffer calls
+    DevBuf in_m_, in_x_, in_s_, in_out_, in_rows_, gate_;
+    std::vector<uint8_t> ok_host_;
+};
+
+// Window bits that minimise the modelled point-addition count for a segment
+// of `len` items.
+int rlc_window_bits(uint32_t len);
+
+}  // namespace uf

@@ -341,11 +341,13 @@ def run_ours(args):
     ecdsa_rate = None
     mixed = None
     rlc = None
+    serving = None
     if rank == 0:
         ecdsa_rate = ecdsa_4096_rate(ctx, torch)
         if not args.no_secondary:
             mixed = bench_mixed(ctx, torch)
             rlc = bench_rlc(ctx, torch)
+            serving = bench_serving(ctx, torch)
 
     # ---- CPU baseline (rank 0, one GPU only) --------------------------------
     cpu = None
@@ -394,7 +396,8 @@ def run_ours(args):
             "clocks": clocks,
             "gpu_launches": args.steps,
             "verdict_agreement": agree / n,
-            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate, "mixed_batches": mixed, "rlc_batch_verify": rlc},
+            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate, "mixed_batches": mixed, "rlc_batch_verify": rlc,
+                          "serving": serving},
         }
         print(json.dumps(line))
     del d_msgs, d_xs, d_sigs, d_out
@@ -546,6 +549,152 @@ def bench_rlc(ctx, torch, n: int = 1 << 20, reps: int = 3):
             "plain": "ufsecp_gpu_ext_schnorr_verify_device, one launch over all items, CUDA events",
             "rlc": "ufsecp_gpu_ext_schnorr_verify_rlc_device (device buffers, wall clock per call)",
             "rows": rows}
+
+
+def serving_pools(ctx, torch, n_s=300_000, n_e=130_000, pool=100_000, seed=5):
+    """Signed item pools for the serving workload: keys drawn Zipf(1.1) from a
+    seeded 100k-key pool, 0.5% one-bit tampering.  Signed on the GPU."""
+    rng = np.random.default_rng(seed)
+    pool_sk = rng.integers(1, 255, (pool, 32), dtype=np.uint8)
+    w = 1.0 / np.arange(1, pool + 1) ** 1.1
+    w /= w.sum()
+    out = {}
+    for kind, n, ps in ((1, n_s, 32), (0, n_e, 33)):
+        sks = pool_sk[rng.choice(pool, size=n, p=w)]
+        msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+        aux = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        d_m, d_k, d_a = dev(msgs), dev(sks), dev(aux)
+        d_p = torch.empty(n * ps, dtype=torch.uint8, device="cuda")
+        d_s = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+        d_ok = torch.empty(n, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        ctx.sign_device(kind, d_m.data_ptr(), d_k.data_ptr(), d_a.data_ptr(), n, d_p.data_ptr(), d_s.data_ptr(),
+                        d_ok.data_ptr(), 0)
+        torch.cuda.ExternalStream(ctx.stream()).synchronize()
+        sigs = d_s.cpu().numpy().reshape(n, 64)
+        expect = np.ones(n, np.uint8)
+        bad = rng.choice(n, size=n // 200, replace=False)
+        for i in bad:
+            bit = int(rng.integers(0, 512))
+            sigs[i, bit // 8] ^= 1 << (bit % 8)
+        expect[bad] = 0
+        out[kind] = (msgs, d_p.cpu().numpy().reshape(n, ps), sigs, expect)
+    return out
+
+
+def serving_requests(pools, rate, duration, seed, fixed_size=None):
+    """Poisson arrivals offering `rate` sigs/s for `duration` s; sizes log-uniform
+    in [1, 4096] (or fixed), 70/30 BIP-340 / ECDSA items per request."""
+    rng = np.random.default_rng(seed)
+    mean_size = 4095 / np.log(4096) if fixed_size is None else fixed_size
+    lam = rate / mean_size
+    t, reqs, off = 0.0, [], {0: 0, 1: 0}
+    while True:
+        t += rng.exponential(1.0 / lam)
+        if t > duration:
+            break
+        size = fixed_size or int(np.clip(np.exp(rng.uniform(0, np.log(4096))), 1, 4096))
+        n_e = int(rng.binomial(size, 0.3))
+        jobs, exp = [], []
+        for kind, n in ((0, n_e), (1, size - n_e)):
+            if n == 0:
+                continue
+            m, p, s, e = pools[kind]
+            lo = off[kind] % (len(m) - 4096)
+            off[kind] += n
+            jobs.append((kind, m[lo:lo + n], p[lo:lo + n], s[lo:lo + n]))
+            exp.append(e[lo:lo + n])
+        reqs.append((t, jobs, exp))
+    return reqs
+
+
+def _pct(v, q):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(q * (len(v) - 1) + 0.5))] if v else None
+
+
+def run_served(uf, reqs, budget=8 << 30):
+    """Submit at the arrival times from one thread, wait from another."""
+    import threading
+    sctx = uf.GpuContext(0)
+    srv = uf.Server(sctx, slots=4, max_launch_items=1 << 16, memory_budget_bytes=budget)
+    # warm the graph buckets
+    for t, jobs, exp in reqs[:8]:
+        srv.wait(srv.submit(jobs))
+    srv.stats(reset=True)
+    ids = [None] * len(reqs)
+    agree = [0]
+    ready = threading.Semaphore(0)
+
+    def waiter():
+        for k in range(len(reqs)):
+            ready.acquire()
+            outs = srv.wait(ids[k], 120_000)
+            agree[0] += sum(int((o == e).sum()) for o, e in zip(outs, reqs[k][2]))
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    t0 = time.perf_counter()
+    for k, (t, jobs, exp) in enumerate(reqs):
+        while time.perf_counter() - t0 < t:
+            pass
+        ids[k] = srv.submit(jobs)
+        ready.release()
+    th.join()
+    st = srv.stats()
+    srv.close()
+    sctx.close()
+    items = sum(len(j[1]) for _, jobs, _ in reqs for j in jobs)
+    return {"sigs_per_s": st["items_done"] / st["span_s"] if st["span_s"] else None,
+            "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3, "max_ms": st["max_us"] / 1e3,
+            "requests": int(st["requests_done"]), "launches": int(st["launches"]),
+            "peak_slots_in_flight": int(st["peak_slots_in_flight"]),
+            "peak_budget_mb": st["peak_budget_bytes"] / 2**20, "verdict_agreement": agree[0] / items}
+
+
+def run_plain(ctx, reqs, limit_s):
+    """The plain kernel under the same arrivals: one synchronous per-kind ABI call
+    per request, in arrival order (a queue, no batching)."""
+    lat, done_items, agree = [], 0, 0
+    t0 = time.perf_counter()
+    t_last = t0
+    for t, jobs, exp in reqs:
+        now = time.perf_counter() - t0
+        if now > limit_s:
+            break
+        while now < t:
+            now = time.perf_counter() - t0
+        for (kind, m, p, s), e in zip(jobs, exp):
+            o = ctx.ecdsa_verify_batch(m, p, s) if kind == 0 else ctx.schnorr_verify_batch(m, p, s)
+            agree += int((o == e).sum())
+            done_items += len(m)
+        t_last = time.perf_counter()
+        lat.append((t_last - t0 - t) * 1e3)
+    span = t_last - t0
+    return {"sigs_per_s": done_items / span if span > 0 else None, "p50_ms": _pct(lat, 0.5),
+            "p99_ms": _pct(lat, 0.99), "max_ms": max(lat) if lat else None, "requests": len(lat),
+            "requests_offered": len(reqs), "verdict_agreement": agree / max(done_items, 1)}
+
+
+def bench_serving(ctx, torch):
+    import ultrafastsecp256k1_b200 as uf
+    pools = serving_pools(ctx, torch)
+    rows = []
+    for rate, dur in ((10_000, 3.0), (100_000, 3.0), (1_000_000, 2.0)):
+        reqs = serving_requests(pools, rate, dur, seed=rate)
+        rows.append({"offered_sigs_per_s": rate, "duration_s": dur, "requests": len(reqs),
+                     "served": run_served(uf, reqs), "plain": run_plain(ctx, reqs, limit_s=dur + 8.0)})
+    reqs = serving_requests(pools, 1_000_000, 2.0, seed=4096, fixed_size=4096)
+    fixed = {"offered_sigs_per_s": 1_000_000, "request_size": 4096, "requests": len(reqs),
+             "served": run_served(uf, reqs)}
+    return {"workload": "Poisson arrivals, request sizes log-uniform [1, 4096], 70/30 BIP-340/ECDSA items, "
+                        "Zipf(1.1) keys from a 100k pool, 0.5% invalid, 8 GiB admission budget",
+            "served": "ufsecp_gpu_ext_server_* (4 slots, continuous batching); latency submit -> verdicts, "
+                      "measured by the server",
+            "plain": "one synchronous ufsecp_gpu_{ecdsa,schnorr}_verify_batch call per request and kind, FIFO; "
+                     "latency arrival -> verdicts (wall clock)",
+            "rates": rows, "fixed_4096": fixed}
 
 
 def ecdsa_4096_rate(ctx, torch):

@@ -117,6 +117,55 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_identify_invalid(ufsecp_g
                                                                         size_t n, size_t* invalid_out,
                                                                         size_t* invalid_count);
 
+/* Serving loop: continuous batching of verify requests (no counterpart in the
+ * reference, which serves one synchronous call per batch).  A request is one
+ * or more jobs (ECDSA and / or BIP-340, host buffers, layouts as above).
+ * submit() returns at once with an id; a scheduler thread packs the oldest
+ * pending requests into persistent-queue launches on `slots` streams as soon
+ * as a slot and the memory budget allow (up to max_launch_items items per
+ * launch; larger requests ride in several launches), so work that arrives
+ * while other launches run overlaps with them on the device.  The request's
+ * buffers must stay valid until wait() on its id returned UFSECP_OK; its
+ * verdicts are then in out_results and equal the per-kind verify calls' for
+ * every item, whatever it was batched with.  wait() returns
+ * UFSECP_ERR_GPU_QUEUE on timeout (the request stays pending).  While a server
+ * runs, its context belongs to the server's thread: make no other call on that
+ * context.  Destroy the server (it finishes the pending requests) before the
+ * context.  The memory budget covers the slots' fixed staging (pinned + device,
+ * reserved at creation; fewer slots are made if they do not fit) plus the
+ * staged bytes of the items in flight; pending requests wait for room.
+ * Config NULL = defaults: 4 slots, 65,536 items per launch, an 8 GiB budget,
+ * no batch window. */
+typedef struct ufsecp_gpu_ext_server ufsecp_gpu_ext_server;
+typedef struct {
+    uint32_t slots;                 /* streams / launches in flight, 1..64 */
+    uint32_t max_launch_items;      /* 1..65536 */
+    uint64_t memory_budget_bytes;
+    uint32_t batch_window_us;       /* 0: launch as soon as a slot is free */
+    uint32_t reserved;              /* 0 */
+} ufsecp_gpu_ext_server_config_t;
+typedef struct {
+    uint64_t requests_done, items_done, launches;
+    uint64_t peak_budget_bytes;               /* slot staging + item bytes in flight, <= the budget */
+    uint64_t reserved_bytes;                  /* the slots' fixed staging (pinned + device) */
+    uint64_t pending_requests;
+    uint32_t peak_slots_in_flight, reserved;
+    double p50_us, p99_us, max_us, mean_us;   /* submit -> verdicts written, completed requests */
+    double busy_s, span_s;                    /* time with a launch in flight; first submit -> last completion */
+} ufsecp_gpu_ext_server_stats_t;
+
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_create(ufsecp_gpu_ctx* ctx,
+                                                       const ufsecp_gpu_ext_server_config_t* config,
+                                                       ufsecp_gpu_ext_server** server_out);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_submit(ufsecp_gpu_ext_server* server,
+                                                       const ufsecp_gpu_ext_job_t* jobs, size_t n_jobs,
+                                                       uint64_t* request_id);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_wait(ufsecp_gpu_ext_server* server, uint64_t request_id,
+                                                     uint32_t timeout_ms);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_stats(ufsecp_gpu_ext_server* server,
+                                                      ufsecp_gpu_ext_server_stats_t* out, int reset);
+UFSECP_API void ufsecp_gpu_ext_server_destroy(ufsecp_gpu_ext_server* server);
+
 /* Batch signing for synthetic workloads (device pointers, asynchronous on
  * `stream`): kind 0 = ECDSA, RFC 6979 nonce, low-S compact r||s, 33-byte
  * compressed pubkeys out; kind 1 = BIP-340 with aux_rand (d_aux32), 32-byte

@@ -54,6 +54,21 @@ class Job(ctypes.Structure):
                 ("msg_hashes32", _vp), ("pubkeys", _vp), ("sigs64", _vp), ("out_results", _vp)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("max_launch_items", ctypes.c_uint32),
+                ("memory_budget_bytes", ctypes.c_uint64), ("batch_window_us", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests_done", ctypes.c_uint64), ("items_done", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("peak_budget_bytes", ctypes.c_uint64), ("reserved_bytes", ctypes.c_uint64),
+                ("pending_requests", ctypes.c_uint64),
+                ("peak_slots_in_flight", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double), ("max_us", ctypes.c_double),
+                ("mean_us", ctypes.c_double), ("busy_s", ctypes.c_double), ("span_s", ctypes.c_double)]
+
+
 class DeviceInfo(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 128), ("global_mem_bytes", ctypes.c_uint64),
                 ("compute_units", ctypes.c_uint32), ("max_clock_mhz", ctypes.c_uint32),
@@ -98,6 +113,12 @@ _SIGS = {
                                                          ctypes.c_int, _vp, _vp]),
     "ufsecp_gpu_ext_schnorr_verify_rlc_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t,
                                                                 _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "ufsecp_gpu_ext_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]),
+    "ufsecp_gpu_ext_server_submit": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_size_t,
+                                                    ctypes.POINTER(ctypes.c_uint64)]),
+    "ufsecp_gpu_ext_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_server_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats), ctypes.c_int]),
+    "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_schnorr_batch_verify": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
     "ufsecp_gpu_ext_schnorr_batch_identify_invalid": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t,
@@ -372,3 +393,75 @@ class GpuContext:
         out = np.zeros(n * osz, np.uint8)
         self._check(self.L.ufsecp_gpu_ext_diag(self._ctx, op, _ptr(a), n, _ptr(out)), "ext_diag")
         return out.reshape(n, osz)
+
+
+class Server:
+    """Serving loop over one context (ufsecp_gpu_ext_server_*): submit requests
+    of ECDSA / BIP-340 jobs from any thread, wait for their verdicts."""
+
+    def __init__(self, ctx: GpuContext, slots: int = 4, max_launch_items: int = 1 << 16,
+                 memory_budget_bytes: int = 8 << 30, batch_window_us: int = 0):
+        self.L = ctx.L
+        self._ctx = ctx
+        cfg = ServerConfig(slots, max_launch_items, memory_budget_bytes, batch_window_us, 0)
+        h = _vp()
+        rc = self.L.ufsecp_gpu_ext_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h))
+        if rc != UFSECP_OK:
+            raise UfsecpError(rc, "server_create", ctx.last_error_msg())
+        self._h = h
+        self._keep = {}
+
+    def submit(self, jobs) -> int:
+        """jobs = [(kind, msgs, pubs, sigs), ...]; returns the request id.  The verdict
+        arrays are returned by wait()."""
+        arr = (Job * max(1, len(jobs)))()
+        keep, outs = [], []
+        for k, (kind, msgs, pubs, sigs) in enumerate(jobs):
+            m = np.ascontiguousarray(np.asarray(msgs, np.uint8)).reshape(-1)
+            n = m.size // 32
+            p = _buf(pubs, (33 if kind == 0 else 32) * n, "pubkeys")
+            s = _buf(sigs, 64 * n, "sigs64")
+            o = np.zeros(n, np.uint8)
+            keep += [m, p, s]
+            outs.append(o)
+            arr[k] = Job(kind, 0, n, _ptr(m) if n else None, _ptr(p) if n else None, _ptr(s) if n else None,
+                         _ptr(o) if n else None)
+        rid = ctypes.c_uint64()
+        rc = self.L.ufsecp_gpu_ext_server_submit(self._h, arr, len(jobs), ctypes.byref(rid))
+        if rc != UFSECP_OK:
+            raise UfsecpError(rc, "server_submit")
+        self._keep[rid.value] = (keep, outs, arr)
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = 60_000):
+        """Verdict arrays of request `rid`, one per job."""
+        rc = self.L.ufsecp_gpu_ext_server_wait(self._h, rid, timeout_ms)
+        if rc != UFSECP_OK:
+            raise UfsecpError(rc, "server_wait")
+        keep, outs, arr = self._keep.pop(rid)
+        return outs
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServerStats()
+        rc = self.L.ufsecp_gpu_ext_server_stats(self._h, ctypes.byref(st), 1 if reset else 0)
+        if rc != UFSECP_OK:
+            raise UfsecpError(rc, "server_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_ if f != "reserved"}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.L.ufsecp_gpu_ext_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -19,6 +19,7 @@
 #include "backend.h"
 #include "batch.h"
 #include "rlc.h"
+#include "server.h"
 #include "ufsecp/ufsecp_gpu.h"
 #include "ufsecp/ufsecp_gpu_ext.h"
 
@@ -27,6 +28,10 @@ struct ufsecp_gpu_ctx {
     uint32_t backend_id;
     uint32_t device_index;
     uf::RlcStats rlc_stats;      // of the last RLC call
+};
+
+struct ufsecp_gpu_ext_server {
+    std::unique_ptr<uf::Server> server;
 };
 
 namespace {
@@ -669,6 +674,89 @@ ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_identify_invalid(ufsecp_gpu_ctx* ctx
         *invalid_count = total;
         return UFSECP_OK;
     });
+}
+
+// ---- serving loop -------------------------------------------------------------
+
+ufsecp_error_t ufsecp_gpu_ext_server_create(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_server_config_t* config,
+                                            ufsecp_gpu_ext_server** server_out) {
+    if (!ctx || !server_out) return UFSECP_ERR_NULL_ARG;
+    *server_out = nullptr;
+    return guarded([&]() -> ufsecp_error_t {
+        uf::ServerConfig cfg;
+        if (config) {
+            cfg.slots = config->slots;
+            cfg.max_launch_items = config->max_launch_items;
+            cfg.memory_budget_bytes = config->memory_budget_bytes;
+            cfg.batch_window_us = config->batch_window_us;
+        }
+        cudaError_t e = cudaSetDevice(ctx->backend->device());
+        if (e != cudaSuccess) return ctx->backend->cuda_error(e, "cudaSetDevice");
+        std::unique_ptr<ufsecp_gpu_ext_server> s(new ufsecp_gpu_ext_server());
+        s->server.reset(new uf::Server(ctx->backend.get()));
+        const int rc = s->server->start(cfg);
+        if (rc != UFSECP_OK) return rc;
+        *server_out = s.release();
+        return UFSECP_OK;
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_server_submit(ufsecp_gpu_ext_server* server, const ufsecp_gpu_ext_job_t* jobs,
+                                            size_t n_jobs, uint64_t* request_id) {
+    if (!server || !request_id || (n_jobs && !jobs)) return UFSECP_ERR_NULL_ARG;
+    size_t total = 0;
+    for (size_t j = 0; j < n_jobs; ++j) {
+        const ufsecp_gpu_ext_job_t& J = jobs[j];
+        if (J.kind > 1) return UFSECP_ERR_BAD_INPUT;
+        if (J.count == 0) continue;
+        if (!J.msg_hashes32 || !J.pubkeys || !J.sigs64 || !J.out_results) return UFSECP_ERR_NULL_ARG;
+        total += J.count;
+    }
+    if (total > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    return guarded([&]() -> ufsecp_error_t {
+        std::vector<uf::VerifyJob> v;
+        v.reserve(n_jobs);
+        for (size_t j = 0; j < n_jobs; ++j) {
+            clear_out(jobs[j].out_results, jobs[j].count, 1);
+            v.push_back(uf::VerifyJob{(int)jobs[j].kind, jobs[j].count, jobs[j].msg_hashes32, jobs[j].pubkeys,
+                                      jobs[j].sigs64, jobs[j].out_results});
+        }
+        return server->server->submit(v.data(), v.size(), request_id);
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_server_wait(ufsecp_gpu_ext_server* server, uint64_t request_id, uint32_t timeout_ms) {
+    if (!server) return UFSECP_ERR_NULL_ARG;
+    return guarded([&]() -> ufsecp_error_t { return server->server->wait(request_id, timeout_ms); });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_server_stats(ufsecp_gpu_ext_server* server, ufsecp_gpu_ext_server_stats_t* out,
+                                           int reset) {
+    if (!server || !out) return UFSECP_ERR_NULL_ARG;
+    uf::ServerStats s;
+    server->server->stats(&s, reset != 0);
+    memset(out, 0, sizeof(*out));
+    out->requests_done = s.requests_done;
+    out->items_done = s.items_done;
+    out->launches = s.launches;
+    out->peak_budget_bytes = s.peak_budget_bytes;
+    out->reserved_bytes = s.reserved_bytes;
+    out->pending_requests = s.pending_requests;
+    out->peak_slots_in_flight = s.peak_slots_in_flight;
+    out->p50_us = s.p50_us;
+    out->p99_us = s.p99_us;
+    out->max_us = s.max_us;
+    out->mean_us = s.mean_us;
+    out->busy_s = s.busy_s;
+    out->span_s = s.span_s;
+    return UFSECP_OK;
+}
+
+void ufsecp_gpu_ext_server_destroy(ufsecp_gpu_ext_server* server) {
+    try {
+        delete server;
+    } catch (...) {
+    }
 }
 
 }  // extern "C"

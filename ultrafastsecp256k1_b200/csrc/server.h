@@ -1,0 +1,120 @@
+// Serving loop: continuous batching of verify requests on one device.
+//
+// No reference counterpart (the reference serves one synchronous call per
+// caller batch, src/cpu/src/ufsecp_gpu_impl.cpp:317-408).  Requests (each one
+// or more ECDSA / BIP-340 jobs in host memory) are submitted from any thread
+// and return at once with an id.  One scheduler thread owns `slots` batch
+// slots (each its own stream, pinned staging and CUDA graphs, batch.h):
+// whenever a slot is free it packs the oldest pending requests, up to
+// max_launch_items items, into one persistent-queue launch, so requests that
+// arrive while others run are admitted as soon as a slot and memory free up,
+// and their launches overlap on the device.  A request larger than
+// max_launch_items is cut into pieces that ride in successive launches.
+// Admission is bounded by a memory budget: the slots' fixed staging (pinned +
+// device, reserved at start) plus the staged bytes of the items of every launch
+// in flight stay within memory_budget_bytes.  The verdicts
+// of a request are the per-kind verify's, whatever it is batched with.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "backend.h"
+#include "batch.h"
+
+namespace uf {
+
+struct ServerConfig {
+    uint32_t slots = 4;
+    uint32_t max_launch_items = 1u << 16;
+    uint64_t memory_budget_bytes = 8ull << 30;
+    uint32_t batch_window_us = 0;     // wait this long for more work before launching a small batch
+};
+
+struct ServerStats {
+    uint64_t requests_done = 0;
+    uint64_t items_done = 0;
+    uint64_t launches = 0;
+    double p50_us = 0, p99_us = 0, max_us = 0, mean_us = 0;
+    double busy_s = 0;                // wall time with at least one launch in flight
+    double span_s = 0;                // first submit to last completion
+    uint64_t peak_budget_bytes = 0;   // reserved staging + item bytes in flight, at most the budget
+    uint64_t reserved_bytes = 0;      // the slots' fixed staging (pinned + device)
+    uint32_t peak_slots_in_flight = 0;
+    uint64_t pending_requests = 0;
+};
+
+class Server {
+public:
+    explicit Server(Backend* be) : be_(be) {}
+    ~Server();
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    int start(const ServerConfig& cfg);
+    // Thread-safe.  The jobs' host buffers must stay valid until wait() for
+    // this id has returned kOk; the verdicts are written into jobs[j].out.
+    int submit(const VerifyJob* jobs, size_t n_jobs, uint64_t* id);
+    // Thread-safe.  kOk once the request is complete (its record is then
+    // released), kErrGpuQueue on timeout, kErrBadInput for an unknown id; a
+    // launch failure is returned as its error code.
+    int wait(uint64_t id, uint32_t timeout_ms);
+    // Latency percentiles over the requests completed since the last reset.
+    void stats(ServerStats* out, bool reset);
+
+private:
+    using Clock = std::chrono::steady_clock;
+
+    struct Request {
+        uint64_t id = 0;
+        std::vector<VerifyJob> jobs;
+        size_t items = 0;
+        size_t next_job = 0, next_item = 0;      // first piece not yet launched
+        uint32_t pieces_in_flight = 0;
+        bool all_launched = false, done = false;
+        int status = kOk;
+        Clock::time_point t_submit;
+    };
+    struct Launch {
+        std::unique_ptr<BatchSlot> slot;
+        std::vector<VerifyJob> jobs;       // pieces of requests, in order
+        std::vector<Request*> owners;      // owner of each piece
+        size_t bytes = 0;
+        bool busy = false;
+    };
+
+    void loop();
+    bool admit(Launch& L);               // under mu_
+    void complete(Launch& L, int rc);    // under mu_
+    static size_t bytes_per_item(int kind) { return 2 * (32 + (kind == 0 ? 33 : 32) + 64 + 1); }
+
+    Backend* be_;
+    ServerConfig cfg_;
+    std::thread thread_;
+    std::mutex mu_;
+    std::condition_variable cv_work_, cv_done_;
+    bool stop_ = false, started_ = false;
+    uint64_t next_id_ = 1;
+    std::deque<Request*> pending_;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs_;
+    std::vector<Launch> launches_;
+    uint64_t budget_used_ = 0, reserved_ = 0;
+    // statistics
+    std::vector<double> lat_us_;
+    uint64_t items_done_ = 0, n_launches_ = 0, peak_budget_ = 0;
+    uint32_t peak_in_flight_ = 0;
+    double busy_s_ = 0;
+    bool have_first_ = false;
+    Clock::time_point t_first_submit_, t_last_done_, t_busy_since_;
+    uint32_t in_flight_ = 0;
+};
+
+}  // namespace uf

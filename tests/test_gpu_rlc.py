@@ -15,8 +15,6 @@ ufsecp_schnorr_batch_identify_invalid (src/cpu/src/impl/ufsecp_taproot.cpp:703,
 :849) on the same 128-byte rows: return codes, the parse gate's order and the
 invalid indices.
 """
-import math
-
 import numpy as np
 import pytest
 
@@ -30,6 +28,24 @@ SEED = bytes(range(32))
 
 def _flip(msgs, i, byte=5, bit=4):
     msgs[i, byte] ^= 1 << bit
+
+
+def _bisection(n, bad, leaf=32, fanout=8):
+    """Rounds and leaf items of the verifier's split policy for one invalid item."""
+    rounds, leaves, segs = 0, 0, [(0, n)]
+    while segs:
+        rounds += 1
+        nxt = []
+        for st, ln in segs:
+            if not st <= bad < st + ln:
+                continue
+            if ln <= leaf:
+                leaves += ln
+                continue
+            parts = min(fanout, ln)
+            nxt += [(st + ln * q // parts, ln * (q + 1) // parts - ln * q // parts) for q in range(parts)]
+        segs = nxt
+    return rounds, leaves
 
 
 @pytest.mark.parametrize("bad", [0, 1])
@@ -46,9 +62,9 @@ def test_rlc_one_batch(gpu_ctx, oracle, n, bad):
     assert bok.tolist() == [0 if bad else 1]
     st = gpu_ctx.rlc_stats()
     if bad:
-        # halving down to the 32-item leaf that holds the invalid item
-        assert st["rounds"] == 1 + int(math.log2(n // 32))
-        assert st["leaf_items"] == 32
+        # eight-way splits down to the leaf (<= 32 items) that holds the invalid item
+        rounds, leaf = _bisection(n, int(np.flatnonzero(want == 0)[0]))
+        assert st["rounds"] == rounds and st["leaf_items"] == leaf
     else:
         assert st["rounds"] == 1 and st["leaf_items"] == 0 and st["segments"] == 1
 

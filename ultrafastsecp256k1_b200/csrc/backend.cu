@@ -16,7 +16,7 @@ namespace uf {
 
 namespace {
 // Items per host->device chunk: bounds device memory at ~130 B x 2^22 = 0.5 GB.
-constexpr size_t kChunk = size_t{1} << 22;
+constexpr size_t kPipeChunk = size_t{1} << 17;   // items per staging slot of a host-buffer call
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
                                                      launch_verify_v3, launch_verify_v4, launch_verify_v5};
@@ -133,6 +133,13 @@ Backend::~Backend() {
         sigs_.release();
         out_.release();
         scratch_.release();
+        for (int j = 0; j < 2; ++j) {
+            if (pstream_[j]) cudaStreamSynchronize(pstream_[j]);
+            pstage_[j].release();
+            dstage_[j].release();
+            if (pev_[j]) cudaEventDestroy(pev_[j]);
+            if (pstream_[j]) cudaStreamDestroy(pstream_[j]);
+        }
         if (d_gtab_) cudaFree(d_gtab_);
         if (stream_) cudaStreamDestroy(stream_);
     }
@@ -208,30 +215,60 @@ int Backend::verify_host(int kind, const uint8_t* msgs, const uint8_t* pubs, con
     if (count == 0) return kOk;
     cudaError_t e = cudaSetDevice(dev_);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
-    const size_t pub_sz = kind == 0 ? 33 : 32;
-    const size_t chunk = std::min(count, kChunk);
-    if ((e = msgs_.ensure(chunk * 32)) != cudaSuccess) return cuda_error(e, "cudaMalloc(msgs)");
-    if ((e = pubs_.ensure(chunk * pub_sz)) != cudaSuccess) return cuda_error(e, "cudaMalloc(pubs)");
-    if ((e = sigs_.ensure(chunk * 64)) != cudaSuccess) return cuda_error(e, "cudaMalloc(sigs)");
-    if ((e = out_.ensure(chunk)) != cudaSuccess) return cuda_error(e, "cudaMalloc(out)");
-    uint8_t* dm = (uint8_t*)msgs_.p;
-    uint8_t* dp = (uint8_t*)pubs_.p;
-    uint8_t* ds = (uint8_t*)sigs_.p;
-    uint8_t* dout = (uint8_t*)out_.p;
-    for (size_t off = 0; off < count; off += chunk) {
-        const size_t m = std::min(chunk, count - off);
-        if ((e = cudaMemcpyAsync(dm, msgs + off * 32, m * 32, cudaMemcpyHostToDevice, stream_)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(dp, pubs + off * pub_sz, m * pub_sz, cudaMemcpyHostToDevice, stream_)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(ds, sigs + off * 64, m * 64, cudaMemcpyHostToDevice, stream_)) != cudaSuccess)
-            return cuda_error(e, "host->device copy");
-        if (collect && (e = cudaMemcpyAsync(dout, out + off, m, cudaMemcpyHostToDevice, stream_)) != cudaSuccess)
-            return cuda_error(e, "host->device copy");
-        e = launch_verify(kind, dm, dp, ds, (uint32_t)m, dout, collect, stream_);
-        if (e != cudaSuccess) return cuda_error(e, "verify launch");
-        if ((e = cudaMemcpyAsync(out + off, dout, m, cudaMemcpyDeviceToHost, stream_)) != cudaSuccess)
-            return cuda_error(e, "device->host copy");
+    if (!pstream_[0]) {
+        for (int j = 0; j < 2 && e == cudaSuccess; ++j) {
+            e = cudaStreamCreateWithFlags(&pstream_[j], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pev_[j], cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) return cuda_error(e, "pipeline streams");
     }
-    if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return cuda_error(e, "verify");
+    // Chunks of up to kPipeChunk items alternate between two pinned staging
+    // slots: the CPU packs chunk k + 1 (and unpacks chunk k - 1's verdicts)
+    // while the device copies in and verifies chunk k.  Per chunk the slot is
+    // laid out msgs | keys | sigs (16-byte aligned) | verdicts, copied in and
+    // out with one transfer each way.
+    const size_t pub_sz = kind == 0 ? 33 : 32;
+    const size_t sub = std::min(count, kPipeChunk);
+    auto a16 = [](size_t v) { return (v + 15) & ~size_t{15}; };
+    const size_t slot_bytes = a16(sub * (32 + pub_sz)) + sub * 64 + sub + 16;
+    for (int j = 0; j < 2; ++j) {
+        if ((e = pstage_[j].ensure(slot_bytes)) != cudaSuccess) return cuda_error(e, "cudaHostAlloc(staging)");
+        if ((e = dstage_[j].ensure(slot_bytes)) != cudaSuccess) return cuda_error(e, "cudaMalloc(staging)");
+    }
+    size_t pend_off[2] = {0, 0}, pend_n[2] = {0, 0}, pend_out[2] = {0, 0};
+    auto drain = [&](int j) -> cudaError_t {
+        if (!pend_n[j]) return cudaSuccess;
+        const cudaError_t r = cudaEventSynchronize(pev_[j]);
+        if (r == cudaSuccess) memcpy(out + pend_off[j], (const uint8_t*)pstage_[j].p + pend_out[j], pend_n[j]);
+        pend_n[j] = 0;
+        return r;
+    };
+    size_t k = 0;
+    for (size_t off = 0; off < count; off += sub, ++k) {
+        const int j = (int)(k & 1);
+        if ((e = drain(j)) != cudaSuccess) return cuda_error(e, "verify");
+        const size_t m = std::min(sub, count - off);
+        const size_t o_p = m * 32, o_s = a16(o_p + m * pub_sz), o_o = o_s + m * 64;
+        uint8_t* h = (uint8_t*)pstage_[j].p;
+        uint8_t* d = (uint8_t*)dstage_[j].p;
+        memcpy(h, msgs + off * 32, m * 32);
+        memcpy(h + o_p, pubs + off * pub_sz, m * pub_sz);
+        memcpy(h + o_s, sigs + off * 64, m * 64);
+        if (collect) memcpy(h + o_o, out + off, m);
+        const size_t in_bytes = o_o + (collect ? m : 0);
+        if ((e = cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, pstream_[j])) != cudaSuccess)
+            return cuda_error(e, "host->device copy");
+        e = launch_verify(kind, d, d + o_p, d + o_s, (uint32_t)m, d + o_o, collect, pstream_[j]);
+        if (e != cudaSuccess) return cuda_error(e, "verify launch");
+        if ((e = cudaMemcpyAsync(h + o_o, d + o_o, m, cudaMemcpyDeviceToHost, pstream_[j])) != cudaSuccess)
+            return cuda_error(e, "device->host copy");
+        if ((e = cudaEventRecord(pev_[j], pstream_[j])) != cudaSuccess) return cuda_error(e, "event record");
+        pend_off[j] = off;
+        pend_n[j] = m;
+        pend_out[j] = o_o;
+    }
+    for (int j = 0; j < 2; ++j)
+        if ((e = drain(j)) != cudaSuccess) return cuda_error(e, "verify");
     clear_error();
     return kOk;
 }

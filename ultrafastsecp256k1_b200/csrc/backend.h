@@ -30,6 +30,14 @@ struct DevBuf {
     void release();
 };
 
+// Pinned (page-locked) host buffer, grow-only.
+struct HostBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
 struct VerifyJob;
 class BatchSlot;
 class RlcVerifier;
@@ -92,6 +100,12 @@ private:
     cudaStream_t stream_ = nullptr;
     void* d_gtab_ = nullptr;
     DevBuf msgs_, pubs_, sigs_, out_, scratch_;
+    // host-buffer calls: two pinned staging slots, each with its own stream,
+    // so that packing chunk k + 1 on the CPU overlaps verifying chunk k
+    HostBuf pstage_[2];
+    DevBuf dstage_[2];
+    cudaStream_t pstream_[2] = {nullptr, nullptr};
+    cudaEvent_t pev_[2] = {nullptr, nullptr};
     int queue_grid_ = 0;
     std::unique_ptr<BatchSlot> batch_;   // slot of the synchronous mixed-batch call
     std::unique_ptr<RlcVerifier> rlc_;

@@ -33,13 +33,6 @@ struct VerifyJob {
     uint8_t* out;         // count verdict bytes, host memory
 };
 
-struct HostBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t bytes);
-    void release();
-};
-
 class BatchSlot {
 public:
     static constexpr uint32_t kGraphMaxItems = 1u << 16;

@@ -32,7 +32,10 @@ struct RlcSeed {
     uint8_t b[32];
 };
 
-constexpr int kSub = 8;          // buckets per running-sum sub-range
+// Running sums of a window's B buckets are split into S sub-ranges of B / S
+// buckets (one thread each) and the S partial results are combined by one
+// thread; S = 2^floor((c - 1) / 2) balances the two serial chains.
+inline int sub_ranges(int c) { return 1 << ((c - 1) / 2); }
 
 __device__ __forceinline__ void store_aff(uint4* q, const Fe& x, const Fe& y) {
     q[0] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
@@ -455,7 +458,7 @@ int rlc_window_bits(uint32_t len) {
     double best_cost = 1e300;
     for (int c = 4; c <= 16; ++c) {
         const int W = (129 + c - 1) / c, B = 1 << (c - 1);
-        const double cost = (3.0 * len + 2.0) * W + 1.5 * 2.0 * W * B * (1.0 + 1.0 / kSub) + 0.7 * (W - 1) * c;
+        const double cost = (3.0 * len + 2.0) * W + 1.5 * 2.0 * W * B + 0.7 * (W - 1) * c;
         if (cost < best_cost) {
             best_cost = cost;
             best = c;
@@ -474,7 +477,7 @@ RlcVerifier::~RlcVerifier() {
 
 int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok) {
     const uint32_t n_seg = (uint32_t)(seg.size() / 2);
-    const int W = (129 + c - 1) / c, B = 1 << (c - 1), S = B >= kSub ? B / kSub : 1;
+    const int W = (129 + c - 1) / c, B = 1 << (c - 1), S = sub_ranges(c);
     std::vector<uint32_t> host(3 * (size_t)n_seg + 1);
     uint64_t total = 0;
     for (uint32_t k = 0; k < n_seg; ++k) {
@@ -629,12 +632,14 @@ int RlcVerifier::verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_
             if (dense || len <= kLeaf) {
                 leaves.push_back(st);
                 leaves.push_back(len);
-            } else {
-                const uint32_t h = len / 2;
-                next.push_back(st);
-                next.push_back(h);
-                next.push_back(st + h);
-                next.push_back(len - h);
+                continue;
+            }
+            // kFanout near-equal children
+            const uint32_t parts = std::min<uint32_t>(kFanout, len);
+            for (uint32_t q = 0; q < parts; ++q) {
+                const uint32_t a = (uint32_t)((uint64_t)len * q / parts), b = (uint32_t)((uint64_t)len * (q + 1) / parts);
+                next.push_back(st + a);
+                next.push_back(b - a);
             }
         }
         seg.swap(next);

@@ -20,8 +20,10 @@
 //    non-zero digit into bucket (segment, window, |digit|); each bucket is
 //    summed in chunks of kChunk points, each window reduced by running sums
 //    over sub-ranges of buckets, windows combined by Horner's rule;
-//  * a failing segment is split in halves and both are checked again (the
-//    per-item data is computed once); segments of at most kLeaf items, or all
+//  * a failing segment is split into kFanout near-equal children, all checked
+//    again in the next round (the per-item data is computed once; eight-way
+//    splits need half the rounds of halving and less MSM work in total: about
+//    2.1x the batch instead of 3x for one invalid item); segments of at most kLeaf items, or all
 //    failing segments once most of a round fails, are verified per signature by
 //    the plain kernel.  Verdicts equal the per-signature verify item by item
 //    (a false accept needs a 2^-128 event per failing segment).
@@ -46,6 +48,7 @@ class RlcVerifier {
 public:
     static constexpr uint32_t kLeaf = 32;      // segments this small are verified per signature
     static constexpr uint32_t kChunk = 16;     // bucket points summed by one thread
+    static constexpr uint32_t kFanout = 8;     // children of a failing segment
     static constexpr uint32_t kMaxItems = 1u << 24;
 
     explicit RlcVerifier(Backend* be) : be_(be) {}

@@ -117,7 +117,15 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_schnorr_verify_collect(ufsecp_gpu_ctx* ctx,
                                                             const uint8_t* pubkeys_x32, const uint8_t* sigs64,
                                                             size_t count, uint8_t* key_buffer);
 
-/* ref :228 / :236 / :278 / :299 -- consensus row / column surfaces. */
+/* ref :228 / :236 / :278 / :299 -- consensus row / column surfaces.
+ * opaque_rows (lbtc_rows is an alias): rows [msg 32 | compressed pubkey 33 |
+ * opaque signature 64 | tail], stride >= 129 bytes (else BAD_INPUT); the
+ * signature is the libsecp in-memory layout, r then s as 32 little-endian
+ * bytes each, r and s in [1, n-1], high-S accepted (normalised), the verdicts
+ * of the reference CPU's ufsecp_ecdsa_verify_opaque_rows
+ * (src/cpu/src/impl/ufsecp_ecdsa.cpp:412).  ecdsa_lbtc_columns: the same
+ * verdicts from three column arrays.  schnorr_lbtc_columns: the BIP-340
+ * verdicts of ufsecp_gpu_schnorr_verify_batch on the same columns. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ecdsa_verify_opaque_rows(ufsecp_gpu_ctx* ctx, const uint8_t* rows, size_t stride,
                                                               size_t count, uint8_t* out_results);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ecdsa_verify_lbtc_rows(ufsecp_gpu_ctx* ctx, const uint8_t* rows, size_t stride,

@@ -63,6 +63,7 @@ class Oracle:
         for name in ("oracle_ecdsa_verify_batch", "oracle_schnorr_verify_batch"):
             getattr(L, name).argtypes = [_u8p, _u8p, _u8p, ctypes.c_size_t, _u8p]
             getattr(L, name).restype = None
+        L.oracle_ecdsa_verify_opaque_rows.argtypes = [_u8p, ctypes.c_size_t, ctypes.c_size_t, _u8p]
         L.oracle_ecdsa_sign_batch.argtypes = [_u8p, _u8p, ctypes.c_size_t, _u8p, _u8p, _u8p]
         L.oracle_schnorr_sign_batch.argtypes = [_u8p, _u8p, _u8p, ctypes.c_size_t, _u8p, _u8p, _u8p]
         L.oracle_set_threads.argtypes = [ctypes.c_int]
@@ -97,6 +98,15 @@ class Oracle:
         return out
 
     # ---- signing (corpus generation) --------------------------------------
+    def ecdsa_verify_opaque_rows(self, rows, stride: int) -> np.ndarray:
+        """Rows [msg 32 | pubkey 33 | opaque LE r, s 64 | tail], `stride` bytes apart."""
+        rows = _as_u8(rows)
+        n = rows.size // stride
+        out = np.zeros(n, np.uint8)
+        if n:
+            self.L.oracle_ecdsa_verify_opaque_rows(_ptr(rows), stride, n, _ptr(out))
+        return out
+
     def ecdsa_sign_batch(self, msgs, sks):
         msgs, sks = _as_u8(msgs), _as_u8(sks)
         n = msgs.size // 32
@@ -173,6 +183,8 @@ class RefLib:
         L.ufsecp_pubkey_xonly.argtypes = [ctypes.c_void_p, _u8p, _u8p]
         L.ufsecp_schnorr_batch_verify.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t]
         L.ufsecp_schnorr_batch_verify.restype = ctypes.c_int
+        L.ufsecp_ecdsa_verify_opaque_rows.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t, ctypes.c_size_t, _u8p]
+        L.ufsecp_ecdsa_verify_opaque_rows.restype = ctypes.c_int
         L.ufsecp_schnorr_batch_identify_invalid.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t,
                                                            ctypes.POINTER(ctypes.c_size_t),
                                                            ctypes.POINTER(ctypes.c_size_t)]
@@ -250,6 +262,14 @@ class RefLib:
         rc1 = self.L.ufsecp_pubkey_xonly(self.ctx(), _ptr(k), ctypes.cast(xo, _u8p))
         rc2 = self.L.ufsecp_schnorr_sign(self.ctx(), _ptr(m), _ptr(k), _ptr(a), ctypes.cast(sig, _u8p))
         return (bytes(xo), bytes(sig)) if rc1 == 0 and rc2 == 0 else None
+
+    def ecdsa_verify_opaque_rows(self, rows, stride: int):
+        """ufsecp_ecdsa_verify_opaque_rows: (return code, per-row verdicts)."""
+        rows = _as_u8(rows)
+        n = rows.size // stride
+        out = np.zeros(max(n, 1), np.uint8)
+        rc = self.L.ufsecp_ecdsa_verify_opaque_rows(self.ctx(), _ptr(rows), stride, n, _ptr(out))
+        return rc, out[:n]
 
     def schnorr_batch_verify_rows(self, rows128: np.ndarray) -> int:
         """ufsecp_schnorr_batch_verify over 128-byte rows pk|msg|sig (RLC form)."""

@@ -435,6 +435,27 @@ int oracle_ecdsa_verify(const uint8_t msg32[32], const uint8_t pub33[33], const 
     return u256_cmp(&x, &r) == 0;
 }
 
+/* Opaque libsecp-layout ECDSA signature (r then s, each 32 little-endian
+ * bytes) as ufsecp_ecdsa_verify_opaque_rows reads it
+ * (src/cpu/src/impl/ufsecp_ecdsa.cpp:105-117, :128-139, :180-189, :412-452):
+ * r, s in [1, n-1] without reduction, s normalised to low-S (high-S accepted),
+ * then the compact verify. */
+int oracle_ecdsa_verify_opaque(const uint8_t msg32[32], const uint8_t pub33[33], const uint8_t opaque64[64]) {
+    uint8_t be[64];
+    for (int i = 0; i < 32; ++i) { be[i] = opaque64[31 - i]; be[32 + i] = opaque64[63 - i]; }
+    u256 r, sv;
+    u256_from_be(&r, be);
+    u256_from_be(&sv, be + 32);
+    if (u256_is_zero(&r) || u256_cmp(&r, &FN) >= 0) return 0;
+    if (u256_is_zero(&sv) || u256_cmp(&sv, &FN) >= 0) return 0;
+    if (u256_cmp(&sv, &HALF_N) > 0) {
+        u256 t;
+        u256_sub(&t, &FN, &sv);
+        u256_to_be(be + 32, &t);
+    }
+    return oracle_ecdsa_verify(msg32, pub33, be);
+}
+
 /* Returns 1 = valid, 0 = invalid (ufsecp_schnorr_verify == UFSECP_OK). */
 int oracle_schnorr_verify(const uint8_t msg32[32], const uint8_t xonly32[32], const uint8_t sig64[64]) {
     u256 r, s, e, ne;
@@ -621,6 +642,17 @@ void oracle_schnorr_verify_batch(const uint8_t *msgs, const uint8_t *pubs, const
                                  size_t n, uint8_t *out) {
     batch_ctx b = {msgs, pubs, sigs, NULL, NULL, out, NULL, NULL};
     parallel_for((long)n, schnorr_verify_item, &b);
+}
+/* Opaque ECDSA rows [msg 32 | pubkey 33 | opaque sig 64 | tail], `stride` bytes apart. */
+typedef struct { const uint8_t *rows; size_t stride; uint8_t *out; } rows_ctx;
+static void ecdsa_opaque_item(void *c, long i) {
+    rows_ctx *b = (rows_ctx *)c;
+    const uint8_t *row = b->rows + (size_t)i * b->stride;
+    b->out[i] = (uint8_t)oracle_ecdsa_verify_opaque(row, row + 32, row + 65);
+}
+void oracle_ecdsa_verify_opaque_rows(const uint8_t *rows, size_t stride, size_t n, uint8_t *out) {
+    rows_ctx b = {rows, stride, out};
+    parallel_for((long)n, ecdsa_opaque_item, &b);
 }
 /* Signs n items; ok[i] = 1 on success. */
 void oracle_ecdsa_sign_batch(const uint8_t *msgs, const uint8_t *sks, size_t n,

@@ -126,3 +126,45 @@ def schnorr_corpus(oracle, n, seed, tamper=0.01):
     sigs = sigs.reshape(n, 64)
     flip_random_bits(rng, (msgs, sigs), tamper)
     return msgs, xs, sigs
+
+
+def opaque_rows_corpus(oracle, n, seed, stride=129):
+    """ECDSA rows [msg 32 | pubkey 33 | opaque sig 64 | tail] in the libsecp
+    in-memory signature layout (r, s as 32-byte little-endian), with high-S
+    twins, one-bit tampering, r / s = 0, r / s >= n, bad prefixes, x >= p and
+    off-curve keys, and random tail bytes when stride > 129."""
+    rng = np.random.default_rng(seed)
+    msgs, pubs, sigs = ecdsa_corpus(oracle, n, seed, tamper=0.0)
+    opaque = np.concatenate([sigs[:, 31::-1], sigs[:, :31:-1]], axis=1)   # BE r||s -> LE r, LE s
+    rows = rng.integers(0, 256, (n, stride), dtype=np.uint8)
+    rows[:, :32] = msgs
+    rows[:, 32:65] = pubs
+    rows[:, 65:129] = opaque
+    le = lambda v: np.frombuffer(v.to_bytes(32, "little"), np.uint8)
+    for i in range(n):
+        k = i % 12
+        if k == 1:      # high-S twin: accepted on this surface
+            s_ = int.from_bytes(bytes(rows[i, 97:129]), "little")
+            rows[i, 97:129] = le(N - s_)
+        elif k == 2:
+            rows[i, int(rng.integers(0, 32))] ^= 1 << int(rng.integers(0, 8))
+        elif k == 3:
+            rows[i, 65:97] = 0
+        elif k == 4:
+            rows[i, 97:129] = 0
+        elif k == 5:
+            rows[i, 65:97] = le(N + int(rng.integers(0, 1000)))
+        elif k == 6:
+            rows[i, 97:129] = le(N + int(rng.integers(0, 1000)))
+        elif k == 7:
+            rows[i, 32] = 0x04
+        elif k == 8:
+            rows[i, 33:65] = np.frombuffer((P + int(rng.integers(0, 977))).to_bytes(32, "big"), np.uint8)
+        elif k == 9:
+            x = int.from_bytes(bytes(rows[i, 33:65]), "big")
+            while True:
+                x = (x + 1) % P
+                if pow((x ** 3 + 7) % P, (P - 1) // 2, P) != 1:
+                    break
+            rows[i, 33:65] = np.frombuffer(x.to_bytes(32, "big"), np.uint8)
+    return np.ascontiguousarray(rows)

@@ -268,11 +268,15 @@ def test_abi_gating_with_context(gpu_ctx):
     kb = np.full(4, 3, np.uint8)
     assert L.ufsecp_gpu_ecdsa_verify_collect(h, None, None, None, 4, kb.ctypes.data) == uf.UFSECP_ERR_NULL_ARG
     assert (kb == 3).all()
-    # operations outside the verify path report UNSUPPORTED and clear their outputs
+    # invalid inputs are verdicts, not errors (all-zero rows: bad pubkey prefix)
     res = np.full(2, 5, np.uint8)
-    assert L.ufsecp_gpu_ecdsa_verify_lbtc_columns(h, out.ctypes.data, out.ctypes.data, out.ctypes.data, 2,
-                                                  res.ctypes.data) == uf.UFSECP_ERR_GPU_UNSUPPORTED
+    z = np.zeros(2 * 64, np.uint8)
+    assert L.ufsecp_gpu_ecdsa_verify_lbtc_columns(h, z.ctypes.data, z.ctypes.data, z.ctypes.data, 2,
+                                                  res.ctypes.data) == uf.UFSECP_OK
     assert (res == 0).all()
+    # operations outside the verify path report UNSUPPORTED
+    L.ufsecp_gpu_generator_mul_batch.argtypes = [uf._vp, uf._vp, uf.ctypes.c_size_t, uf._vp]
+    assert L.ufsecp_gpu_generator_mul_batch(h, z.ctypes.data, 1, res.ctypes.data) == uf.UFSECP_ERR_GPU_UNSUPPORTED
     assert gpu_ctx.is_ready()
     info = uf.device_info(0)
     assert info.compute_units > 0 and info.global_mem_bytes > 0

@@ -63,6 +63,18 @@ def test_oracle_vs_reference_library(oracle, reflib):
     assert (oracle.schnorr_verify_batch(m, x, s) == reflib.schnorr_verify_batch(m, x, s)).all()
 
 
+@pytest.mark.parametrize("stride", [129, 141])
+def test_opaque_rows_vs_reference_library(oracle, reflib, stride):
+    from conftest import opaque_rows_corpus
+    rows = opaque_rows_corpus(oracle, 600, seed=31 + stride, stride=stride)
+    rc, ref = reflib.ecdsa_verify_opaque_rows(rows, stride)
+    assert rc == 0
+    got = oracle.ecdsa_verify_opaque_rows(rows, stride)
+    assert (got == ref).all()
+    assert 0 < int(got.sum()) < len(got)
+    assert got[1::12].all()          # high-S twins are accepted on this surface
+
+
 def test_oracle_signers_vs_reference_library(oracle, reflib):
     rng = np.random.default_rng(5)
     for i in range(16):

@@ -264,7 +264,15 @@ ufsecp_error_t ufsecp_gpu_ecdsa_verify_opaque_rows(ufsecp_gpu_ctx* ctx, const ui
     if (count > kMaxBatch || stride < 129u) return UFSECP_ERR_BAD_INPUT;
     if (!rows || !out_results) return UFSECP_ERR_NULL_ARG;
     clear_out(out_results, count, 1);
-    return unsupported(ctx, count);
+    try {
+        return finish(ctx->backend->verify_host_strided(2, rows, stride, rows + 32, stride, rows + 65, stride, count,
+                                                        out_results, false),
+                      out_results, count, 1);
+    } catch (const std::bad_alloc&) {
+        return finish(UFSECP_ERR_GPU_MEMORY, out_results, count, 1);
+    } catch (...) {
+        return finish(UFSECP_ERR_INTERNAL, out_results, count, 1);
+    }
 }
 
 ufsecp_error_t ufsecp_gpu_ecdsa_verify_lbtc_rows(ufsecp_gpu_ctx* ctx, const uint8_t* rows, size_t stride, size_t count,
@@ -275,14 +283,17 @@ ufsecp_error_t ufsecp_gpu_ecdsa_verify_lbtc_rows(ufsecp_gpu_ctx* ctx, const uint
 ufsecp_error_t ufsecp_gpu_ecdsa_verify_lbtc_columns(ufsecp_gpu_ctx* ctx, const uint8_t* digests32,
                                                     const uint8_t* pubkeys33, const uint8_t* sigs64, size_t count,
                                                     uint8_t* out_results) {
-    return gated_verify(ctx, digests32, pubkeys33, sigs64, count, out_results,
-                        [&] { return unsupported(ctx, count); });
+    return gated_verify(ctx, digests32, pubkeys33, sigs64, count, out_results, [&] {
+        return ctx->backend->verify_host(2, digests32, pubkeys33, sigs64, count, out_results, false);
+    });
 }
 
 ufsecp_error_t ufsecp_gpu_schnorr_verify_lbtc_columns(ufsecp_gpu_ctx* ctx, const uint8_t* digests32,
                                                       const uint8_t* xonly32, const uint8_t* sigs64, size_t count,
                                                       uint8_t* out_results) {
-    return gated_verify(ctx, digests32, xonly32, sigs64, count, out_results, [&] { return unsupported(ctx, count); });
+    return gated_verify(ctx, digests32, xonly32, sigs64, count, out_results, [&] {
+        return ctx->backend->verify_host(1, digests32, xonly32, sigs64, count, out_results, false);
+    });
 }
 
 // ---- the rest of the reference surface: not implemented here -----------------

@@ -211,6 +211,12 @@ int Backend::verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pub
 
 int Backend::verify_host(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs, size_t count,
                          uint8_t* out, bool collect) {
+    return verify_host_strided(kind, msgs, 32, pubs, kind == 1 ? 32 : 33, sigs, 64, count, out, collect);
+}
+
+int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride, const uint8_t* pubs,
+                                 size_t p_stride, const uint8_t* sigs, size_t s_stride, size_t count, uint8_t* out,
+                                 bool collect) {
     if (!ready_) return set_error(kErrGpuDevice, "context not ready");
     if (count == 0) return kOk;
     cudaError_t e = cudaSetDevice(dev_);
@@ -227,7 +233,7 @@ int Backend::verify_host(int kind, const uint8_t* msgs, const uint8_t* pubs, con
     // while the device copies in and verifies chunk k.  Per chunk the slot is
     // laid out msgs | keys | sigs (16-byte aligned) | verdicts, copied in and
     // out with one transfer each way.
-    const size_t pub_sz = kind == 0 ? 33 : 32;
+    const size_t pub_sz = kind == 1 ? 32 : 33;
     const size_t sub = std::min(count, kPipeChunk);
     auto a16 = [](size_t v) { return (v + 15) & ~size_t{15}; };
     const size_t slot_bytes = a16(sub * (32 + pub_sz)) + sub * 64 + sub + 16;
@@ -251,9 +257,16 @@ int Backend::verify_host(int kind, const uint8_t* msgs, const uint8_t* pubs, con
         const size_t o_p = m * 32, o_s = a16(o_p + m * pub_sz), o_o = o_s + m * 64;
         uint8_t* h = (uint8_t*)pstage_[j].p;
         uint8_t* d = (uint8_t*)dstage_[j].p;
-        memcpy(h, msgs + off * 32, m * 32);
-        memcpy(h + o_p, pubs + off * pub_sz, m * pub_sz);
-        memcpy(h + o_s, sigs + off * 64, m * 64);
+        auto pack = [m, off](uint8_t* dst, const uint8_t* src, size_t width, size_t stride) {
+            if (stride == width) {
+                memcpy(dst, src + off * width, m * width);
+            } else {
+                for (size_t i = 0; i < m; ++i) memcpy(dst + i * width, src + (off + i) * stride, width);
+            }
+        };
+        pack(h, msgs, 32, m_stride);
+        pack(h + o_p, pubs, pub_sz, p_stride);
+        pack(h + o_s, sigs, 64, s_stride);
         if (collect) memcpy(h + o_o, out + off, m);
         const size_t in_bytes = o_o + (collect ? m : 0);
         if ((e = cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, pstream_[j])) != cudaSuccess)

@@ -59,8 +59,13 @@ public:
     int sms() const { return sms_; }
 
     // Host buffers in, host verdicts out; synchronous (the reference contract).
+    // kind 0 ECDSA (compact big-endian r || s, low-S), 1 BIP-340, 2 ECDSA with the
+    // opaque little-endian signature layout (high-S accepted).
     int verify_host(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs, size_t count,
                     uint8_t* out, bool collect);
+    // The same with byte strides between consecutive items of each field (rows).
+    int verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride, const uint8_t* pubs, size_t p_stride,
+                            const uint8_t* sigs, size_t s_stride, size_t count, uint8_t* out, bool collect);
     // Device buffers in / out, asynchronous on `stream` (nullptr = context stream).
     int verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pubs, const uint8_t* d_sigs, size_t count,
                       uint8_t* d_out, cudaStream_t stream);

@@ -27,7 +27,8 @@
 namespace uf {
 namespace UF_CAT(vk, UF_VARIANT) {
 
-template <bool kEcdsa>
+// kKind: 0 ECDSA (compact r || s), 1 BIP-340, 2 ECDSA (opaque little-endian r, s; high-S accepted)
+template <int kKind>
 __global__ void __launch_bounds__(kVerifyThreads)
 k_verify(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs, const uint8_t* __restrict__ sigs,
          uint32_t n, const uint4* __restrict__ gt, uint8_t* __restrict__ out, int collect) {
@@ -40,8 +41,10 @@ k_verify(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs, con
         load_words8(sw, sigs + 64ull * i);
         load_words8(sw + 8, sigs + 64ull * i + 32);
         bool ok;
-        if (kEcdsa) {
+        if (kKind == 0) {
             ok = ecdsa_verify_one(mw, pubs + 33ull * i, sw, tab, g);
+        } else if (kKind == 2) {
+            ok = ecdsa_verify_opaque_one(mw, pubs + 33ull * i, sw, tab, g);
         } else {
             uint32_t pw[8];
             load_words8(pw, pubs + 32ull * i);
@@ -67,21 +70,26 @@ cudaError_t UF_CAT(launch_verify_v, UF_VARIANT)(int kind, const uint8_t* msgs, c
     if (grid <= 0 || grid > need) grid = need;
     const uint4* gt = reinterpret_cast<const uint4*>(d_gtab);
     if (kind == 0)
-        UF_CAT(vk, UF_VARIANT)::k_verify<true><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+        UF_CAT(vk, UF_VARIANT)::k_verify<0><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+    else if (kind == 2)
+        UF_CAT(vk, UF_VARIANT)::k_verify<2><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
     else
-        UF_CAT(vk, UF_VARIANT)::k_verify<false><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+        UF_CAT(vk, UF_VARIANT)::k_verify<1><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
     return cudaGetLastError();
 }
 
 int UF_CAT(verify_occupancy_v, UF_VARIANT)(int kind) {
     int blocks = 0;
     const size_t smem = kVerifyThreads * kVerifySmemPerThread;
-    if (kind == 0) {
-        auto f = UF_CAT(vk, UF_VARIANT)::k_verify<true>;
+    if (kind != 1) {
+        // the opaque ECDSA instance shares kind 0's shape; opt both in
+        auto f2 = UF_CAT(vk, UF_VARIANT)::k_verify<2>;
+        cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        auto f = UF_CAT(vk, UF_VARIANT)::k_verify<0>;
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, kVerifyThreads, smem);
     } else {
-        auto f = UF_CAT(vk, UF_VARIANT)::k_verify<false>;
+        auto f = UF_CAT(vk, UF_VARIANT)::k_verify<1>;
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, kVerifyThreads, smem);
     }

@@ -1,7 +1,7 @@
 // Per-signature ECDSA and BIP-340 verification with the reference CPU's
 // semantics (the reference GPU kernels are laxer; the CPU verify is the oracle).
 //
-// ECDSA, as ufsecp_ecdsa_verify (src/cpu/src/impl/ufsecp_ecdsa.cpp:244-272):
+// ECDSA (compact form), as ufsecp_ecdsa_verify (src/cpu/src/impl/ufsecp_ecdsa.cpp:244-272):
 //   r, s in [1, n-1] (ECDSASignature::parse_compact_strict, src/cpu/src/ecdsa.cpp:94),
 //   s <= n/2 (BIP-62 low-S, :259-262), pubkey 02/03 prefix, x < p, on the curve
 //   (ecdsa_pubkey_parse, src/cpu/src/ecdsa.cpp:891-906), z = msg mod n,
@@ -28,16 +28,10 @@ UF_HD bool r_below_p_minus_n(const uint32_t r[8]) {
     return lt256(r, pmn);
 }
 
-// msg_w / sig_w: the 32 / 64 input bytes as words loaded little-endian.
+// ECDSA after the signature's scalars are parsed (r, s in [1, n-1]).
 template <class Tab, class GT>
-UF_HDI bool ecdsa_verify_one(const uint32_t msg_w[8], const uint8_t* pub33, const uint32_t sig_w[16],
-                             Tab& tab, const GT& gt) {
-    Sc r, s;
-    words_be_to_limbs(r.v, sig_w);
-    words_be_to_limbs(s.v, sig_w + 8);
-    if (sc_is_zero(r) || !limbs_lt_n(r.v)) return false;
-    if (sc_is_zero(s) || !limbs_lt_n(s.v)) return false;
-    if (!sc_is_low(s.v)) return false;
+UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const Sc& r, const Sc& s, Tab& tab,
+                            const GT& gt) {
     const uint8_t prefix = pub33[0];
     if (prefix != 0x02 && prefix != 0x03) return false;
     Fe qx, qy;
@@ -70,6 +64,40 @@ UF_HDI bool ecdsa_verify_one(const uint32_t msg_w[8], const uint8_t* pub33, cons
     }
     fe_mul(t, rf, z2);
     return fe_equal(t, R.X);
+}
+
+// msg_w / sig_w: the 32 / 64 input bytes as words loaded little-endian;
+// compact big-endian r || s, low-S required.
+template <class Tab, class GT>
+UF_HDI bool ecdsa_verify_one(const uint32_t msg_w[8], const uint8_t* pub33, const uint32_t sig_w[16],
+                             Tab& tab, const GT& gt) {
+    Sc r, s;
+    words_be_to_limbs(r.v, sig_w);
+    words_be_to_limbs(s.v, sig_w + 8);
+    if (sc_is_zero(r) || !limbs_lt_n(r.v)) return false;
+    if (sc_is_zero(s) || !limbs_lt_n(s.v)) return false;
+    if (!sc_is_low(s.v)) return false;
+    return ecdsa_verify_rs(msg_w, pub33, r, s, tab, gt);
+}
+
+// The libsecp in-memory signature layout of the consensus surfaces
+// (ufsecp_gpu_ecdsa_verify_opaque_rows / _lbtc_columns): r then s, each 32
+// little-endian bytes, so the little-endian words ARE the limbs.  r, s in
+// [1, n-1] without reduction; a high s is normalised to n - s, i.e. accepted
+// (ecdsa_sig_parse_opaque with normalize, src/cpu/src/impl/ufsecp_ecdsa.cpp:128-139).
+template <class Tab, class GT>
+UF_HDI bool ecdsa_verify_opaque_one(const uint32_t msg_w[8], const uint8_t* pub33, const uint32_t sig_w[16],
+                                    Tab& tab, const GT& gt) {
+    Sc r, s;
+    UF_UNROLL
+    for (int i = 0; i < 8; ++i) {
+        r.v[i] = sig_w[i];
+        s.v[i] = sig_w[8 + i];
+    }
+    if (sc_is_zero(r) || !limbs_lt_n(r.v)) return false;
+    if (sc_is_zero(s) || !limbs_lt_n(s.v)) return false;
+    if (!sc_is_low(s.v)) sc_neg(s, s);
+    return ecdsa_verify_rs(msg_w, pub33, r, s, tab, gt);
 }
 
 template <class Tab, class GT>

@@ -166,6 +166,25 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_stats(ufsecp_gpu_ext_server* ser
                                                       ufsecp_gpu_ext_server_stats_t* out, int reset);
 UFSECP_API void ufsecp_gpu_ext_server_destroy(ufsecp_gpu_ext_server* server);
 
+/* Engine hook provider: the GPU side of the reference engine's column-verify
+ * accelerator hook (secp256k1::GpuColumnsVerifyHook,
+ * src/cpu/include/secp256k1/batch_verify.hpp:143-168; the reference's own
+ * provider is src/gpu/src/gpu_engine_hook.cpp:81-104).  Same signature and
+ * return contract: kind 0 = ECDSA opaque little-endian columns (keys =
+ * compressed pubkeys), kind 1 = BIP-340 columns (keys = x-only); returns 1 when
+ * every row is valid, 0 when at least one is invalid (out_results fully
+ * written), -1 to decline (no CUDA device, bad arguments or any GPU error) so
+ * that the engine runs its CPU path.  Uses one process-wide context on device
+ * 0, created on first use and serialised by a mutex.  Install it with
+ * secp256k1::install_gpu_columns_verify_hook(&ufsecp_gpu_ext_engine_columns_hook). */
+UFSECP_API int ufsecp_gpu_ext_engine_columns_hook(int kind, const uint8_t* digests32, const uint8_t* keys,
+                                                  const uint8_t* sigs64, size_t count,
+                                                  uint8_t* out_results) UFSECP_NOEXCEPT;
+/* Calls the hook handled on the GPU / declined, since load. */
+UFSECP_API void ufsecp_gpu_ext_engine_hook_counters(uint64_t* handled, uint64_t* declined);
+/* Destroys the hook's process-wide context (the next call creates it again). */
+UFSECP_API void ufsecp_gpu_ext_engine_hook_release(void);
+
 /* Batch signing for synthetic workloads (device pointers, asynchronous on
  * `stream`): kind 0 = ECDSA, RFC 6979 nonce, low-S compact r||s, 33-byte
  * compressed pubkeys out; kind 1 = BIP-340 with aux_rand (d_aux32), 32-byte

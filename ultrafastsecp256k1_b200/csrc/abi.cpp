@@ -10,6 +10,7 @@
 
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <random>
 #include <algorithm>
@@ -768,6 +769,68 @@ void ufsecp_gpu_ext_server_destroy(ufsecp_gpu_ext_server* server) {
         delete server;
     } catch (...) {
     }
+}
+
+}  // extern "C"
+
+// ---- engine hook provider ------------------------------------------------------
+
+namespace {
+
+std::mutex g_hook_mu;
+std::unique_ptr<ufsecp_gpu_ctx> g_hook_ctx;   // process-wide context of the hook (device 0)
+bool g_hook_probed = false;
+uint64_t g_hook_handled = 0, g_hook_declined = 0;
+
+}  // namespace
+
+extern "C" {
+
+int ufsecp_gpu_ext_engine_columns_hook(int kind, const uint8_t* digests32, const uint8_t* keys,
+                                       const uint8_t* sigs64, size_t count, uint8_t* out_results) noexcept {
+    try {
+        std::lock_guard<std::mutex> lk(g_hook_mu);
+        if (!g_hook_probed) {
+            g_hook_probed = true;
+            if (cuda_device_count() > 0) {
+                std::unique_ptr<ufsecp_gpu_ctx> c(new ufsecp_gpu_ctx());
+                c->backend_id = UFSECP_GPU_BACKEND_CUDA;
+                c->device_index = 0;
+                c->backend.reset(new uf::Backend());
+                if (c->backend->init(0) == UFSECP_OK && c->backend->ready()) g_hook_ctx = std::move(c);
+            }
+        }
+        const bool usable = g_hook_ctx && (kind == 0 || kind == 1) && digests32 && keys && sigs64 && out_results &&
+                            count > 0 && count <= kMaxBatch;
+        if (!usable) {
+            ++g_hook_declined;
+            return -1;
+        }
+        const int rc = g_hook_ctx->backend->verify_host(kind == 0 ? 2 : 1, digests32, keys, sigs64, count,
+                                                        out_results, false);
+        if (rc != UFSECP_OK) {
+            ++g_hook_declined;
+            return -1;   // operational error: the engine falls back to its CPU path
+        }
+        ++g_hook_handled;
+        for (size_t i = 0; i < count; ++i)
+            if (out_results[i] == 0) return 0;
+        return 1;
+    } catch (...) {
+        return -1;
+    }
+}
+
+void ufsecp_gpu_ext_engine_hook_counters(uint64_t* handled, uint64_t* declined) {
+    std::lock_guard<std::mutex> lk(g_hook_mu);
+    if (handled) *handled = g_hook_handled;
+    if (declined) *declined = g_hook_declined;
+}
+
+void ufsecp_gpu_ext_engine_hook_release(void) {
+    std::lock_guard<std::mutex> lk(g_hook_mu);
+    g_hook_ctx.reset();
+    g_hook_probed = false;
 }
 
 }  // extern "C"

@@ -251,34 +251,16 @@ def run_reference(args):
 # -------------------------------------------------------------------- our arm --
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     import ultrafastsecp256k1_b200 as uf
 
+    from ultrafastsecp256k1_b200.shard import Ranks
+
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=180), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks.from_env(device="cuda")
+    rank = ranks.rank
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
     ctx = uf.GpuContext(local)
     n = args.batch
@@ -402,8 +384,7 @@ def run_ours(args):
         print(json.dumps(line))
     del d_msgs, d_xs, d_sigs, d_out
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 

@@ -63,6 +63,9 @@ class Oracle:
         for name in ("oracle_ecdsa_verify_batch", "oracle_schnorr_verify_batch"):
             getattr(L, name).argtypes = [_u8p, _u8p, _u8p, ctypes.c_size_t, _u8p]
             getattr(L, name).restype = None
+        L.oracle_msm.argtypes = [_u8p, _u8p, ctypes.c_size_t, _u8p]
+        L.oracle_msm.restype = ctypes.c_int
+        L.oracle_ops_batch.argtypes = [ctypes.c_int, _u8p, _u8p, _u8p, _u8p, ctypes.c_size_t, _u8p]
         L.oracle_ecdsa_verify_opaque_rows.argtypes = [_u8p, ctypes.c_size_t, ctypes.c_size_t, _u8p]
         L.oracle_ecdsa_sign_batch.argtypes = [_u8p, _u8p, ctypes.c_size_t, _u8p, _u8p, _u8p]
         L.oracle_schnorr_sign_batch.argtypes = [_u8p, _u8p, _u8p, ctypes.c_size_t, _u8p, _u8p, _u8p]
@@ -106,6 +109,31 @@ class Oracle:
         if n:
             self.L.oracle_ecdsa_verify_opaque_rows(_ptr(rows), stride, n, _ptr(out))
         return out
+
+    def _ops(self, op, n, a, b=None, c=None, d=None) -> np.ndarray:
+        out = np.zeros(max(n, 1), np.uint8)
+        arrs = [_as_u8(x) if x is not None else np.zeros(1, np.uint8) for x in (a, b, c, d)]
+        self.L.oracle_ops_batch(op, *[_ptr(x) for x in arrs], n, _ptr(out))
+        return out[:n]
+
+    def xonly_validate(self, keys32) -> np.ndarray:
+        k = _as_u8(keys32)
+        return self._ops(0, k.size // 32, k)
+
+    def pubkey_validate(self, pubs33) -> np.ndarray:
+        p = _as_u8(pubs33)
+        return self._ops(1, p.size // 33, p)
+
+    def commitment_verify(self, internal_x32, tweak32, tweaked_x32, parity) -> np.ndarray:
+        ix = _as_u8(internal_x32)
+        return self._ops(2, ix.size // 32, ix, tweak32, tweaked_x32, parity)
+
+    def msm(self, scalars32, points33):
+        """(status, compressed sum): status 0 OK, 5 scalar >= n, 3 bad point, 7 infinity."""
+        k, p = _as_u8(scalars32), _as_u8(points33)
+        out = np.zeros(33, np.uint8)
+        st = self.L.oracle_msm(_ptr(k), _ptr(p), k.size // 32, _ptr(out))
+        return st, out.tobytes()
 
     def ecdsa_sign_batch(self, msgs, sks):
         msgs, sks = _as_u8(msgs), _as_u8(sks)
@@ -270,6 +298,14 @@ class RefLib:
         out = np.zeros(max(n, 1), np.uint8)
         rc = self.L.ufsecp_ecdsa_verify_opaque_rows(self.ctx(), _ptr(rows), stride, n, _ptr(out))
         return rc, out[:n]
+
+    def msm(self, scalars32, points33):
+        """ufsecp_multi_scalar_mul: (return code, compressed sum)."""
+        k, p = _as_u8(scalars32), _as_u8(points33)
+        out = np.zeros(33, np.uint8)
+        self.L.ufsecp_multi_scalar_mul.argtypes = [ctypes.c_void_p, _u8p, _u8p, ctypes.c_size_t, _u8p]
+        rc = self.L.ufsecp_multi_scalar_mul(self.ctx(), _ptr(k), _ptr(p), k.size // 32, _ptr(out))
+        return rc, out.tobytes()
 
     def schnorr_batch_verify_rows(self, rows128: np.ndarray) -> int:
         """ufsecp_schnorr_batch_verify over 128-byte rows pk|msg|sig (RLC form)."""

@@ -643,6 +643,61 @@ void oracle_schnorr_verify_batch(const uint8_t *msgs, const uint8_t *pubs, const
     batch_ctx b = {msgs, pubs, sigs, NULL, NULL, out, NULL, NULL};
     parallel_for((long)n, schnorr_verify_item, &b);
 }
+/* Per-item batch operations next to verify (the reference GPU's libbitcoin
+ * bridge ops, src/gpu/src/gpu_backend_cuda.cu:748-803):
+ * x-only key valid = x < p and lift_x succeeds; compressed key valid = prefix
+ * 02/03, x < p, on the curve; BIP-341 commitment valid = lift_x(internal) +
+ * (tweak mod n) G is finite with x == tweaked_x and y parity == parity. */
+int oracle_xonly_validate(const uint8_t x32[32]) { gej P; return lift_x(&P, x32); }
+int oracle_pubkey_validate(const uint8_t pub33[33]) { gej P; return pubkey33_parse(&P, pub33); }
+int oracle_commitment_verify(const uint8_t ix[32], const uint8_t tw[32], const uint8_t tx[32], uint8_t parity) {
+    gej P, T, Q;
+    if (!lift_x(&P, ix)) return 0;
+    u256 t, x, y, want;
+    u256_from_be(&t, tw);
+    sc_reduce_once(&t);
+    gen_mul(&T, &t);
+    gej_add(&Q, &T, &P);
+    if (!gej_to_affine(&x, &y, &Q)) return 0;
+    u256_from_be(&want, tx);
+    return u256_cmp(&x, &want) == 0 && (int)(y.d[0] & 1) == (parity ? 1 : 0);
+}
+void oracle_ops_batch(int op, const uint8_t *a, const uint8_t *b, const uint8_t *c, const uint8_t *d, size_t n,
+                      uint8_t *out) {
+    for (size_t i = 0; i < n; ++i) {
+        if (op == 0) out[i] = (uint8_t)oracle_xonly_validate(a + 32 * i);
+        else if (op == 1) out[i] = (uint8_t)oracle_pubkey_validate(a + 33 * i);
+        else out[i] = (uint8_t)oracle_commitment_verify(a + 32 * i, b + 32 * i, c + 32 * i, d[i]);
+    }
+}
+
+/* sum k_i P_i as ufsecp_multi_scalar_mul (src/cpu/src/impl/ufsecp_taproot.cpp:957-991):
+ * returns 0 and the compressed sum, 5 for a scalar >= n, 3 for an invalid
+ * point (first bad item in order, scalar before point), 7 for infinity. */
+int oracle_msm(const uint8_t *scalars, const uint8_t *points, size_t n, uint8_t out33[33]) {
+    memset(out33, 0, 33);
+    gej acc, P, T;
+    gej_set_inf(&acc);
+    for (size_t i = 0; i < n; ++i) {
+        u256 k;
+        u256_from_be(&k, scalars + 32 * i);
+        if (u256_cmp(&k, &FN) >= 0) return 5;
+        if (!pubkey33_parse(&P, points + 33 * i)) return 3;
+    }
+    for (size_t i = 0; i < n; ++i) {
+        u256 k;
+        u256_from_be(&k, scalars + 32 * i);
+        pubkey33_parse(&P, points + 33 * i);
+        gej_mul(&T, &P, &k);
+        gej_add(&acc, &acc, &T);
+    }
+    u256 x, y;
+    if (!gej_to_affine(&x, &y, &acc)) return 7;
+    out33[0] = (uint8_t)(0x02 | (y.d[0] & 1));
+    u256_to_be(out33 + 1, &x);
+    return 0;
+}
+
 /* Opaque ECDSA rows [msg 32 | pubkey 33 | opaque sig 64 | tail], `stride` bytes apart. */
 typedef struct { const uint8_t *rows; size_t stride; uint8_t *out; } rows_ctx;
 static void ecdsa_opaque_item(void *c, long i) {

@@ -168,3 +168,81 @@ def opaque_rows_corpus(oracle, n, seed, stride=129):
                     break
             rows[i, 33:65] = np.frombuffer(x.to_bytes(32, "big"), np.uint8)
     return np.ascontiguousarray(rows)
+
+
+def _offcurve(x):
+    while True:
+        x = (x + 1) % P
+        if pow((x ** 3 + 7) % P, (P - 1) // 2, P) != 1:
+            return x
+
+
+def key_corpus(oracle, n, seed):
+    """Compressed keys (33 B) and x-only keys (32 B) with invalid classes mixed in:
+    prefix 0x00 / 0x04, x >= p, off-curve x."""
+    rng = np.random.default_rng(seed)
+    _, pubs, _ = ecdsa_corpus(oracle, n, seed, tamper=0.0)
+    pubs = pubs.copy()
+    xs = pubs[:, 1:].copy()
+    for i in range(n):
+        k = i % 6
+        if k == 1:
+            pubs[i, 0] = (0x00, 0x04, 0x05)[i % 3]
+        elif k == 2:
+            v = np.frombuffer((P + int(rng.integers(0, 977))).to_bytes(32, "big"), np.uint8)
+            pubs[i, 1:] = v
+            xs[i] = v
+        elif k == 3:
+            v = np.frombuffer(_offcurve(int.from_bytes(bytes(xs[i]), "big")).to_bytes(32, "big"), np.uint8)
+            pubs[i, 1:] = v
+            xs[i] = v
+    return np.ascontiguousarray(pubs), np.ascontiguousarray(xs)
+
+
+def tap_tweak(internal_x32: bytes, merkle_root: bytes) -> bytes:
+    import hashlib
+    tag = hashlib.sha256(b"TapTweak").digest()
+    return hashlib.sha256(tag + tag + internal_x32 + merkle_root).digest()
+
+
+def commitment_corpus(reflib, oracle, n, seed):
+    """(internal_x, tweak, tweaked_x, parity) rows: outputs derived by the reference's
+    ufsecp_taproot_output_key, with flipped parity / tampered x / off-curve internal keys."""
+    import ctypes
+    rng = np.random.default_rng(seed)
+    _, xs = key_corpus(oracle, n, seed)
+    L = reflib.L
+    L.ufsecp_taproot_output_key.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                            ctypes.POINTER(ctypes.c_int)]
+    ix, tw, tx, par, mr = [], [], [], [], []
+    for i in range(n):
+        x = bytes(xs[i])
+        root = rng.bytes(32)
+        out = ctypes.create_string_buffer(32)
+        p = ctypes.c_int(0)
+        rc = L.ufsecp_taproot_output_key(reflib.ctx(), x, root, out, ctypes.byref(p))
+        ox, pp = (out.raw, p.value) if rc == 0 else (rng.bytes(32), 0)
+        k = i % 5
+        if k == 1:
+            pp ^= 1
+        elif k == 2:
+            ox = bytes([ox[0] ^ 1]) + ox[1:]
+        ix.append(x)
+        tw.append(tap_tweak(x, root))
+        tx.append(ox)
+        par.append(pp)
+        mr.append(root)
+    cat = lambda v: np.frombuffer(b"".join(v), np.uint8).reshape(n, 32)
+    return cat(ix), cat(tw), cat(tx), np.array(par, np.uint8), cat(mr)
+
+
+def msm_corpus(oracle, n, seed):
+    """Scalars below n (some 0, some n-1) and valid compressed points (repeats included)."""
+    rng = np.random.default_rng(seed)
+    _, pubs, _ = ecdsa_corpus(oracle, max(n // 2, 1), seed, tamper=0.0)
+    pts = pubs[rng.integers(0, len(pubs), n)]
+    ks = rand_keys(rng, n)
+    if n > 3:
+        ks[1] = 0
+        ks[2] = np.frombuffer((N - 1).to_bytes(32, "big"), np.uint8)
+    return np.ascontiguousarray(ks), np.ascontiguousarray(pts)

@@ -75,6 +75,54 @@ def test_opaque_rows_vs_reference_library(oracle, reflib, stride):
     assert got[1::12].all()          # high-S twins are accepted on this surface
 
 
+def test_key_validation_vs_reference_library(oracle, reflib):
+    import ctypes
+    from conftest import key_corpus
+    pubs, xs = key_corpus(oracle, 300, seed=41)
+    L = reflib.L
+    L.ufsecp_pubkey_parse.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p]
+    out = ctypes.create_string_buffer(33)
+    ref = np.array([L.ufsecp_pubkey_parse(reflib.ctx(), bytes(p), 33, out) == 0 for p in pubs], np.uint8)
+    assert (oracle.pubkey_validate(pubs) == ref).all()
+    # an x-only key is valid iff 02 || x parses
+    ref_x = np.array([L.ufsecp_pubkey_parse(reflib.ctx(), b"\x02" + bytes(x), 33, out) == 0 for x in xs], np.uint8)
+    assert (oracle.xonly_validate(xs) == ref_x).all()
+    assert 0 < ref.sum() < len(ref) and 0 < ref_x.sum() < len(ref_x)
+
+
+def test_commitment_vs_reference_library(oracle, reflib):
+    import ctypes
+    from conftest import commitment_corpus
+    ix, tw, tx, par, mr = commitment_corpus(reflib, oracle, 200, seed=42)
+    L = reflib.L
+    L.ufsecp_taproot_verify.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
+                                        ctypes.c_char_p, ctypes.c_size_t]
+    ref = np.array([L.ufsecp_taproot_verify(reflib.ctx(), bytes(tx[i]), int(par[i]), bytes(ix[i]), bytes(mr[i]), 32)
+                    == 0 for i in range(len(ix))], np.uint8)
+    got = oracle.commitment_verify(ix, tw, tx, par)
+    assert (got == ref).all()
+    assert 0 < ref.sum() < len(ref)
+
+
+def test_msm_vs_reference_library(oracle, reflib):
+    from conftest import msm_corpus
+    for n, seed in ((1, 1), (7, 2), (150, 3)):
+        ks, pts = msm_corpus(oracle, n, seed)
+        assert oracle.msm(ks, pts) == reflib.msm(ks, pts)
+    ks, pts = msm_corpus(oracle, 10, 4)
+    bad_k = ks.copy()
+    bad_k[3] = 0xFF                                       # scalar >= n
+    assert oracle.msm(bad_k, pts)[0] == reflib.msm(bad_k, pts)[0] == 5
+    bad_p = pts.copy()
+    bad_p[5, 0] = 0x04                                    # invalid point
+    assert oracle.msm(ks, bad_p)[0] == reflib.msm(ks, bad_p)[0] == 3
+    # k P + (n - k) P = infinity
+    two_k = np.concatenate([ks[:1], np.frombuffer((N - int.from_bytes(bytes(ks[0]), "big")).to_bytes(32, "big"),
+                                                  np.uint8)[None]])
+    two_p = np.concatenate([pts[:1], pts[:1]])
+    assert oracle.msm(two_k, two_p)[0] == reflib.msm(two_k, two_p)[0] == 7
+
+
 def test_oracle_signers_vs_reference_library(oracle, reflib):
     rng = np.random.default_rng(5)
     for i in range(16):

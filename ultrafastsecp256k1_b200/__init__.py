@@ -26,6 +26,7 @@ UFSECP_ERR_BAD_PUBKEY = 3
 UFSECP_ERR_BAD_SIG = 4
 UFSECP_ERR_BAD_INPUT = 5
 UFSECP_ERR_VERIFY_FAIL = 6
+UFSECP_ERR_ARITH = 7
 UFSECP_ERR_INTERNAL = 9
 UFSECP_ERR_GPU_UNAVAILABLE = 100
 UFSECP_ERR_GPU_DEVICE = 101

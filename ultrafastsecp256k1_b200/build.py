@@ -51,7 +51,7 @@ _VARIANT_FLAGS = [
 _BEST_FLAGS = ["-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]
 VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS, "kernels_probe.cu": _VARIANT_FLAGS,
             "kernels_queue.cu": [("", _BEST_FLAGS)], "kernels_noalloc.cu": [("", _BEST_FLAGS)],
-            "rlc.cu": [("", _BEST_FLAGS)]}
+            "rlc.cu": [("", _BEST_FLAGS)], "kernels_ops.cu": [("", _BEST_FLAGS)]}
 
 
 def _sources():

@@ -94,6 +94,18 @@ ufsecp_error_t gated_collect(ufsecp_gpu_ctx* ctx, const uint8_t* a, const uint8_
     }
 }
 
+// Runs a result-bearing call, re-clearing its output on failure.
+template <class F>
+ufsecp_error_t guarded_out(uint8_t* out, size_t count, size_t stride, F&& run) {
+    try {
+        return finish(run(), out, count, stride);
+    } catch (const std::bad_alloc&) {
+        return finish(UFSECP_ERR_GPU_MEMORY, out, count, stride);
+    } catch (...) {
+        return finish(UFSECP_ERR_INTERNAL, out, count, stride);
+    }
+}
+
 ufsecp_error_t unsupported(ufsecp_gpu_ctx* ctx, size_t count) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     if (count == 0) return UFSECP_OK;
@@ -308,26 +320,80 @@ ufsecp_error_t ufsecp_gpu_ecdh_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, const 
 ufsecp_error_t ufsecp_gpu_hash160_pubkey_batch(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t count, uint8_t*) {
     return unsupported(ctx, count);
 }
-ufsecp_error_t ufsecp_gpu_msm(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, size_t n, uint8_t*) {
-    return unsupported(ctx, n);
+ufsecp_error_t ufsecp_gpu_msm(ufsecp_gpu_ctx* ctx, const uint8_t* scalars32, const uint8_t* points33, size_t n,
+                              uint8_t* out_result33) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!clear_out(out_result33, 1, 33)) return UFSECP_ERR_BAD_INPUT;
+    if (!scalars32 || !points33 || !out_result33) return UFSECP_ERR_NULL_ARG;
+    return guarded_out(out_result33, 1, 33, [&]() -> int {
+        uf::Backend& be = *ctx->backend;
+        if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
+        if (n > uf::RlcVerifier::kMaxItems) return be.set_error(UFSECP_ERR_BAD_INPUT, "MSM: more than 2^24 points");
+        cudaError_t e = cudaSetDevice(be.device());
+        if (e != cudaSuccess) return be.cuda_error(e, "cudaSetDevice");
+        int status = 0;
+        const int rc = be.rlc().msm_host(scalars32, points33, (uint32_t)n, out_result33, &status);
+        if (rc != UFSECP_OK) return rc;
+        if (status == UFSECP_ERR_BAD_INPUT) return be.set_error(status, "scalar >= n");
+        if (status == UFSECP_ERR_BAD_PUBKEY) return be.set_error(status, "invalid point in array");
+        if (status == UFSECP_ERR_ARITH) return be.set_error(status, "MSM result is infinity");
+        be.clear_error();
+        return UFSECP_OK;
+    });
 }
-ufsecp_error_t ufsecp_gpu_xonly_validate(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t n, uint8_t*) {
-    return unsupported(ctx, n);
+ufsecp_error_t ufsecp_gpu_xonly_validate(ufsecp_gpu_ctx* ctx, const uint8_t* keys32, size_t n, uint8_t* results) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!clear_out(results, n, 1)) return UFSECP_ERR_BAD_INPUT;
+    if (!keys32 || !results) return UFSECP_ERR_NULL_ARG;
+    return guarded_out(results, n, 1, [&] { return ctx->backend->xonly_validate(keys32, n, results); });
 }
-ufsecp_error_t ufsecp_gpu_commitment_verify(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, const uint8_t*,
-                                            const uint8_t*, size_t n, uint8_t*) {
-    return unsupported(ctx, n);
+ufsecp_error_t ufsecp_gpu_commitment_verify(ufsecp_gpu_ctx* ctx, const uint8_t* internal_x32, const uint8_t* tweak32,
+                                            const uint8_t* tweaked_x32, const uint8_t* parity, size_t n,
+                                            uint8_t* results) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!clear_out(results, n, 1)) return UFSECP_ERR_BAD_INPUT;
+    if (!internal_x32 || !tweak32 || !tweaked_x32 || !parity || !results) return UFSECP_ERR_NULL_ARG;
+    return guarded_out(results, n, 1, [&] {
+        return ctx->backend->commitment_verify(internal_x32, tweak32, tweaked_x32, parity, n, results);
+    });
 }
-ufsecp_error_t ufsecp_gpu_tagged_hash(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, size_t, size_t n,
-                                      uint8_t*) {
-    return unsupported(ctx, n);
+ufsecp_error_t ufsecp_gpu_tagged_hash(ufsecp_gpu_ctx* ctx, const uint8_t* tag_hash32, const uint8_t* msgs,
+                                      size_t msg_len, size_t n, uint8_t* out32) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (msg_len == 0 || msg_len > 256) return UFSECP_ERR_BAD_INPUT;
+    if (!clear_out(out32, n, 32)) return UFSECP_ERR_BAD_INPUT;
+    if (!tag_hash32 || !msgs || !out32) return UFSECP_ERR_NULL_ARG;
+    return guarded_out(out32, n, 32, [&] {
+        return ctx->backend->tagged_hash(tag_hash32, msgs, nullptr, msg_len, msg_len, n, out32);
+    });
 }
-ufsecp_error_t ufsecp_gpu_pubkey_validate(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t n, uint8_t*) {
-    return unsupported(ctx, n);
+ufsecp_error_t ufsecp_gpu_pubkey_validate(ufsecp_gpu_ctx* ctx, const uint8_t* pubkeys33, size_t n, uint8_t* results) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (!clear_out(results, n, 1)) return UFSECP_ERR_BAD_INPUT;
+    if (!pubkeys33 || !results) return UFSECP_ERR_NULL_ARG;
+    return guarded_out(results, n, 1, [&] { return ctx->backend->pubkey_validate(pubkeys33, n, results); });
 }
-ufsecp_error_t ufsecp_gpu_tagged_hash_var(ufsecp_gpu_ctx* ctx, const uint8_t*, const uint8_t*, const uint32_t*,
-                                          size_t, size_t n, uint8_t*) {
-    return unsupported(ctx, n);
+ufsecp_error_t ufsecp_gpu_tagged_hash_var(ufsecp_gpu_ctx* ctx, const uint8_t* tag_hash32, const uint8_t* msgs,
+                                          const uint32_t* msg_lens, size_t stride, size_t n, uint8_t* out32) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (n == 0) return UFSECP_OK;
+    if (n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    if (stride == 0 || stride > 256) return UFSECP_ERR_BAD_INPUT;
+    if (!clear_out(out32, n, 32)) return UFSECP_ERR_BAD_INPUT;
+    if (!tag_hash32 || !msgs || !msg_lens || !out32) return UFSECP_ERR_NULL_ARG;
+    return guarded_out(out32, n, 32, [&] {
+        return ctx->backend->tagged_hash(tag_hash32, msgs, msg_lens, 0, stride, n, out32);
+    });
 }
 ufsecp_error_t ufsecp_gpu_hash256(ufsecp_gpu_ctx* ctx, const uint8_t*, size_t, size_t n, uint8_t*) {
     return unsupported(ctx, n);

@@ -132,6 +132,7 @@ Backend::~Backend() {
         pubs_.release();
         sigs_.release();
         out_.release();
+        ops_in_.release();
         scratch_.release();
         for (int j = 0; j < 2; ++j) {
             if (pstream_[j]) cudaStreamSynchronize(pstream_[j]);

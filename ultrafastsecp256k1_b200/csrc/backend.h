@@ -78,6 +78,14 @@ public:
     // RLC batch verifier of BIP-340 signatures (created on first use).
     RlcVerifier& rlc();
     int queue_grid() const { return queue_grid_; }
+    // Per-item batch operations (ops.cpp): host buffers, synchronous.
+    int xonly_validate(const uint8_t* keys32, size_t n, uint8_t* out);
+    int pubkey_validate(const uint8_t* pubs33, size_t n, uint8_t* out);
+    int commitment_verify(const uint8_t* internal_x, const uint8_t* tweak, const uint8_t* tweaked_x,
+                          const uint8_t* parity, size_t n, uint8_t* out);
+    // lens == nullptr: fixed_len bytes per message, else lens[i] (each <= stride).
+    int tagged_hash(const uint8_t* tag_hash32, const uint8_t* msgs, const uint32_t* lens, size_t fixed_len,
+                    size_t stride, size_t n, uint8_t* out32);
     int diag(uint32_t op, const uint8_t* in, size_t n, uint8_t* out, size_t in_sz, size_t out_sz);
     int imad_peak(double* ops_per_s);
     int probe(int op, int blocks, int threads, int iters, float* ms);
@@ -104,7 +112,7 @@ private:
     void load_tuning();
     cudaStream_t stream_ = nullptr;
     void* d_gtab_ = nullptr;
-    DevBuf msgs_, pubs_, sigs_, out_, scratch_;
+    DevBuf msgs_, pubs_, sigs_, out_, scratch_, ops_in_;
     // host-buffer calls: two pinned staging slots, each with its own stream,
     // so that packing chunk k + 1 on the CPU overlaps verifying chunk k
     HostBuf pstage_[2];

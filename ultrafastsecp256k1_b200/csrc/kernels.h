@@ -47,6 +47,16 @@ int verify_occupancy_v3(int kind);
 int verify_occupancy_v4(int kind);
 int verify_occupancy_v5(int kind);
 
+// Per-item batch operations (kernels_ops.cu); device pointers, asynchronous.
+cudaError_t launch_xonly_validate(const uint8_t* keys32, uint32_t n, uint8_t* out, int sms, cudaStream_t s);
+cudaError_t launch_pubkey_validate(const uint8_t* pubs33, uint32_t n, uint8_t* out, int sms, cudaStream_t s);
+cudaError_t launch_commitment_verify(const uint8_t* internal_x, const uint8_t* tweak, const uint8_t* tweaked_x,
+                                     const uint8_t* parity, uint32_t n, const void* d_gtab, uint8_t* out, int sms,
+                                     cudaStream_t s);
+cudaError_t launch_tagged_hash(const uint8_t tag_hash[32], const uint8_t* msgs, const uint32_t* lens,
+                               uint32_t fixed_len, uint32_t stride, uint32_t n, uint8_t* out32, int sms,
+                               cudaStream_t s);
+
 // Mixed-batch staging layout shared by host (pinned) and device buffers:
 //   [header 256 B: counts n_e, n_s][e_msgs cap_e*32][s_msgs cap_s*32]
 //   [e_sigs cap_e*64][s_sigs cap_s*64][s_pubs cap_s*32][e_pubs cap_e*33]

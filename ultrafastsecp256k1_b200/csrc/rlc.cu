@@ -380,7 +380,7 @@ k_rlc_wcomb(RoundGeo g, const uint4* __restrict__ wu, const uint4* __restrict__ 
 // infinity, | 2 if the segment holds an item that failed to parse.
 __global__ void __launch_bounds__(64)
 k_rlc_finish(RoundGeo g, const uint4* __restrict__ wins, const uint32_t* __restrict__ segbad,
-             uint8_t* __restrict__ segok) {
+             uint8_t* __restrict__ segok, uint4* __restrict__ segpt) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.n_seg) return;
     const uint4* base = wins + kJacQ * (uint64_t)s * g.W;
@@ -392,6 +392,7 @@ k_rlc_finish(RoundGeo g, const uint4* __restrict__ wins, const uint32_t* __restr
         jac_add(acc, w);
     }
     segok[s] = (uint8_t)((acc.inf ? 1 : 0) | (segbad[s] ? 2 : 0));
+    store_jac(segpt + kJacQ * (uint64_t)s, acc);
 }
 
 __global__ void k_rlc_gather(const uint32_t* __restrict__ idx, uint32_t m, const uint8_t* __restrict__ msgs,
@@ -447,6 +448,70 @@ __global__ void k_rlc_rows(const uint8_t* __restrict__ rows, uint32_t n, uint8_t
     if (code) atomicMin(first, (i << 2) | (code - 3));
 }
 
+// MSM input: scalar k (32 bytes big-endian, k < n) and compressed point P per
+// item.  Item i becomes the points P and lambda P with the GLV halves of k (signs
+// folded into y) in the first two point slots of the RLC item layout; the third
+// slot and t are zero, so the round computes sum k_i P_i with no generator term.
+// *first = min over bad items of (i << 2 | 0 for k >= n, 1 for a bad point),
+// the scalar tested first (ufsecp_multi_scalar_mul, src/cpu/src/impl/ufsecp_taproot.cpp:975-983).
+__global__ void __launch_bounds__(128)
+k_msm_prep(const uint8_t* __restrict__ scalars, const uint8_t* __restrict__ points, uint32_t n,
+           RlcItem* __restrict__ items, uint4* __restrict__ mags, uint32_t* __restrict__ tsc,
+           uint8_t* __restrict__ okb, uint32_t* __restrict__ first) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Sc k;
+    be32_to_limbs(k.v, scalars + 32ull * i);
+    const uint8_t* p = points + 33ull * i;
+    Fe x, y;
+    uint32_t code = 0xFFFFFFFFu;
+    if (!limbs_lt_n(k.v)) {
+        code = 0;
+    } else {
+        be32_to_limbs(x.v, p + 1);
+        if ((p[0] != 0x02 && p[0] != 0x03) || !limbs_lt_p(x.v) || !lift_x_parity(y, x, p[0] == 0x03)) code = 1;
+    }
+    okb[i] = 1;
+    for (int j = 0; j < 8; ++j) tsc[8ull * i + j] = 0;
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    mags[3ull * i + 2] = z;
+    if (code != 0xFFFFFFFFu) {
+        atomicMin(first, (i << 2) | code);
+        mags[3ull * i] = z;
+        mags[3ull * i + 1] = z;
+        return;
+    }
+    GlvSplit g;
+    glv_split(g, k);
+    Fe beta, yn, lx;
+    fe_beta(beta);
+    yn = y;
+    if (g.neg1) { fe_neg(yn, y); fe_normalize(yn); }
+    store_aff(items[i].pt[0], x, yn);
+    yn = y;
+    if (g.neg2) { fe_neg(yn, y); fe_normalize(yn); }
+    fe_mul(lx, x, beta);
+    fe_normalize(lx);
+    store_aff(items[i].pt[1], lx, yn);
+    mags[3ull * i] = make_uint4(g.k1[0], g.k1[1], g.k1[2], g.k1[3]);
+    mags[3ull * i + 1] = make_uint4(g.k2[0], g.k2[1], g.k2[2], g.k2[3]);
+}
+
+// Jacobian sum -> 33-byte compressed point; ok = 0 for infinity.
+__global__ void k_msm_out(const uint4* __restrict__ pt, uint8_t* __restrict__ out33, uint8_t* __restrict__ ok) {
+    Jac P;
+    load_jac(pt, P);
+    Aff a;
+    if (!jac_to_aff(a, P)) {
+        *ok = 0;
+        for (int k = 0; k < 33; ++k) out33[k] = 0;
+        return;
+    }
+    *ok = 1;
+    out33[0] = (a.y.v[0] & 1u) ? 0x03 : 0x02;
+    limbs_to_be32(out33 + 1, a.x.v);
+}
+
 inline unsigned grid_for(uint64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 }  // namespace
@@ -471,7 +536,7 @@ RlcVerifier::~RlcVerifier() {
     for (DevBuf* b : {&items_, &mags_, &tsc_, &okb_, &segs_, &segmag_, &segneg_, &segbad_, &counts_, &offsets_,
                       &cursor_, &nch_, &coff_, &entries_, &partials_, &buckets_, &wu_, &wt_, &wins_, &segok_,
                       &scan_tmp_, &leaf_idx_, &leaf_m_, &leaf_x_, &leaf_s_, &leaf_out_, &in_m_, &in_x_, &in_s_,
-                      &in_out_, &in_rows_, &gate_})
+                      &in_out_, &in_rows_, &gate_, &segpt_})
         b->release();
 }
 
@@ -505,6 +570,7 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
         (e = wu_.ensure((uint64_t)n_seg * W * S * 112)) != cudaSuccess ||
         (e = wt_.ensure((uint64_t)n_seg * W * S * 112)) != cudaSuccess ||
         (e = wins_.ensure((uint64_t)n_seg * W * 112)) != cudaSuccess || (e = segok_.ensure(n_seg)) != cudaSuccess ||
+        (e = segpt_.ensure((uint64_t)n_seg * 112)) != cudaSuccess ||
         (e = scan_tmp_.ensure(std::max<size_t>(scan_bytes, 16))) != cudaSuccess)
         return be_->cuda_error(e, "RLC round buffers");
     uint32_t* d_seg = (uint32_t*)segs_.p;
@@ -544,7 +610,7 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     k_rlc_wcomb<<<grid_for((uint64_t)n_seg * W, 128), 128, 0, s>>>(g, (const uint4*)wu_.p, (const uint4*)wt_.p,
                                                                   (uint4*)wins_.p);
     k_rlc_finish<<<grid_for(n_seg, 64), 64, 0, s>>>(g, (const uint4*)wins_.p, (const uint32_t*)segbad_.p,
-                                                   (uint8_t*)segok_.p);
+                                                   (uint8_t*)segok_.p, (uint4*)segpt_.p);
     e = cudaGetLastError();
     ok.resize(n_seg);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ok.data(), segok_.p, n_seg, cudaMemcpyDeviceToHost, s);
@@ -704,6 +770,50 @@ int RlcVerifier::verify_entries(const uint8_t* rows, uint32_t n, const uint8_t s
     e = cudaMemcpyAsync(h_out, in_out_.p, n, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC copy out");
+    return kOk;
+}
+
+int RlcVerifier::msm_host(const uint8_t* scalars32, const uint8_t* points33, uint32_t n, uint8_t out33[33],
+                          int* status) {
+    *status = 0;
+    if (n == 0) return kOk;
+    if (n > kMaxItems) return be_->set_error(kErrBadInput, "MSM: more than 2^24 points");
+    const cudaStream_t s = be_->stream();
+    cudaError_t e;
+    if ((e = in_m_.ensure(32ull * n)) != cudaSuccess || (e = in_x_.ensure(33ull * n + 16)) != cudaSuccess ||
+        (e = items_.ensure((uint64_t)n * sizeof(RlcItem))) != cudaSuccess ||
+        (e = mags_.ensure((uint64_t)n * 48)) != cudaSuccess || (e = tsc_.ensure((uint64_t)n * 32)) != cudaSuccess ||
+        (e = okb_.ensure(n)) != cudaSuccess || (e = gate_.ensure(64)) != cudaSuccess)
+        return be_->cuda_error(e, "MSM buffers");
+    uint32_t first = 0xFFFFFFFFu;
+    e = cudaMemcpyAsync(in_m_.p, scalars32, 32ull * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in_x_.p, points33, 33ull * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(gate_.p, 0xFF, 4, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "MSM copy in");
+    k_msm_prep<<<grid_for(n, 128), 128, 0, s>>>((const uint8_t*)in_m_.p, (const uint8_t*)in_x_.p, n,
+                                                (RlcItem*)items_.p, (uint4*)mags_.p, (uint32_t*)tsc_.p,
+                                                (uint8_t*)okb_.p, (uint32_t*)gate_.p);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&first, gate_.p, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "MSM parse");
+    if (first != 0xFFFFFFFFu) {
+        *status = (first & 3u) == 0 ? kErrBadInput : 3;   // scalar >= n / invalid point
+        return kOk;
+    }
+    n_ = n;
+    const std::vector<uint32_t> seg = {0u, n};
+    const int rc = run_round(seg, rlc_window_bits(n), s, ok_host_);
+    if (rc != kOk) return rc;
+    uint8_t* d_out = (uint8_t*)gate_.p + 16;
+    uint8_t ok = 0;
+    k_msm_out<<<1, 1, 0, s>>>((const uint4*)segpt_.p, d_out, d_out + 40);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out33, d_out, 33, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ok, d_out + 40, 1, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "MSM result");
+    if (!ok) *status = 7;   // the sum is the point at infinity
     return kOk;
 }
 

@@ -79,6 +79,14 @@ public:
     int verify_entries(const uint8_t* entries, uint32_t n, const uint8_t seed[32], uint8_t* h_out, int* gate_code,
                        uint32_t* gate_index, RlcStats* stats);
 
+    // Multi-scalar multiplication sum k_i P_i over host arrays (32-byte
+    // big-endian scalars, 33-byte compressed points) with the same Pippenger
+    // rounds (ufsecp_gpu_msm).  *status: 0 and out33 = the compressed sum; 5
+    // (BAD_INPUT) for a scalar >= n, 3 (BAD_PUBKEY) for an invalid point (the
+    // first bad item in index order decides, scalar before point); 7 (ARITH)
+    // when the sum is infinity.
+    int msm_host(const uint8_t* scalars32, const uint8_t* points33, uint32_t n, uint8_t out33[33], int* status);
+
 private:
     // One MSM check of every segment (start, length pairs); ok[k] bit 0 = the
     // equation holds, bit 1 = the segment holds an item that failed to parse.
@@ -97,6 +105,7 @@ private:
     DevBuf leaf_idx_, leaf_m_, leaf_x_, leaf_s_, leaf_out_;
     // host-buffer calls
     DevBuf in_m_, in_x_, in_s_, in_out_, in_rows_, gate_;
+    DevBuf segpt_;       // each segment's final sum (Jacobian, 112 B)
     std::vector<uint8_t> ok_host_;
 };
 

@@ -131,18 +131,23 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_identify_invalid(ufsecp_g
  * UFSECP_ERR_GPU_QUEUE on timeout (the request stays pending).  While a server
  * runs, its context belongs to the server's thread: make no other call on that
  * context.  Destroy the server (it finishes the pending requests) before the
- * context.  The memory budget covers the slots' fixed staging (pinned + device,
- * reserved at creation; fewer slots are made if they do not fit) plus the
+ * context.  With key_cache_log2 set, decompressed keys with their 1P..8P
+ * tables stay resident in a device cache shared by the slots, so a key seen
+ * before skips its square root, table additions and inversion (verdicts are
+ * unchanged); off by default (on B200 it measured no faster, see the bench).  The memory
+ * budget covers the slots' fixed staging (pinned + device) and the key cache,
+ * reserved at creation (fewer slots are made if they do not fit), plus the
  * staged bytes of the items in flight; pending requests wait for room.
  * Config NULL = defaults: 4 slots, 65,536 items per launch, an 8 GiB budget,
- * no batch window. */
+ * no batch window, no key cache. */
 typedef struct ufsecp_gpu_ext_server ufsecp_gpu_ext_server;
 typedef struct {
     uint32_t slots;                 /* streams / launches in flight, 1..64 */
     uint32_t max_launch_items;      /* 1..65536 */
     uint64_t memory_budget_bytes;
     uint32_t batch_window_us;       /* 0: launch as soon as a slot is free */
-    uint32_t reserved;              /* 0 */
+    uint32_t key_cache_log2;        /* resident key / P-table cache of 2^k slots, 576 B each:
+                                       0 or 1 = no cache (the default), else 8..24 */
 } ufsecp_gpu_ext_server_config_t;
 typedef struct {
     uint64_t requests_done, items_done, launches;
@@ -152,6 +157,7 @@ typedef struct {
     uint32_t peak_slots_in_flight, reserved;
     double p50_us, p99_us, max_us, mean_us;   /* submit -> verdicts written, completed requests */
     double busy_s, span_s;                    /* time with a launch in flight; first submit -> last completion */
+    uint64_t cache_lookups, cache_hits;       /* resident key cache since creation */
 } ufsecp_gpu_ext_server_stats_t;
 
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_create(ufsecp_gpu_ctx* ctx,

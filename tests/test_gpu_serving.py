@@ -126,3 +126,24 @@ def test_server_gating(gpu_ctx):
         # an empty request completes at once
         assert L.ufsecp_gpu_ext_server_submit(srv._h, arr, 0, rid) == uf.UFSECP_OK
         assert L.ufsecp_gpu_ext_server_wait(srv._h, rid.value, 1000) == uf.UFSECP_OK
+
+
+@pytest.mark.parametrize("cache_log2", [1, 8, 17])
+def test_resident_key_cache_keeps_verdicts(oracle, pools, cache_log2):
+    """Same requests with no cache, a tiny cache that overflows (256 slots, many
+    keys) and a 2^17-slot cache: identical verdicts, and hits when cached."""
+    reqs = _requests(pools, 80, seed=13)
+    reqs = reqs + reqs            # the second pass sees every key again
+    with uf.GpuContext(0) as sctx, uf.Server(sctx, slots=2, max_launch_items=4096,
+                                             key_cache_log2=cache_log2) as srv:
+        outs = [srv.wait(srv.submit(r)) for r in reqs]
+        st = srv.stats()
+    for jobs, got in zip(reqs, outs):
+        for g, w in zip(got, _oracle(oracle, jobs)):
+            assert (g == w).all()
+    if cache_log2 == 1:
+        assert st["cache_lookups"] == 0
+    else:
+        assert st["cache_lookups"] > 0 and st["cache_hits"] > 0
+        if cache_log2 == 17:
+            assert st["cache_hits"] >= st["cache_lookups"] // 3

@@ -58,7 +58,7 @@ class Job(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_uint32), ("max_launch_items", ctypes.c_uint32),
                 ("memory_budget_bytes", ctypes.c_uint64), ("batch_window_us", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("key_cache_log2", ctypes.c_uint32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -67,7 +67,8 @@ class ServerStats(ctypes.Structure):
                 ("pending_requests", ctypes.c_uint64),
                 ("peak_slots_in_flight", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
                 ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double), ("max_us", ctypes.c_double),
-                ("mean_us", ctypes.c_double), ("busy_s", ctypes.c_double), ("span_s", ctypes.c_double)]
+                ("mean_us", ctypes.c_double), ("busy_s", ctypes.c_double), ("span_s", ctypes.c_double),
+                ("cache_lookups", ctypes.c_uint64), ("cache_hits", ctypes.c_uint64)]
 
 
 class DeviceInfo(ctypes.Structure):
@@ -401,10 +402,11 @@ class Server:
     of ECDSA / BIP-340 jobs from any thread, wait for their verdicts."""
 
     def __init__(self, ctx: GpuContext, slots: int = 4, max_launch_items: int = 1 << 16,
-                 memory_budget_bytes: int = 8 << 30, batch_window_us: int = 0):
+                 memory_budget_bytes: int = 8 << 30, batch_window_us: int = 0, key_cache_log2: int = 0):
+        """key_cache_log2: 0 or 1 = no resident key cache (default), 8..24 = a cache of 2^k slots."""
         self.L = ctx.L
         self._ctx = ctx
-        cfg = ServerConfig(slots, max_launch_items, memory_budget_bytes, batch_window_us, 0)
+        cfg = ServerConfig(slots, max_launch_items, memory_budget_bytes, batch_window_us, key_cache_log2)
         h = _vp()
         rc = self.L.ufsecp_gpu_ext_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h))
         if rc != UFSECP_OK:

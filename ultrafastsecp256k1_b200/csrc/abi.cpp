@@ -767,6 +767,7 @@ ufsecp_error_t ufsecp_gpu_ext_server_create(ufsecp_gpu_ctx* ctx, const ufsecp_gp
             cfg.max_launch_items = config->max_launch_items;
             cfg.memory_budget_bytes = config->memory_budget_bytes;
             cfg.batch_window_us = config->batch_window_us;
+            cfg.key_cache_log2 = config->key_cache_log2 <= 1 ? 0 : config->key_cache_log2;
         }
         cudaError_t e = cudaSetDevice(ctx->backend->device());
         if (e != cudaSuccess) return ctx->backend->cuda_error(e, "cudaSetDevice");
@@ -827,6 +828,8 @@ ufsecp_error_t ufsecp_gpu_ext_server_stats(ufsecp_gpu_ext_server* server, ufsecp
     out->mean_us = s.mean_us;
     out->busy_s = s.busy_s;
     out->span_s = s.span_s;
+    out->cache_lookups = s.cache_lookups;
+    out->cache_hits = s.cache_hits;
     return UFSECP_OK;
 }
 

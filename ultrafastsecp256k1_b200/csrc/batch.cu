@@ -46,7 +46,11 @@ BatchSlot::~BatchSlot() {
     if (stream_) cudaStreamSynchronize(stream_);
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     graphs_.clear();
+    if (stream2_) cudaStreamSynchronize(stream2_);
     if (done_) cudaEventDestroy(done_);
+    if (fork_) cudaEventDestroy(fork_);
+    if (join_) cudaEventDestroy(join_);
+    if (stream2_) cudaStreamDestroy(stream2_);
     if (d_head_) cudaFree(d_head_);
     pinned_.release();
     big_pinned_.release();
@@ -60,6 +64,9 @@ int BatchSlot::init(Backend* be, bool use_graphs) {
     use_graphs_ = use_graphs;
     cudaError_t e = cudaSetDevice(be->device());
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join_, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done_, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(&d_head_, 256);
     if (e == cudaSuccess && use_graphs) {
@@ -85,6 +92,9 @@ QueueArgs BatchSlot::args_for(uint8_t* d) const {
     a.e_pubs = d + layout_.e_pubs;
     a.e_out = d + layout_.e_out;
     a.s_out = d + layout_.s_out;
+    a.cache = cache_;
+    a.cache_mask = cache_mask_;
+    a.cache_stats = cache_stats_;
     return a;
 }
 
@@ -92,7 +102,7 @@ int BatchSlot::run_direct(const QueueArgs& a) {
     uint8_t* h = staged_big_ ? (uint8_t*)big_pinned_.p : (uint8_t*)pinned_.p;
     uint8_t* d = staged_big_ ? (uint8_t*)big_dev_.p : (uint8_t*)dev_.p;
     cudaError_t e = cudaMemcpyAsync(d, h, layout_.in_bytes, cudaMemcpyHostToDevice, stream_);
-    if (e == cudaSuccess) e = launch_verify_queue(a, be_->gtab(), d_head_, be_->queue_grid(), stream_);
+    if (e == cudaSuccess) e = launch_verify_queue(a, be_->gtab(), d_head_, be_->queue_grid(), stream_, stream2_, fork_, join_);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(h + layout_.e_out, d + layout_.e_out, layout_.out_bytes, cudaMemcpyDeviceToHost, stream_);
     if (e != cudaSuccess) return be_->cuda_error(e, "batch enqueue");

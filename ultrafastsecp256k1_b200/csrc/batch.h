@@ -53,6 +53,13 @@ public:
     // Waits for the enqueued work and writes every job's verdicts.
     int finish(const VerifyJob* jobs, size_t n_jobs);
 
+    // Resident key / table cache for the queue kernel (kernels.h QueueArgs);
+    // set before the first enqueue: captured graphs keep the pointers.
+    void set_cache(PubCacheSlot* slots, uint32_t mask, unsigned long long* stats) {
+        cache_ = slots;
+        cache_mask_ = mask;
+        cache_stats_ = stats;
+    }
     cudaStream_t stream() const { return stream_; }
     size_t staged_bytes() const { return layout_.total; }
     size_t graphs_cached() const { return graphs_.size(); }
@@ -66,6 +73,8 @@ private:
     Backend* be_ = nullptr;
     bool use_graphs_ = true;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t stream2_ = nullptr;           // the BIP-340 queue's branch
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
     cudaEvent_t done_ = nullptr;
     unsigned int* d_head_ = nullptr;
     HostBuf pinned_;                 // graph-bucket staging (fixed size, graphs bind it)
@@ -76,6 +85,9 @@ private:
     bool staged_big_ = false;
     bool last_graph_ = false;
     std::map<uint64_t, cudaGraphExec_t> graphs_;
+    PubCacheSlot* cache_ = nullptr;
+    uint32_t cache_mask_ = 0;
+    unsigned long long* cache_stats_ = nullptr;
 };
 
 }  // namespace uf

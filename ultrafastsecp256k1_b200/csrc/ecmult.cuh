@@ -20,6 +20,7 @@
 #include "fe.cuh"
 #include "fn.cuh"
 #include "point.cuh"
+#include "pubcache.cuh"
 
 namespace uf {
 
@@ -124,9 +125,13 @@ UF_HD void add_gtab(Jac& R, const GT& gt, int d, bool sneg, int lam) {
     jac_add_aff(R, x, y);
 }
 
-// R = a*G + b*P for P = (px, py) on the curve (not infinity).
-template <class Tab, class GT>
-UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt) {
+// R = a*G + b*P for P = (px, py) on the curve (not infinity).  With
+// have_tab the caller already filled `tab` (a cached key) and px, py are not
+// read; otherwise the table is built here, after the digit recoding (the order
+// that keeps the kernel at 3 blocks per SM), and offered to `cache`.
+template <class Tab, class GT, class Cache>
+UF_HDI void dual_mul_c(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt,
+                       bool have_tab, const Cache& cache, bool odd) {
     GlvSplit sa, sb;
     glv_split(sa, a);
     glv_split(sb, b);
@@ -136,7 +141,10 @@ UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& 
     booth_recode<kWP, kNWP>(dp2, sb.k2);
     booth_recode<kWG, kNWG>(dg1, sa.k1);
     booth_recode<kWG, kNWG>(dg2, sa.k2);
-    build_ptable(tab, px, py);
+    if (!have_tab) {
+        build_ptable(tab, px, py);
+        cache.put(px, odd, tab);
+    }
     Fe beta;
     fe_beta(beta);
     jac_set_inf(R);
@@ -153,6 +161,11 @@ UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& 
             add_gtab(R, gt, dg2[i >> 1], sa.neg2, 1);
         }
     }
+}
+
+template <class Tab, class GT>
+UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt) {
+    dual_mul_c(R, a, px, py, b, tab, gt, false, NoPubCache(), false);
 }
 
 }  // namespace uf

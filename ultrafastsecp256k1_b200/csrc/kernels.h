@@ -83,17 +83,27 @@ struct QueueLayout {
     }
 };
 
+struct PubCacheSlot;
 struct QueueArgs {
     const uint32_t* counts;  // device header: n_e, n_s
     uint32_t cap_e, cap_s;   // region capacities: the kernel never reads past them
     const uint8_t *e_msgs, *e_pubs, *e_sigs, *s_msgs, *s_pubs, *s_sigs;
     uint8_t *e_out, *s_out;
+    // optional resident key / table cache (pubcache.cuh): slots, slot count - 1,
+    // and two counters (lookups, hits); null = no cache
+    PubCacheSlot* cache = nullptr;
+    uint32_t cache_mask = 0;
+    unsigned long long* cache_stats = nullptr;
 };
+constexpr size_t kPubCacheSlotBytes = 576;
 
-// Zeroes the queue head, then launches the persistent queue kernel (`grid`
-// resident blocks) over the items described by `a` (kernels_queue.cu).
+// Zeroes the two queue heads (d_head[0] ECDSA, d_head[1] BIP-340), then
+// launches the per-kind persistent queue kernels (`grid` resident blocks
+// each) over the items described by `a`: kinds with capacity 0 are skipped;
+// with both kinds, the BIP-340 kernel runs on s2 between a fork event recorded
+// on s and a join event s waits for (kernels_queue.cu).
 cudaError_t launch_verify_queue(const QueueArgs& a, const void* d_gtab, unsigned int* d_head, int grid,
-                                cudaStream_t s);
+                                cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
 int verify_queue_occupancy();
 
 // Allocation-free mixed verification (kernels_noalloc.cu): jobs hold

@@ -12,7 +12,9 @@
 // max_launch_items is cut into pieces that ride in successive launches.
 // Admission is bounded by a memory budget: the slots' fixed staging (pinned +
 // device, reserved at start) plus the staged bytes of the items of every launch
-// in flight stay within memory_budget_bytes.  The verdicts
+// in flight stay within memory_budget_bytes.  Decompressed keys and their
+// 1P..8P tables stay resident in a device cache shared by all slots
+// (pubcache.cuh), so repeated keys skip decompression and table set-up.  The verdicts
 // of a request are the per-kind verify's, whatever it is batched with.
 #pragma once
 #include <stddef.h>
@@ -37,6 +39,7 @@ struct ServerConfig {
     uint32_t max_launch_items = 1u << 16;
     uint64_t memory_budget_bytes = 8ull << 30;
     uint32_t batch_window_us = 0;     // wait this long for more work before launching a small batch
+    uint32_t key_cache_log2 = 0;      // resident key / table cache of 2^k slots (576 B each); 0 = none
 };
 
 struct ServerStats {
@@ -50,6 +53,7 @@ struct ServerStats {
     uint64_t reserved_bytes = 0;      // the slots' fixed staging (pinned + device)
     uint32_t peak_slots_in_flight = 0;
     uint64_t pending_requests = 0;
+    uint64_t cache_lookups = 0, cache_hits = 0;   // resident key cache, since start
 };
 
 class Server {
@@ -107,6 +111,7 @@ private:
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs_;
     std::vector<Launch> launches_;
     uint64_t budget_used_ = 0, reserved_ = 0;
+    void* d_cache_ = nullptr;        // key cache slots, then 2 counters
     // statistics
     std::vector<double> lat_us_;
     uint64_t items_done_ = 0, n_launches_ = 0, peak_budget_ = 0;

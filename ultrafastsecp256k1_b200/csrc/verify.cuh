@@ -28,16 +28,19 @@ UF_HD bool r_below_p_minus_n(const uint32_t r[8]) {
     return lt256(r, pmn);
 }
 
-// ECDSA after the signature's scalars are parsed (r, s in [1, n-1]).
-template <class Tab, class GT>
+// ECDSA after the signature's scalars are parsed (r, s in [1, n-1]).  `cache`
+// (PubCache / NoPubCache) may supply the key's table instead of decompressing
+// the key and building it.
+template <class Tab, class GT, class Cache = NoPubCache>
 UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const Sc& r, const Sc& s, Tab& tab,
-                            const GT& gt) {
+                            const GT& gt, const Cache& cache = Cache()) {
     const uint8_t prefix = pub33[0];
     if (prefix != 0x02 && prefix != 0x03) return false;
     Fe qx, qy;
     be32_to_limbs(qx.v, pub33 + 1);
     if (!limbs_lt_p(qx.v)) return false;
-    if (!lift_x_parity(qy, qx, prefix == 0x03)) return false;
+    const bool cached = cache.fetch(qx, prefix == 0x03, tab);
+    if (!cached && !lift_x_parity(qy, qx, prefix == 0x03)) return false;
     Sc z, w, u1, u2;
     words_be_to_limbs(z.v, msg_w);
     sc_reduce_once(z);
@@ -45,7 +48,7 @@ UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const
     sc_mul(u1, z, w);
     sc_mul(u2, r, w);
     Jac R;
-    dual_mul(R, u1, qx, qy, u2, tab, gt);
+    dual_mul_c(R, u1, qx, qy, u2, tab, gt, cached, cache, prefix == 0x03);
     if (R.inf) return false;
     Fe z2, t, rf;
     fe_sqr(z2, R.Z);
@@ -68,16 +71,16 @@ UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const
 
 // msg_w / sig_w: the 32 / 64 input bytes as words loaded little-endian;
 // compact big-endian r || s, low-S required.
-template <class Tab, class GT>
+template <class Tab, class GT, class Cache = NoPubCache>
 UF_HDI bool ecdsa_verify_one(const uint32_t msg_w[8], const uint8_t* pub33, const uint32_t sig_w[16],
-                             Tab& tab, const GT& gt) {
+                             Tab& tab, const GT& gt, const Cache& cache = Cache()) {
     Sc r, s;
     words_be_to_limbs(r.v, sig_w);
     words_be_to_limbs(s.v, sig_w + 8);
     if (sc_is_zero(r) || !limbs_lt_n(r.v)) return false;
     if (sc_is_zero(s) || !limbs_lt_n(s.v)) return false;
     if (!sc_is_low(s.v)) return false;
-    return ecdsa_verify_rs(msg_w, pub33, r, s, tab, gt);
+    return ecdsa_verify_rs(msg_w, pub33, r, s, tab, gt, cache);
 }
 
 // The libsecp in-memory signature layout of the consensus surfaces
@@ -100,9 +103,9 @@ UF_HDI bool ecdsa_verify_opaque_one(const uint32_t msg_w[8], const uint8_t* pub3
     return ecdsa_verify_rs(msg_w, pub33, r, s, tab, gt);
 }
 
-template <class Tab, class GT>
+template <class Tab, class GT, class Cache = NoPubCache>
 UF_HDI bool schnorr_verify_one(const uint32_t msg_w[8], const uint32_t px_w[8], const uint32_t sig_w[16],
-                               Tab& tab, const GT& gt) {
+                               Tab& tab, const GT& gt, const Cache& cache = Cache()) {
     uint32_t r[8];
     Sc s;
     words_be_to_limbs(r, sig_w);
@@ -112,7 +115,8 @@ UF_HDI bool schnorr_verify_one(const uint32_t msg_w[8], const uint32_t px_w[8], 
     Fe px, py;
     words_be_to_limbs(px.v, px_w);
     if (!limbs_lt_p(px.v)) return false;
-    if (!lift_x_parity(py, px, false)) return false;
+    const bool cached = cache.fetch(px, false, tab);
+    if (!cached && !lift_x_parity(py, px, false)) return false;
     uint32_t rbe[8], pbe[8], mbe[8], h[8];
     UF_UNROLL
     for (int i = 0; i < 8; ++i) {
@@ -127,7 +131,7 @@ UF_HDI bool schnorr_verify_one(const uint32_t msg_w[8], const uint32_t px_w[8], 
     sc_reduce_once(e);
     sc_neg(ne, e);
     Jac R;
-    dual_mul(R, s, px, py, ne, tab, gt);
+    dual_mul_c(R, s, px, py, ne, tab, gt, cached, cache, false);
     Aff A;
     if (!jac_to_aff(A, R)) return false;
     if (A.y.v[0] & 1u) return false;

@@ -19,7 +19,11 @@ extern "C" {
  * torch CUDA storage) of the same layout as the host calls; msgs, x-only keys
  * and signatures must be 16-byte aligned.  The launch is enqueued on `stream`
  * (a cudaStream_t; NULL = the context's stream) and the call returns without
- * waiting; d_out[i] = 1 / 0 once the stream reaches that point. */
+ * waiting; d_out[i] = 1 / 0 once the stream reaches that point.  Calls of at
+ * least 262,144 items are cut into launches of 131,072 that alternate between
+ * `stream` and a second stream forked from it and joined back into it, so one
+ * launch's last partial wave overlaps the next; the work stays ordered on
+ * `stream`. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_ecdsa_verify_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
                                                              const uint8_t* d_pubkeys33, const uint8_t* d_sigs64,
                                                              size_t count, uint8_t* d_out_results, void* stream);
@@ -215,7 +219,7 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* 
  * point arithmetic is inlined (instruction-cache footprint vs. call overhead).
  * ultrafastsecp256k1_b200.autotune measures them and writes the tuning file
  * read at context creation (UFSECP_B200_TUNING). */
-#define UFSECP_EXT_VERIFY_VARIANTS 6
+#define UFSECP_EXT_VERIFY_VARIANTS 7
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_variant(ufsecp_gpu_ctx* ctx, int kind, int variant);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out,
                                                      int* blocks_per_sm_out);

@@ -6,7 +6,11 @@ For each signature kind (ECDSA, BIP-340) it times every verify-kernel variant
 (ufsecp_gpu_ext_set_variant; the variants differ in how much field / point
 arithmetic is inlined, i.e. instruction-cache footprint against call
 overhead) on a GPU-signed batch, checks that all variants return identical
-verdicts, and writes the winners to a tuning file of "key value" lines:
+verdicts, and picks them; then, for RLC batch verification, it times the
+Pippenger window width (the MSM bucket width, 2^(c-1) buckets per window)
+for each batch size of 64 / 512 / 4096 / 16384 over the model's choice and
+its neighbours and picks the fastest.  The winners go to a tuning file of
+"key value" lines:
 
     ultrafastsecp256k1_b200/tuning/<device name>_<SMs>sm.txt
 
@@ -25,7 +29,8 @@ import numpy as np
 import ultrafastsecp256k1_b200 as uf
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
-VARIANTS = 6
+VARIANTS = 7
+RLC_SIZES = (64, 512, 4096, 16384)
 
 
 def tuning_path(name: str, sms: int) -> str:
@@ -71,6 +76,44 @@ def time_variant(ctx, torch, kind, bufs, n, reps=3):
     return n / (ms * 1e-3), out.cpu().numpy()
 
 
+def model_window(n: int) -> int:
+    """The backend's cost model (rlc_window_bits in csrc/rlc.cu)."""
+    best, cost = 4, float("inf")
+    for c in range(4, 17):
+        w, b = -(-129 // c), 1 << (c - 1)
+        v = (3.0 * n + 2.0) * w + 3.0 * w * b + 0.7 * (w - 1) * c
+        if v < cost:
+            best, cost = c, v
+    return best
+
+
+def tune_rlc(ctx, torch, total: int = 1 << 18, reps: int = 2) -> dict:
+    import time
+    d_m, d_p, d_s = signed_batch(ctx, torch, 1, total, seed=91)
+    d_s.view(total, 64)[::50, 40] ^= 0x04        # undo the flips: an all-valid corpus
+    torch.cuda.synchronize()
+    out = torch.zeros(total, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    res = {}
+    for size in RLC_SIZES:
+        c0 = model_window(size)
+        rates = {}
+        for c in range(max(4, c0 - 2), min(16, c0 + 2) + 1):
+            call = lambda: ctx.schnorr_verify_rlc_device(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), total,
+                                                         out.data_ptr(), batch_size=size, seed32=bytes(32),
+                                                         window_bits=c, stream=st.cuda_stream)
+            call()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                call()
+            rates[c] = total * reps / (time.perf_counter() - t0)
+            if not bool(out.all()):
+                raise RuntimeError("RLC rejected a valid corpus while tuning")
+        best = max(rates, key=rates.get)
+        res[str(size)] = {"model": c0, "best": best, "sigs_per_s": {str(k): v for k, v in rates.items()}}
+    return res
+
+
 def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = True) -> dict:
     import torch
     info = uf.device_info(0)
@@ -91,12 +134,16 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
             best = max(rates, key=rates.get)
             res["kinds"][label] = {"sigs_per_s": {str(k): r for k, r in rates.items()}, "best": best,
                                    "valid": int(ref.sum())}
+            ctx.set_variant(kind, best)
+        res["rlc_window"] = tune_rlc(ctx, torch)
     if write:
         path = out_path or tuning_path(name, info.compute_units)
         os.makedirs(os.path.dirname(path), exist_ok=True)
         with open(path, "w") as f:
             f.write(f"ecdsa_variant {res['kinds']['ecdsa']['best']}\n")
             f.write(f"schnorr_variant {res['kinds']['schnorr']['best']}\n")
+            for size, r in res["rlc_window"].items():
+                f.write(f"rlc_window_{size} {r['best']}\n")
         res["tuning_file"] = path
     return res
 

@@ -4,6 +4,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -17,12 +18,15 @@ namespace uf {
 namespace {
 // Items per host->device chunk: bounds device memory at ~130 B x 2^22 = 0.5 GB.
 constexpr size_t kPipeChunk = size_t{1} << 17;   // items per staging slot of a host-buffer call
+constexpr size_t kDeviceChunk = size_t{1} << 17; // items per launch of a large device-buffer call
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
-                                                     launch_verify_v3, launch_verify_v4, launch_verify_v5};
+                                                     launch_verify_v3, launch_verify_v4, launch_verify_v5,
+                                                     launch_verify_v6};
 const verify_occupancy_fn kOccupancy[kVerifyVariants] = {verify_occupancy_v0, verify_occupancy_v1,
                                                          verify_occupancy_v2, verify_occupancy_v3,
-                                                         verify_occupancy_v4, verify_occupancy_v5};
+                                                         verify_occupancy_v4, verify_occupancy_v5,
+                                                         verify_occupancy_v6};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -83,6 +87,9 @@ void Backend::load_tuning() {
             while (fscanf(f, "%63s %d", key, &val) == 2) {
                 if (!strcmp(key, "ecdsa_variant") && val >= 0 && val < kVerifyVariants) variant_[0] = val;
                 if (!strcmp(key, "schnorr_variant") && val >= 0 && val < kVerifyVariants) variant_[1] = val;
+                unsigned size = 0;
+                if (sscanf(key, "rlc_window_%u", &size) == 1 && size > 0 && val >= 4 && val <= 16)
+                    rlc_window_[size] = val;
             }
             fclose(f);
         }
@@ -116,6 +123,21 @@ void DevBuf::release() {
 
 Backend::Backend() = default;
 
+int Backend::rlc_window(uint32_t len) const {
+    // the tuned batch size nearest in log scale, else the cost model
+    if (rlc_window_.empty() || len == 0) return rlc_window_bits(len);
+    int best = 0;
+    double dist = 1e300;
+    for (const auto& kv : rlc_window_) {
+        const double d = fabs(log2((double)kv.first) - log2((double)len));
+        if (d < dist) {
+            dist = d;
+            best = kv.second;
+        }
+    }
+    return best;
+}
+
 RlcVerifier& Backend::rlc() {
     if (!rlc_) rlc_.reset(new RlcVerifier(this));
     return *rlc_;
@@ -134,6 +156,12 @@ Backend::~Backend() {
         out_.release();
         ops_in_.release();
         scratch_.release();
+        if (dstream_) {
+            cudaStreamSynchronize(dstream_);
+            cudaEventDestroy(dfork_);
+            cudaEventDestroy(djoin_);
+            cudaStreamDestroy(dstream_);
+        }
         for (int j = 0; j < 2; ++j) {
             if (pstream_[j]) cudaStreamSynchronize(pstream_[j]);
             pstage_[j].release();
@@ -204,8 +232,34 @@ int Backend::verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pub
     cudaError_t e = cudaSetDevice(dev_);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
     cudaStream_t s = stream ? stream : stream_;
-    e = launch_verify(kind, d_msgs, d_pubs, d_sigs, (uint32_t)count, d_out, 0, s);
-    if (e != cudaSuccess) return cuda_error(e, "verify launch");
+    if (count < 2 * kDeviceChunk) {
+        e = launch_verify(kind, d_msgs, d_pubs, d_sigs, (uint32_t)count, d_out, 0, s);
+        if (e != cudaSuccess) return cuda_error(e, "verify launch");
+        clear_error();
+        return kOk;
+    }
+    // Large calls: chunks of kDeviceChunk alternate between the caller's stream
+    // and a second stream forked from it and joined back, so that one chunk's
+    // tail (its last, partly filled wave of signatures) overlaps the next
+    // chunk's start.  Completion is still ordered on the caller's stream.
+    if (!dstream_) {
+        if ((e = cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&dfork_, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&djoin_, cudaEventDisableTiming)) != cudaSuccess)
+            return cuda_error(e, "device-call streams");
+    }
+    if ((e = cudaEventRecord(dfork_, s)) != cudaSuccess || (e = cudaStreamWaitEvent(dstream_, dfork_, 0)) != cudaSuccess)
+        return cuda_error(e, "fork");
+    const size_t pub_sz = kind == 1 ? 32 : 33;
+    size_t k = 0;
+    for (size_t off = 0; off < count; off += kDeviceChunk, ++k) {
+        const size_t m = std::min(kDeviceChunk, count - off);
+        e = launch_verify(kind, d_msgs + 32 * off, d_pubs + pub_sz * off, d_sigs + 64 * off, (uint32_t)m, d_out + off,
+                          0, (k & 1) ? dstream_ : s);
+        if (e != cudaSuccess) return cuda_error(e, "verify launch");
+    }
+    if ((e = cudaEventRecord(djoin_, dstream_)) != cudaSuccess || (e = cudaStreamWaitEvent(s, djoin_, 0)) != cudaSuccess)
+        return cuda_error(e, "join");
     clear_error();
     return kOk;
 }
@@ -371,7 +425,8 @@ int Backend::probe(int op, int blocks, int threads, int iters, float* ms) {
     cudaEventCreate(&b);
     // the probe copy built like the BIP-340 verify kernel's current variant
     static const probe_launcher kProbes[kVerifyVariants] = {launch_probe_v0, launch_probe_v1, launch_probe_v2,
-                                                            launch_probe_v3, launch_probe_v4, launch_probe_v5};
+                                                            launch_probe_v3, launch_probe_v4, launch_probe_v5,
+                                                            launch_probe_v6};
     const probe_launcher launch_probe = kProbes[variant_[1]];
     e = launch_probe(op, blocks, threads, 1, (uint32_t*)scratch_.p, stream_);   // warm-up
     if (e == cudaSuccess) {

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <map>
 #include <memory>
 #include <string>
 
@@ -77,6 +78,10 @@ public:
     int verify_jobs(const VerifyJob* jobs, size_t n_jobs);
     // RLC batch verifier of BIP-340 signatures (created on first use).
     RlcVerifier& rlc();
+    // Pippenger window bits for an RLC segment of `len` items: the tuned value
+    // of the nearest tuned batch size (tuning file lines "rlc_window_<n> <c>"),
+    // else the cost model.
+    int rlc_window(uint32_t len) const;
     int queue_grid() const { return queue_grid_; }
     // Per-item batch operations (ops.cpp): host buffers, synchronous.
     int xonly_validate(const uint8_t* keys32, size_t n, uint8_t* out);
@@ -105,7 +110,7 @@ private:
     int dev_ = -1;
     int sms_ = 0;
     std::string dev_name_;
-    int grid_[6][2] = {};        // [variant][kind] resident-grid size
+    int grid_[7][2] = {};        // [variant][kind] resident-grid size
     int variant_[2] = {4, 4};    // chosen variant per kind (4: out-of-line field / point ops, PTX chains)
     cudaError_t launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
                               uint8_t* out, int collect, cudaStream_t st);
@@ -119,9 +124,13 @@ private:
     DevBuf dstage_[2];
     cudaStream_t pstream_[2] = {nullptr, nullptr};
     cudaEvent_t pev_[2] = {nullptr, nullptr};
+    // large device-buffer calls: second stream with fork / join events
+    cudaStream_t dstream_ = nullptr;
+    cudaEvent_t dfork_ = nullptr, djoin_ = nullptr;
     int queue_grid_ = 0;
     std::unique_ptr<BatchSlot> batch_;   // slot of the synchronous mixed-batch call
     std::unique_ptr<RlcVerifier> rlc_;
+    std::map<uint32_t, int> rlc_window_;   // tuned window bits per RLC batch size
     int last_err_ = kOk;
     std::string last_msg_ = "OK";
 };

@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "backend.h"
 
@@ -173,6 +174,28 @@ int BatchSlot::enqueue(const VerifyJob* jobs, size_t n_jobs) {
     const int rc = graph ? run_graph(a, ((uint64_t)layout_.cap_e << 32) | layout_.cap_s) : run_direct(a);
     if (rc != kOk) return rc;
     if ((e = cudaEventRecord(done_, stream_)) != cudaSuccess) return be_->cuda_error(e, "event record");
+    return kOk;
+}
+
+int BatchSlot::prewarm(uint32_t max_items) {
+    if (!use_graphs_) return kOk;
+    std::vector<uint32_t> caps = {0};
+    for (uint32_t b = kMinBucket; b <= kGraphMaxItems; b <<= 1) caps.push_back(b);
+    cudaError_t e = cudaSetDevice(be_->device());
+    if (e != cudaSuccess) return be_->cuda_error(e, "cudaSetDevice");
+    for (uint32_t ce : caps) {
+        for (uint32_t cs : caps) {
+            if ((ce == 0 && cs == 0) || (uint64_t)ce + cs > 2ull * std::max(max_items, kMinBucket)) continue;
+            layout_ = QueueLayout(ce, cs);
+            staged_big_ = false;
+            uint32_t* hdr = reinterpret_cast<uint32_t*>(pinned_.p);
+            hdr[0] = 0;
+            hdr[1] = 0;
+            const int rc = run_graph(args_for((uint8_t*)dev_.p), ((uint64_t)ce << 32) | cs);
+            if (rc != kOk) return rc;
+        }
+    }
+    if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return be_->cuda_error(e, "prewarm");
     return kOk;
 }
 

@@ -48,6 +48,10 @@ public:
     // Packs `jobs` and enqueues the work; returns immediately.  The jobs' host
     // buffers must stay valid until finish() returns.
     int enqueue(const VerifyJob* jobs, size_t n_jobs);
+    // Captures and runs (with zero items) the graph of every capacity bucket
+    // pair whose total is at most max_items, so that later launches of any
+    // shape find their graph instantiated and their kernels loaded.
+    int prewarm(uint32_t max_items);
     // True once the enqueued work has completed on the device.
     bool ready();
     // Waits for the enqueued work and writes every job's verdicts.

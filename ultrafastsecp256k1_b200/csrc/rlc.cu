@@ -677,7 +677,7 @@ int RlcVerifier::verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_
     while (!seg.empty()) {
         uint32_t maxlen = 0;
         for (size_t k = 1; k < seg.size(); k += 2) maxlen = std::max(maxlen, seg[k]);
-        const int c = window_bits > 0 ? window_bits : rlc_window_bits(maxlen);
+        const int c = window_bits > 0 ? window_bits : be_->rlc_window(maxlen);
         const int rc = run_round(seg, c, s, ok_host_);
         if (rc != kOk) return rc;
         if (stats) {
@@ -803,7 +803,7 @@ int RlcVerifier::msm_host(const uint8_t* scalars32, const uint8_t* points33, uin
     }
     n_ = n;
     const std::vector<uint32_t> seg = {0u, n};
-    const int rc = run_round(seg, rlc_window_bits(n), s, ok_host_);
+    const int rc = run_round(seg, be_->rlc_window(n), s, ok_host_);
     if (rc != kOk) return rc;
     uint8_t* d_out = (uint8_t*)gate_.p + 16;
     uint8_t ok = 0;

@@ -56,6 +56,12 @@ int Server::start(const ServerConfig& cfg) {
         if (d_cache_)
             L.slot->set_cache((PubCacheSlot*)d_cache_, (uint32_t)(cache_slots - 1),
                               (unsigned long long*)((uint8_t*)d_cache_ + cache_slots * kPubCacheSlotBytes));
+        // instantiate every launch shape now, not on a request's critical path
+        const int pw = L.slot->prewarm(cfg_.max_launch_items);
+        if (pw != kOk) {
+            launches_.clear();
+            return pw;
+        }
     }
     reserved_ = slot_bytes * launches_.size() + cache_bytes;
     budget_used_ = reserved_;

@@ -21,6 +21,16 @@
 #ifndef UF_VARIANT
 #define UF_VARIANT 0
 #endif
+// Block size and the minimum resident blocks per SM asked of the register
+// allocator.  The default is 128 threads with no register cap (3 blocks per SM:
+// registers and the 512-byte per-thread table both limit it); 64-thread blocks
+// capped at 128 registers fit 7 blocks, 14 warps per SM.
+#ifndef UF_PLAIN_THREADS
+#define UF_PLAIN_THREADS kVerifyThreads
+#endif
+#ifndef UF_MIN_BLOCKS
+#define UF_MIN_BLOCKS 1
+#endif
 #define UF_CAT2(a, b) a##b
 #define UF_CAT(a, b) UF_CAT2(a, b)
 
@@ -29,7 +39,7 @@ namespace UF_CAT(vk, UF_VARIANT) {
 
 // kKind: 0 ECDSA (compact r || s), 1 BIP-340, 2 ECDSA (opaque little-endian r, s; high-S accepted)
 template <int kKind>
-__global__ void __launch_bounds__(kVerifyThreads)
+__global__ void __launch_bounds__(UF_PLAIN_THREADS, UF_MIN_BLOCKS)
 k_verify(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs, const uint8_t* __restrict__ sigs,
          uint32_t n, const uint4* __restrict__ gt, uint8_t* __restrict__ out, int collect) {
     extern __shared__ uint4 smem_tab[];
@@ -65,33 +75,33 @@ cudaError_t UF_CAT(launch_verify_v, UF_VARIANT)(int kind, const uint8_t* msgs, c
                                                 int collect, int grid, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     // the shared-memory opt-in was set per device by verify_occupancy_v*() at context creation
-    const size_t smem = kVerifyThreads * kVerifySmemPerThread;
-    const int need = (int)((n + kVerifyThreads - 1) / kVerifyThreads);
+    const size_t smem = UF_PLAIN_THREADS * kVerifySmemPerThread;
+    const int need = (int)((n + UF_PLAIN_THREADS - 1) / UF_PLAIN_THREADS);
     if (grid <= 0 || grid > need) grid = need;
     const uint4* gt = reinterpret_cast<const uint4*>(d_gtab);
     if (kind == 0)
-        UF_CAT(vk, UF_VARIANT)::k_verify<0><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+        UF_CAT(vk, UF_VARIANT)::k_verify<0><<<grid, UF_PLAIN_THREADS, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
     else if (kind == 2)
-        UF_CAT(vk, UF_VARIANT)::k_verify<2><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+        UF_CAT(vk, UF_VARIANT)::k_verify<2><<<grid, UF_PLAIN_THREADS, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
     else
-        UF_CAT(vk, UF_VARIANT)::k_verify<1><<<grid, kVerifyThreads, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
+        UF_CAT(vk, UF_VARIANT)::k_verify<1><<<grid, UF_PLAIN_THREADS, smem, s>>>(msgs, pubs, sigs, n, gt, out, collect);
     return cudaGetLastError();
 }
 
 int UF_CAT(verify_occupancy_v, UF_VARIANT)(int kind) {
     int blocks = 0;
-    const size_t smem = kVerifyThreads * kVerifySmemPerThread;
+    const size_t smem = UF_PLAIN_THREADS * kVerifySmemPerThread;
     if (kind != 1) {
         // the opaque ECDSA instance shares kind 0's shape; opt both in
         auto f2 = UF_CAT(vk, UF_VARIANT)::k_verify<2>;
         cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         auto f = UF_CAT(vk, UF_VARIANT)::k_verify<0>;
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, kVerifyThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, UF_PLAIN_THREADS, smem);
     } else {
         auto f = UF_CAT(vk, UF_VARIANT)::k_verify<1>;
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, kVerifyThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, f, UF_PLAIN_THREADS, smem);
     }
     return blocks;
 }

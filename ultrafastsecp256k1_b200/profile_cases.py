@@ -70,7 +70,7 @@ def case_verify(ctx, torch, a):
 
 
 def case_rlc(ctx, torch, a):
-    n_bad = (a.n // a.batch) // 8
+    n_bad = (a.n // a.batch) // a.bad_every if a.bad_every else 0
     d_m, d_x, d_s, expect, _ = _signed(ctx, torch, 1, a.n, 2, n_bad)
     d_o = torch.zeros(a.n, dtype=torch.uint8, device="cuda")
     st = torch.cuda.Stream()
@@ -120,6 +120,7 @@ def main():
     ap.add_argument("--n", type=int, default=1 << 18)
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--bad-every", type=int, default=8, help="rlc: one invalid signature per this many batches (0: none)")
     a = ap.parse_args()
     import torch
     with uf.GpuContext(0) as ctx:

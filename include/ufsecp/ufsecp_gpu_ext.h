@@ -219,7 +219,7 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* 
  * point arithmetic is inlined (instruction-cache footprint vs. call overhead).
  * ultrafastsecp256k1_b200.autotune measures them and writes the tuning file
  * read at context creation (UFSECP_B200_TUNING). */
-#define UFSECP_EXT_VERIFY_VARIANTS 8
+#define UFSECP_EXT_VERIFY_VARIANTS 9
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_variant(ufsecp_gpu_ctx* ctx, int kind, int variant);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out,
                                                      int* blocks_per_sm_out);

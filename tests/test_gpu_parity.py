@@ -282,7 +282,7 @@ def test_abi_gating_with_context(gpu_ctx):
     assert info.compute_units > 0 and info.global_mem_bytes > 0
 
 
-@pytest.mark.parametrize("variant", range(8))
+@pytest.mark.parametrize("variant", range(9))
 def test_every_kernel_variant_matches_oracle(gpu_ctx, oracle, variant):
     """The code-size variants (ufsecp_gpu_ext_set_variant) compute identical verdicts."""
     _, wy, e = load_golden()

@@ -29,7 +29,7 @@ import numpy as np
 import ultrafastsecp256k1_b200 as uf
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
-VARIANTS = 8
+VARIANTS = 9
 RLC_SIZES = (64, 512, 4096, 16384)
 
 

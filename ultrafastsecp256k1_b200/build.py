@@ -48,6 +48,8 @@ _VARIANT_FLAGS = [
         ("v6", ["-DUF_VARIANT=6", "-DUF_NOINLINE_POINT", "-DUF_PTX_MUL"]),
         ("v7", ["-DUF_VARIANT=7", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL",
                 "-DUF_PLAIN_THREADS=64", "-DUF_MIN_BLOCKS=7"]),
+        ("v8", ["-DUF_VARIANT=8", "-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL", "-DUF_TAB7",
+                "-DUF_PLAIN_THREADS=128", "-DUF_MIN_BLOCKS=4"]),
 ]
 # the batched / served kernels are built once, with the code generation that
 # measured fastest for the per-signature kernel on B200 (variant 4)

@@ -22,11 +22,12 @@ constexpr size_t kDeviceChunk = size_t{1} << 17; // items per launch of a large 
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
                                                      launch_verify_v3, launch_verify_v4, launch_verify_v5,
-                                                     launch_verify_v6, launch_verify_v7};
+                                                     launch_verify_v6, launch_verify_v7, launch_verify_v8};
 const verify_occupancy_fn kOccupancy[kVerifyVariants] = {verify_occupancy_v0, verify_occupancy_v1,
                                                          verify_occupancy_v2, verify_occupancy_v3,
                                                          verify_occupancy_v4, verify_occupancy_v5,
-                                                         verify_occupancy_v6, verify_occupancy_v7};
+                                                         verify_occupancy_v6, verify_occupancy_v7,
+                                                         verify_occupancy_v8};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -426,7 +427,7 @@ int Backend::probe(int op, int blocks, int threads, int iters, float* ms) {
     // the probe copy built like the BIP-340 verify kernel's current variant
     static const probe_launcher kProbes[kVerifyVariants] = {launch_probe_v0, launch_probe_v1, launch_probe_v2,
                                                             launch_probe_v3, launch_probe_v4, launch_probe_v5,
-                                                            launch_probe_v6, launch_probe_v7};
+                                                            launch_probe_v6, launch_probe_v7, launch_probe_v8};
     const probe_launcher launch_probe = kProbes[variant_[1]];
     e = launch_probe(op, blocks, threads, 1, (uint32_t*)scratch_.p, stream_);   // warm-up
     if (e == cudaSuccess) {

@@ -110,7 +110,7 @@ private:
     int dev_ = -1;
     int sms_ = 0;
     std::string dev_name_;
-    int grid_[8][2] = {};        // [variant][kind] resident-grid size
+    int grid_[9][2] = {};        // [variant][kind] resident-grid size
     int variant_[2] = {4, 4};    // chosen variant per kind (4: out-of-line field / point ops, PTX chains)
     cudaError_t launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
                               uint8_t* out, int collect, cudaStream_t st);

@@ -30,6 +30,39 @@ struct SmemTab {
     }
 };
 
+// 1P in registers, 2P..8P in shared memory: 448 bytes per thread instead of
+// 512, so four 128-thread blocks fit an SM's shared memory.
+struct SmemTab7 {
+    uint4* base;        // this thread's column
+    uint32_t stride;    // blockDim.x
+    Fe x0, y0;
+    __device__ __forceinline__ void store(int k, const Fe& x, const Fe& y) {
+        if (k == 0) {
+            x0 = x;
+            y0 = y;
+            return;
+        }
+        uint4* p = base + (uint32_t)((k - 1) * 4) * stride;
+        p[0] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+        p[stride] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+        p[2 * stride] = make_uint4(y.v[0], y.v[1], y.v[2], y.v[3]);
+        p[3 * stride] = make_uint4(y.v[4], y.v[5], y.v[6], y.v[7]);
+    }
+    __device__ __forceinline__ void load(int k, Fe& x, Fe& y) const {
+        if (k == 0) {
+            x = x0;
+            y = y0;
+            return;
+        }
+        const uint4* p = base + (uint32_t)((k - 1) * 4) * stride;
+        uint4 a = p[0], b = p[stride], c = p[2 * stride], d = p[3 * stride];
+        x.v[0] = a.x; x.v[1] = a.y; x.v[2] = a.z; x.v[3] = a.w;
+        x.v[4] = b.x; x.v[5] = b.y; x.v[6] = b.z; x.v[7] = b.w;
+        y.v[0] = c.x; y.v[1] = c.y; y.v[2] = c.z; y.v[3] = c.w;
+        y.v[4] = d.x; y.v[5] = d.y; y.v[6] = d.z; y.v[7] = d.w;
+    }
+};
+
 struct GlobalGT {
     const uint4* __restrict__ p;
     __device__ __forceinline__ void load(int k, Fe& x, Fe& y) const {

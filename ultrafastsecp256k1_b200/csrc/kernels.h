@@ -23,7 +23,7 @@ cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s);
 // for a valid signature, 0 otherwise.  With collect != 0 a valid signature
 // writes 0 and an invalid one leaves out[i] untouched.  Variants 0..5 are the
 // same kernel built with different code-size choices (kernels_verify.cu).
-constexpr int kVerifyVariants = 8;
+constexpr int kVerifyVariants = 9;
 typedef cudaError_t (*verify_launcher)(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs,
                                        uint32_t n, const void* d_gtab, uint8_t* out, int collect, int grid,
                                        cudaStream_t s);
@@ -44,6 +44,8 @@ cudaError_t launch_verify_v6(int, const uint8_t*, const uint8_t*, const uint8_t*
                              int, int, cudaStream_t);
 cudaError_t launch_verify_v7(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
                              int, int, cudaStream_t);
+cudaError_t launch_verify_v8(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
 int verify_occupancy_v0(int kind);
 int verify_occupancy_v1(int kind);
 int verify_occupancy_v2(int kind);
@@ -52,6 +54,7 @@ int verify_occupancy_v4(int kind);
 int verify_occupancy_v5(int kind);
 int verify_occupancy_v6(int kind);
 int verify_occupancy_v7(int kind);
+int verify_occupancy_v8(int kind);
 
 // Per-item batch operations (kernels_ops.cu); device pointers, asynchronous.
 cudaError_t launch_xonly_validate(const uint8_t* keys32, uint32_t n, uint8_t* out, int sms, cudaStream_t s);
@@ -151,5 +154,6 @@ cudaError_t launch_probe_v4(int, int, int, int, uint32_t*, cudaStream_t);
 cudaError_t launch_probe_v5(int, int, int, int, uint32_t*, cudaStream_t);
 cudaError_t launch_probe_v6(int, int, int, int, uint32_t*, cudaStream_t);
 cudaError_t launch_probe_v7(int, int, int, int, uint32_t*, cudaStream_t);
+cudaError_t launch_probe_v8(int, int, int, int, uint32_t*, cudaStream_t);
 
 }  // namespace uf

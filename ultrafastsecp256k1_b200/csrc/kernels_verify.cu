@@ -28,8 +28,18 @@
 #ifndef UF_PLAIN_THREADS
 #define UF_PLAIN_THREADS kVerifyThreads
 #endif
-#ifndef UF_MIN_BLOCKS
-#define UF_MIN_BLOCKS 1
+#ifdef UF_MIN_BLOCKS
+#define UF_BOUNDS __launch_bounds__(UF_PLAIN_THREADS, UF_MIN_BLOCKS)
+#else
+#define UF_BOUNDS __launch_bounds__(UF_PLAIN_THREADS)
+#endif
+// UF_TAB7: 1P kept in registers, 448 bytes of shared memory per thread.
+#ifdef UF_TAB7
+#define UF_TAB_T SmemTab7
+#define UF_SMEM_PER_THREAD 448
+#else
+#define UF_TAB_T const SmemTab
+#define UF_SMEM_PER_THREAD kVerifySmemPerThread
 #endif
 #define UF_CAT2(a, b) a##b
 #define UF_CAT(a, b) UF_CAT2(a, b)
@@ -39,11 +49,11 @@ namespace UF_CAT(vk, UF_VARIANT) {
 
 // kKind: 0 ECDSA (compact r || s), 1 BIP-340, 2 ECDSA (opaque little-endian r, s; high-S accepted)
 template <int kKind>
-__global__ void __launch_bounds__(UF_PLAIN_THREADS, UF_MIN_BLOCKS)
+__global__ void UF_BOUNDS
 k_verify(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs, const uint8_t* __restrict__ sigs,
          uint32_t n, const uint4* __restrict__ gt, uint8_t* __restrict__ out, int collect) {
     extern __shared__ uint4 smem_tab[];
-    const SmemTab tab{smem_tab + threadIdx.x, blockDim.x};
+    UF_TAB_T tab{smem_tab + threadIdx.x, blockDim.x};
     const GlobalGT g{gt};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t mw[8], sw[16];
@@ -75,7 +85,7 @@ cudaError_t UF_CAT(launch_verify_v, UF_VARIANT)(int kind, const uint8_t* msgs, c
                                                 int collect, int grid, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     // the shared-memory opt-in was set per device by verify_occupancy_v*() at context creation
-    const size_t smem = UF_PLAIN_THREADS * kVerifySmemPerThread;
+    const size_t smem = UF_PLAIN_THREADS * UF_SMEM_PER_THREAD;
     const int need = (int)((n + UF_PLAIN_THREADS - 1) / UF_PLAIN_THREADS);
     if (grid <= 0 || grid > need) grid = need;
     const uint4* gt = reinterpret_cast<const uint4*>(d_gtab);
@@ -90,7 +100,7 @@ cudaError_t UF_CAT(launch_verify_v, UF_VARIANT)(int kind, const uint8_t* msgs, c
 
 int UF_CAT(verify_occupancy_v, UF_VARIANT)(int kind) {
     int blocks = 0;
-    const size_t smem = UF_PLAIN_THREADS * kVerifySmemPerThread;
+    const size_t smem = UF_PLAIN_THREADS * UF_SMEM_PER_THREAD;
     if (kind != 1) {
         // the opaque ECDSA instance shares kind 0's shape; opt both in
         auto f2 = UF_CAT(vk, UF_VARIANT)::k_verify<2>;

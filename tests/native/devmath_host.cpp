@@ -105,7 +105,7 @@ void hm_glv(const uint8_t* k, uint8_t* k1, uint8_t* k2, uint8_t* negs) {
     limbs_to_be32(buf, t); memcpy(k2, buf + 16, 16);
     negs[0] = g.neg1; negs[1] = g.neg2;
 }
-// booth digits of a 128-bit magnitude (16 bytes BE), w = 4 (33 digits) or 8 (17 digits)
+// booth digits of a 128-bit magnitude (16 bytes BE), w = 4 (33 digits) or the G window (UF_GWIN)
 void hm_booth(const uint8_t* k16, int w, int32_t* out) {
     uint8_t buf[32] = {0};
     memcpy(buf + 16, k16, 16);

@@ -12,8 +12,8 @@
 //    data-dependent positions would make the warp add at almost every bit);
 //  * P streams: 4-bit windows, table of 1P..8P (affine, one field inversion per
 //    signature through a batch-to-affine), lambda P via one beta multiplication;
-//  * G streams: 8-bit windows every second P window, tables of 1..128 multiples
-//    of G and of lambda G computed once per context and read through the L1;
+//  * G streams: UF_GWIN-bit windows (12: every third P window), tables of the 2^(UF_GWIN-1) multiples
+//    of G and of lambda G computed once per context and read through L1 / L2;
 //  * 33 P windows x 4 bits = 132 >= 129 bits, so 128 doublings in total.
 #pragma once
 #include "common.cuh"
@@ -26,10 +26,13 @@ namespace uf {
 
 constexpr int kWP = 4;     // P window bits
 constexpr int kNWP = 33;   // P windows
-constexpr int kWG = 8;     // G window bits
-constexpr int kNWG = 17;   // G windows (one per two P windows)
+constexpr int kWG = UF_GWIN;                  // G window bits (a multiple of kWP)
+constexpr int kNWG = (129 + kWG - 1) / kWG;   // G windows: 17 for 8 bits (one per two P windows)
+constexpr int kGEvery = kWG / kWP;            // P windows per G window
+static_assert(kWG % kWP == 0 && kNWG * kGEvery >= kNWP, "G windows must align with P windows");
+static_assert(kWG <= 15, "G Booth digits (up to 2^(kWG-1)) are stored as int16_t");
 constexpr int kPTab = 8;   // 1P..8P
-constexpr int kGTab = 128; // 1G..128G (and the same for lambda G)
+constexpr int kGTab = 1 << (kWG - 1); // 1G..2048G for 12-bit windows (and the same for lambda G)
 
 // Signed fixed-window (Booth) digits of a magnitude k < 2^129:
 // d_i = b_{wi-1} + sum_{t<w-1} b_{wi+t} 2^t - b_{wi+w-1} 2^(w-1), d_i in [-2^(w-1), 2^(w-1)],
@@ -156,9 +159,9 @@ UF_HDI void dual_mul_c(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc
         }
         add_ptab(R, tab, dp1[i], sb.neg1, false, beta);
         add_ptab(R, tab, dp2[i], sb.neg2, true, beta);
-        if ((i & 1) == 0) {
-            add_gtab(R, gt, dg1[i >> 1], sa.neg1, 0);
-            add_gtab(R, gt, dg2[i >> 1], sa.neg2, 1);
+        if (i % kGEvery == 0) {
+            add_gtab(R, gt, dg1[i / kGEvery], sa.neg1, 0);
+            add_gtab(R, gt, dg2[i / kGEvery], sa.neg2, 1);
         }
     }
 }

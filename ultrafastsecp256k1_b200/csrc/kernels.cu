@@ -8,19 +8,22 @@
 namespace uf {
 
 // ---------------------------------------------------------------- G tables --
-// thread t < 128: (t+1)*G ; t >= 128: (t-127)*lambda*G = (beta x, y)
+// entry t < kGTab: (t+1)*G ; t >= kGTab: (t-kGTab+1)*lambda*G = (beta x, y)
 __global__ void k_gtable_init(uint4* out) {
-    const int t = threadIdx.x;
-    if (t >= 256) return;
-    const int m = (t & 127) + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * kGTab) return;
+    const int m = (t & (kGTab - 1)) + 1;
     Aff G;
     gen_point(G);
     Jac acc;
     jac_set_inf(acc);
-    for (int i = 0; i < m; ++i) jac_add_aff(acc, G.x, G.y);
+    for (int b = 31 - __clz(m); b >= 0; --b) {     // left-to-right double and add
+        jac_dbl(acc);
+        if ((m >> b) & 1) jac_add_aff(acc, G.x, G.y);
+    }
     Aff A;
     jac_to_aff(A, acc);
-    if (t >= 128) {
+    if (t >= kGTab) {
         Fe beta;
         fe_beta(beta);
         fe_mul(A.x, A.x, beta);
@@ -34,7 +37,7 @@ __global__ void k_gtable_init(uint4* out) {
 }
 
 cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s) {
-    k_gtable_init<<<1, 256, 0, s>>>(reinterpret_cast<uint4*>(d_gtab));
+    k_gtable_init<<<(2 * kGTab + 255) / 256, 256, 0, s>>>(reinterpret_cast<uint4*>(d_gtab));
     return cudaGetLastError();
 }
 

@@ -4,11 +4,14 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "common.cuh"
+
 namespace uf {
 
-// Byte size of the per-context generator tables: 128 multiples of G and of
-// lambda*G, affine, 64 bytes each.
-constexpr size_t kGTableBytes = 2 * 128 * 64;
+// Byte size of the per-context generator tables: 2^(UF_GWIN-1) multiples of G
+// and of lambda*G, affine, 64 bytes each.
+constexpr size_t kGTableEntries = size_t{1} << (UF_GWIN - 1);   // per table (G, lambda G)
+constexpr size_t kGTableBytes = 2 * kGTableEntries * 64;
 
 // Threads per block of the per-signature verify kernels and the dynamic
 // shared memory each block needs (8 table points x 64 bytes per thread).

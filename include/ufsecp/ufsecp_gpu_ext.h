@@ -233,7 +233,10 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* 
  * returns the launch time in milliseconds (CUDA events).  op: 1 two fe_mul
  * chains, 2 two fe_sqr chains, 3 fe_inv, 4 sqrt exponentiation, 5 Jacobian
  * doubling, 6 Jacobian + affine add, 7 scalar inverse, 8 GLV split,
- * 9 BIP-340 challenge hash. */
+ * 9 BIP-340 challenge hash; integer multiply-add forms, 8 per round with
+ * data-dependent multipliers: 10 mad.lo.u32, 11 mad.hi.u32, 12 mad.wide.u32,
+ * 13 mad.lo.cc / madc.hi.cc carry chain, 14 operand-scanning step
+ * (32x32 + 32 + 32 -> 64). */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int blocks, int threads, int iters,
                                                float* ms_out);
 
@@ -246,6 +249,8 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int 
  *  8  k (32) -> (k*G).x | (k*G).y (64), zeros for infinity
  *  9  a|x|b (96) -> finite (1) | x (32) | y (32) of a*G + b*P, P = lift_x(x)
  * 10  r|p|m (96) -> BIP-340 challenge digest (32)
+ * 11  a|b (64) -> a*b | a^2 | a+b | a-b mod p (128), through the field code
+ *     of the verify kernels (PTX carry chains), inputs any 256-bit values
  * All values big-endian. */
 #define UFSECP_EXT_DIAG_FE_MUL    1
 #define UFSECP_EXT_DIAG_FE_SQR    2
@@ -257,6 +262,7 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int 
 #define UFSECP_EXT_DIAG_GEN_MUL   8
 #define UFSECP_EXT_DIAG_DUAL_MUL  9
 #define UFSECP_EXT_DIAG_CHALLENGE 10
+#define UFSECP_EXT_DIAG_FE_PTX    11
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_diag(ufsecp_gpu_ctx* ctx, uint32_t op, const uint8_t* in, size_t n,
                                               uint8_t* out);
 

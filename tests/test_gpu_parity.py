@@ -48,6 +48,97 @@ def test_diag_field_and_scalar(gpu_ctx):
     assert [int.from_bytes(r.tobytes(), "big") for r in out] == [pow(x, -1, N) for x in nzn]
 
 
+M32 = (1 << 32) - 1
+K = (1 << 32) + 977
+
+
+def _fold_paths(t):
+    """Which rare paths the device reduction of the 512-bit t takes in its
+    second fold: (top >= 2^32, carry past limb 2, wrap past 2^256)."""
+    L, H = t % 2**256, t >> 256
+    sf = L + 977 * H + (H << 32)
+    s, top = sf % 2**256, sf >> 256
+    tl, th = top & M32, top >> 32
+    s0, s1, s2 = s & M32, (s >> 32) & M32, (s >> 64) & M32
+    x = s0 + ((tl * 977) & M32)
+    y = s1 + ((tl * 977) >> 32) + (x >> 32)
+    z = s2 + th + (y >> 32)
+    c = z >> 32
+    y2 = (y & M32) + tl
+    c += ((z & M32) + (y2 >> 32)) >> 32
+    return th, c, (s + top * K) >> 256
+
+
+def _add_paths(a, b):
+    """(carry past limb 1 after the +K fold, second wrap) of the device a + b."""
+    sm = a + b
+    if sm < 2**256:
+        return 0, 0
+    r = sm - 2**256
+    return int(((r & (2**64 - 1)) + K) >> 64), int(r + K >= 2**256)
+
+
+def _sub_paths(a, b):
+    """(borrow past limb 1 after the -K fold, second borrow) of the device a - b."""
+    if a >= b:
+        return 0, 0
+    r = a - b + 2**256
+    return int((r & (2**64 - 1)) < K), int(r < K)
+
+
+def _hard_field_pairs(rng):
+    """Operand pairs that drive the device field code into its rare carry paths."""
+    pairs = []
+    # reduction, carry past limb 2 in the second fold: b = 2^96 and a chosen so
+    # that L + H*K = 2^256 + s with limbs 1 and 2 of s all ones
+    kinv = pow(K, -1, 2**96)
+    for _ in range(64):
+        X = int(rng.integers(0, 2**32)) | (M32 << 32) | (M32 << 64)
+        H = X * kinv % 2**96
+        if H * K <= X:
+            continue
+        L = 2**256 + X - H * K
+        pairs.append(((H << 160) | (L >> 96), 2**96))
+    # top >= 2^32 and a wrap: operands near 2^256
+    for d1 in range(0, 40, 3):
+        for d2 in range(0, 40, 7):
+            pairs.append((2**256 - 1 - d1, 2**256 - 1 - d2))
+    # add: sums 2^256 + r with limb 1 of r all ones, and r >= 2^256 - K
+    for _ in range(32):
+        r = int.from_bytes(rng.bytes(32), "big") | (M32 << 32)
+        pairs.append((2**256 - 1, (r + 1) % 2**256))
+    pairs += [(2**256 - 1, 2**256 - 1 - d) for d in range(0, 3000, 97)]
+    # sub: borrows with limb 1 of a - b + 2^256 zero, and a tiny with b near 2^256
+    for _ in range(32):
+        r = int.from_bytes(rng.bytes(32), "big") & ~(M32 << 32)
+        a = int(rng.integers(0, 2**20))
+        pairs.append((a, (a - r) % 2**256))
+    pairs += [(d, 2**256 - 1 - e) for d in range(0, 5) for e in range(0, 2000, 401)]
+    return pairs
+
+
+def test_diag_ptx_field_rare_paths(gpu_ctx):
+    """The field code the verify kernels run (PTX carry chains) on random
+    weakly reduced operands and on pairs built to reach every rare carry path
+    of the reduction, the add and the sub; the models above confirm that each
+    path is reached."""
+    rng = np.random.default_rng(11)
+    pairs = _hard_field_pairs(rng)
+    pairs += [(int.from_bytes(rng.bytes(32), "big"), int.from_bytes(rng.bytes(32), "big")) for _ in range(2000)]
+    special = [0, 1, 2, P - 1, P, P + 1, 2**256 - 1, 2**255, N - 1, N, K, 2**256 - K]
+    pairs += [(x, y) for x in special for y in special]
+    fold = [_fold_paths(a * b) for a, b in pairs] + [_fold_paths(a * a) for a, _ in pairs]
+    assert all(any(f[k] for f in fold) for k in range(3)), "a reduction path is not reached"
+    assert all(any(_add_paths(a, b)[k] for a, b in pairs) for k in range(2)), "an add path is not reached"
+    assert all(any(_sub_paths(a, b)[k] for a, b in pairs) for k in range(2)), "a sub path is not reached"
+    data = np.frombuffer(b"".join(be(a) + be(b) for a, b in pairs), np.uint8)
+    out = gpu_ctx.diag(11, data)
+    got = [[int.from_bytes(r[32 * k:32 * k + 32].tobytes(), "big") for k in range(4)] for r in out]
+    want = [[a * b % P, a * a % P, (a + b) % P, (a - b) % P] for a, b in pairs]
+    bad = [(i, pairs[i]) for i in range(len(pairs)) if got[i] != want[i]]
+    assert not bad, bad[:4]
+
+
 def test_diag_sqrt_glv_challenge(gpu_ctx):
     import hashlib
     rng = np.random.default_rng(2)

@@ -587,7 +587,7 @@ ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) 
 
 ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int blocks, int threads, int iters, float* ms_out) {
     if (!ctx || !ms_out) return UFSECP_ERR_NULL_ARG;
-    if (op < 1 || op > 9 || blocks < 1 || threads < 1 || threads > 1024 || iters < 1) return UFSECP_ERR_BAD_INPUT;
+    if (op < 1 || op > 14 || blocks < 1 || threads < 1 || threads > 1024 || iters < 1) return UFSECP_ERR_BAD_INPUT;
     return ctx->backend->probe(op, blocks, threads, iters, ms_out);
 }
 
@@ -595,9 +595,9 @@ ufsecp_error_t ufsecp_gpu_ext_diag(ufsecp_gpu_ctx* ctx, uint32_t op, const uint8
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     if (n == 0) return UFSECP_OK;
     if (!in || !out) return UFSECP_ERR_NULL_ARG;
-    static const int in_sz[11] = {0, 64, 32, 32, 32, 64, 32, 32, 32, 96, 96};
-    static const int out_sz[11] = {0, 32, 32, 32, 33, 32, 32, 34, 64, 65, 32};
-    if (op < 1 || op > 10 || n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    static const int in_sz[12] = {0, 64, 32, 32, 32, 64, 32, 32, 32, 96, 96, 64};
+    static const int out_sz[12] = {0, 32, 32, 32, 33, 32, 32, 34, 64, 65, 32, 128};
+    if (op < 1 || op > 11 || n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
     return ctx->backend->diag(op, in, n, out, (size_t)in_sz[op], (size_t)out_sz[op]);
 }
 

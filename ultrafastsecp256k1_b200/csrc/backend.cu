@@ -379,8 +379,9 @@ int Backend::diag(uint32_t op, const uint8_t* in, size_t n, uint8_t* out, size_t
     if ((e = out_.ensure(n * out_sz + 16)) != cudaSuccess) return cuda_error(e, "cudaMalloc");
     if ((e = cudaMemcpyAsync(msgs_.p, in, n * in_sz, cudaMemcpyHostToDevice, stream_)) != cudaSuccess)
         return cuda_error(e, "copy");
-    if ((e = launch_diag(op, (const uint8_t*)msgs_.p, (uint32_t)n, (uint8_t*)out_.p, d_gtab_, stream_)) != cudaSuccess)
-        return cuda_error(e, "diag launch");
+    e = op == 11 ? launch_field_diag((const uint8_t*)msgs_.p, (uint32_t)n, (uint8_t*)out_.p, sms_, stream_)
+                 : launch_diag(op, (const uint8_t*)msgs_.p, (uint32_t)n, (uint8_t*)out_.p, d_gtab_, stream_);
+    if (e != cudaSuccess) return cuda_error(e, "diag launch");
     if ((e = cudaMemcpyAsync(out, out_.p, n * out_sz, cudaMemcpyDeviceToHost, stream_)) != cudaSuccess)
         return cuda_error(e, "copy");
     if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return cuda_error(e, "diag");

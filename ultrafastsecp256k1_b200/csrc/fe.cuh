@@ -138,7 +138,10 @@ UF_HD void fe_fold_top(Fe& r, uint32_t s[8], uint64_t s8) {
 UF_HD void fe_reduce512(Fe& r, const uint32_t t[16]) {
     uint32_t s[8];
 #if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
-    const uint64_t s8 = fold_977_ptx(s, t);
+    fold_top_ptx(s, fold_977_ptx(s, t));
+    UF_UNROLL
+    for (int j = 0; j < 8; ++j) r.v[j] = s[j];
+    return;
 #else
     uint64_t c = (uint64_t)t[8] * 977u + t[0];
     s[0] = lo32(c);
@@ -150,8 +153,8 @@ UF_HD void fe_reduce512(Fe& r, const uint32_t t[16]) {
         c >>= 32;
     }
     const uint64_t s8 = c + t[15];          // < 2^45: weight 2^256
-#endif
     fe_fold_top(r, s, s8);
+#endif
 }
 
 // 256x256 -> 512 schoolbook product (operand scanning, 64-bit accumulators:

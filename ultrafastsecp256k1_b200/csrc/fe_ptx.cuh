@@ -115,10 +115,53 @@ __device__ __forceinline__ uint64_t fold_977_ptx(uint32_t s[8], const uint32_t t
     return ((uint64_t)s9 << 32) | s8;
 }
 
+// Second fold: s[0..7] + top * 2^256 -> weakly reduced s, for the top
+// (< 2^32 + 978) that fold_977_ptx returns.  top * K (K = 2^32 + 977) lands on
+// limbs 0..2: lo(tl*977) on 0, hi(tl*977) + tl on 1, th on 2 (top = th*2^32 +
+// tl).  The common path is those seven carry-chained instructions.  Three rare
+// cases take the branch: th = 1 (top >= 2^32, its 977 * 2^32 still to add),
+// a carry out of limb 2 (limb 2 was 0xFFFFFFFF), and a wrap past 2^256, which
+// is folded once more as + K (the value is then below 2^65, so it cannot wrap
+// again).
+__device__ __forceinline__ void fold_top_ptx(uint32_t s[8], uint64_t top) {
+    const uint32_t tl = (uint32_t)top, th = (uint32_t)(top >> 32);
+    uint32_t c;
+    asm("mad.lo.cc.u32 %0, %4, 977, %0;\n\t"
+        "madc.hi.cc.u32 %1, %4, 977, %1;\n\t"
+        "addc.cc.u32 %2, %2, %5;\n\t"
+        "addc.u32 %3, 0, 0;"
+        : "+r"(s[0]), "+r"(s[1]), "+r"(s[2]), "=r"(c)
+        : "r"(tl), "r"(th));
+    asm("add.cc.u32 %0, %0, %3;\n\t"
+        "addc.cc.u32 %1, %1, 0;\n\t"
+        "addc.u32 %2, %2, 0;"
+        : "+r"(s[1]), "+r"(s[2]), "+r"(c)
+        : "r"(tl));
+    if (__builtin_expect((c | th) != 0, 0)) {
+        uint32_t w;
+        asm("mad.lo.cc.u32 %0, %8, 977, %0;\n\t"   // th * 977 * 2^32 on limb 1
+            "addc.cc.u32 %1, %1, 0;\n\t"
+            "addc.cc.u32 %2, %2, %9;\n\t"          // the carry out of limb 2
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.cc.u32 %4, %4, 0;\n\t"
+            "addc.cc.u32 %5, %5, 0;\n\t"
+            "addc.cc.u32 %6, %6, 0;\n\t"
+            "addc.u32 %7, 0, 0;"
+            : "+r"(s[1]), "+r"(s[2]), "+r"(s[3]), "+r"(s[4]), "+r"(s[5]), "+r"(s[6]), "+r"(s[7]), "=r"(w)
+            : "r"(th), "r"(c));
+        if (w) {   // wrapped past 2^256: + K (the value is now below 2^65: limbs 3..7 are zero)
+            asm("add.cc.u32 %0, %0, 977;\n\t"
+                "addc.cc.u32 %1, %1, 1;\n\t"
+                "addc.u32 %2, %2, 0;"
+                : "+r"(s[0]), "+r"(s[1]), "+r"(s[2]));
+        }
+    }
+}
+
 // r = a + b mod p (weakly reduced in and out).  The carry out of the 256-bit
-// add is folded back as +K (K = 2^32 + 977); that fold can itself carry only
-// when the result is below K, which takes a further +K (practically never
-// taken, kept exact behind a branch).
+// add is folded back as +K (K = 2^32 + 977) on limbs 0..1; carrying further
+// (limb 1 all ones) and wrapping past 2^256 again (only when the sum is below
+// K) take rare branches.
 __device__ __forceinline__ void fe_add_ptx(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
     uint32_t c;
     asm("add.cc.u32 %0, %9, %17;\n\t"
@@ -134,33 +177,35 @@ __device__ __forceinline__ void fe_add_ptx(uint32_t r[8], const uint32_t a[8], c
           "=&r"(c)
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
           "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
-    asm("mad.lo.cc.u32 %0, %9, 977, %0;\n\t"
-        "addc.cc.u32 %1, %1, %9;\n\t"
-        "addc.cc.u32 %2, %2, 0;\n\t"
-        "addc.cc.u32 %3, %3, 0;\n\t"
-        "addc.cc.u32 %4, %4, 0;\n\t"
-        "addc.cc.u32 %5, %5, 0;\n\t"
-        "addc.cc.u32 %6, %6, 0;\n\t"
-        "addc.cc.u32 %7, %7, 0;\n\t"
-        "addc.u32 %8, 0, 0;"
-        : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(c)
+    // + K on carry: 977 on limb 0, 1 on limb 1; a carry out of limb 1
+    // (limb 1 was 0xFFFFFFFF) continues on the rare path
+    uint32_t c2;
+    asm("mad.lo.cc.u32 %0, %3, 977, %0;\n\t"
+        "addc.cc.u32 %1, %1, %3;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "+r"(r[0]), "+r"(r[1]), "=r"(c2)
         : "r"(c));
-    if (__builtin_expect(c != 0, 0)) {
-        asm("add.cc.u32 %0, %0, 977;\n\t"
-            "addc.cc.u32 %1, %1, 1;\n\t"
+    if (__builtin_expect(c2 != 0, 0)) {
+        asm("add.cc.u32 %0, %0, 1;\n\t"
+            "addc.cc.u32 %1, %1, 0;\n\t"
             "addc.cc.u32 %2, %2, 0;\n\t"
             "addc.cc.u32 %3, %3, 0;\n\t"
             "addc.cc.u32 %4, %4, 0;\n\t"
             "addc.cc.u32 %5, %5, 0;\n\t"
-            "addc.cc.u32 %6, %6, 0;\n\t"
-            "addc.u32 %7, %7, 0;"
-            : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+            "addc.u32 %6, 0, 0;"
+            : "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(c2));
+        if (c2) {   // wrapped again: the sum is below K (limbs 2..7 zero, limb 1 <= 1): + K
+            asm("add.cc.u32 %0, %0, 977;\n\t"
+                "addc.u32 %1, %1, 1;"
+                : "+r"(r[0]), "+r"(r[1]));
+        }
     }
 }
 
 // r = a - b mod p (weakly reduced in and out).  A borrow out of the 256-bit
-// subtraction is folded as -K (adds p); a second borrow, possible only when
-// b > p and a is tiny, takes one more -K behind a branch.
+// subtraction is folded as -K (adds p) on limbs 0..1; borrowing further (limb
+// 1 zero) and a second borrow (possible only when b > p and a is tiny, one
+// more -K) take rare branches.
 __device__ __forceinline__ void fe_sub_ptx(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
     uint32_t br;
     asm("sub.cc.u32 %0, %9, %17;\n\t"
@@ -176,29 +221,30 @@ __device__ __forceinline__ void fe_sub_ptx(uint32_t r[8], const uint32_t a[8], c
           "=&r"(br)
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
           "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
-    // br is 0 or 0xFFFFFFFF; subtract K & br
+    // br is 0 or 0xFFFFFFFF: subtract K & br (977 on limb 0, 1 on limb 1); a
+    // borrow out of limb 1 (limb 1 was 0) continues on the rare path
     const uint32_t k0 = br & 977u, k1 = br & 1u;
-    asm("sub.cc.u32 %0, %0, %9;\n\t"
-        "subc.cc.u32 %1, %1, %10;\n\t"
-        "subc.cc.u32 %2, %2, 0;\n\t"
-        "subc.cc.u32 %3, %3, 0;\n\t"
-        "subc.cc.u32 %4, %4, 0;\n\t"
-        "subc.cc.u32 %5, %5, 0;\n\t"
-        "subc.cc.u32 %6, %6, 0;\n\t"
-        "subc.cc.u32 %7, %7, 0;\n\t"
-        "subc.u32 %8, 0, 0;"
-        : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(br)
+    uint32_t b2;
+    asm("sub.cc.u32 %0, %0, %3;\n\t"
+        "subc.cc.u32 %1, %1, %4;\n\t"
+        "subc.u32 %2, 0, 0;"
+        : "+r"(r[0]), "+r"(r[1]), "=r"(b2)
         : "r"(k0), "r"(k1));
-    if (__builtin_expect(br != 0, 0)) {
-        asm("sub.cc.u32 %0, %0, 977;\n\t"
-            "subc.cc.u32 %1, %1, 1;\n\t"
+    if (__builtin_expect(b2 != 0, 0)) {
+        asm("sub.cc.u32 %0, %0, 1;\n\t"
+            "subc.cc.u32 %1, %1, 0;\n\t"
             "subc.cc.u32 %2, %2, 0;\n\t"
             "subc.cc.u32 %3, %3, 0;\n\t"
             "subc.cc.u32 %4, %4, 0;\n\t"
             "subc.cc.u32 %5, %5, 0;\n\t"
-            "subc.cc.u32 %6, %6, 0;\n\t"
-            "subc.u32 %7, %7, 0;"
-            : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+            "subc.u32 %6, 0, 0;"
+            : "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(b2));
+        if (b2) {   // a second borrow (b > p and a tiny): the value is 2^256 - (K - x) with
+                    // x < K, limbs 2..7 all ones and limb 1 >= 2^32 - 3: - K stays in limbs 0..1
+            asm("sub.cc.u32 %0, %0, 977;\n\t"
+                "subc.u32 %1, %1, 1;"
+                : "+r"(r[0]), "+r"(r[1]));
+        }
     }
 }
 

@@ -142,6 +142,10 @@ cudaError_t launch_sign(int kind, const uint8_t* msgs, const uint8_t* sks, const
 cudaError_t launch_diag(uint32_t op, const uint8_t* in, uint32_t n, uint8_t* out,
                         const void* d_gtab, cudaStream_t s);
 
+// Field multiply / square / add / sub as the verify kernels compile them
+// (diag op 11): a | b (64 B) -> a*b | a^2 | a+b | a-b (128 B, normalized).
+cudaError_t launch_field_diag(const uint8_t* in, uint32_t n, uint8_t* out, int sms, cudaStream_t s);
+
 // Integer multiply-add issue-rate probe: every thread runs `iters` rounds of
 // 16 independent 32-bit IMADs.  Returns a checksum so the work is not elided.
 cudaError_t launch_imad_peak(uint32_t* d_sink, int blocks, int threads, int iters, cudaStream_t s);

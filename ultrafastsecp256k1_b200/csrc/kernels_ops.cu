@@ -124,6 +124,32 @@ k_tagged_hash(Mid mid, const uint8_t* __restrict__ msgs, const uint32_t* __restr
     }
 }
 
+// Field arithmetic exactly as the verify kernels compile it (this file is
+// built with their flags: PTX carry chains, out-of-line multiply): per item
+// a | b (any 256-bit values, i.e. weakly reduced) -> a*b, a^2, a+b, a-b, each
+// normalized, big-endian.
+__global__ void __launch_bounds__(128)
+k_field_diag(const uint8_t* __restrict__ in, uint32_t n, uint8_t* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Fe a, b, r;
+        be32_to_limbs(a.v, in + 64ull * i);
+        be32_to_limbs(b.v, in + 64ull * i + 32);
+        uint8_t* o = out + 128ull * i;
+        fe_mul(r, a, b);
+        fe_normalize(r);
+        limbs_to_be32(o, r.v);
+        fe_sqr(r, a);
+        fe_normalize(r);
+        limbs_to_be32(o + 32, r.v);
+        fe_add(r, a, b);
+        fe_normalize(r);
+        limbs_to_be32(o + 64, r.v);
+        fe_sub(r, a, b);
+        fe_normalize(r);
+        limbs_to_be32(o + 96, r.v);
+    }
+}
+
 inline int grid_ops(uint32_t n, int sms) {
     const int need = (int)((n + 127) / 128);
     return need < sms * 8 ? need : sms * 8;
@@ -147,6 +173,12 @@ cudaError_t launch_commitment_verify(const uint8_t* ix, const uint8_t* tw, const
                                      uint32_t n, const void* d_gtab, uint8_t* out, int sms, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_commitment_verify<<<grid_ops(n, sms), 128, 0, s>>>(ix, tw, tx, par, n, (const uint4*)d_gtab, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_field_diag(const uint8_t* in, uint32_t n, uint8_t* out, int sms, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_field_diag<<<grid_ops(n, sms), 128, 0, s>>>(in, n, out);
     return cudaGetLastError();
 }
 

@@ -79,6 +79,54 @@ __global__ void k_probe(int op, int iters, uint32_t* sink) {
             for (int i = 0; i < iters; ++i) { bip340_challenge(h, a.v, b.v, c.v); a.v[0] ^= h[0]; }
             break;
         }
+#if defined(__CUDA_ARCH__)
+        // Integer multiply-add forms, 8 independent chains per thread, 8 ops
+        // per round; every multiplier comes from the previous round's result
+        // so that no product is loop-invariant: the issue cost of each form.
+        case 10:  // mad.lo.u32
+            for (int i = 0; i < iters; ++i)
+                for (int k = 0; k < 8; ++k)
+                    asm("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a.v[k]) : "r"(b.v[k]), "r"(c.v[k]));
+            break;
+        case 11:  // mad.hi.u32
+            for (int i = 0; i < iters; ++i)
+                for (int k = 0; k < 8; ++k)
+                    asm("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a.v[k]) : "r"(b.v[k]), "r"(c.v[k]));
+            break;
+        case 12: {  // mad.wide.u32: w = lo(w) * b + w
+            uint64_t w[8];
+            for (int k = 0; k < 8; ++k) w[k] = ((uint64_t)c.v[k] << 32) | a.v[k];
+            for (int i = 0; i < iters; ++i)
+                for (int k = 0; k < 8; ++k)
+                    asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[k]) : "r"((uint32_t)w[k]), "r"(b.v[k]));
+            for (int k = 0; k < 8; ++k) a.v[k] = (uint32_t)w[k] ^ (uint32_t)(w[k] >> 32);
+            break;
+        }
+        case 13:  // carry-chained mad.lo.cc / madc.hi.cc pairs, multiplier = last round's top limb
+            for (int i = 0; i < iters; ++i) {
+                const uint32_t m = a.v[7];
+                asm("mad.lo.cc.u32 %0, %8, %9, %0;\n\t"
+                    "madc.hi.cc.u32 %1, %8, %9, %1;\n\t"
+                    "madc.lo.cc.u32 %2, %10, %9, %2;\n\t"
+                    "madc.hi.cc.u32 %3, %10, %9, %3;\n\t"
+                    "madc.lo.cc.u32 %4, %11, %9, %4;\n\t"
+                    "madc.hi.cc.u32 %5, %11, %9, %5;\n\t"
+                    "madc.lo.cc.u32 %6, %12, %9, %6;\n\t"
+                    "madc.hi.u32 %7, %12, %9, %7;"
+                    : "+r"(a.v[0]), "+r"(a.v[1]), "+r"(a.v[2]), "+r"(a.v[3]), "+r"(a.v[4]), "+r"(a.v[5]),
+                      "+r"(a.v[6]), "+r"(a.v[7])
+                    : "r"(b.v[0]), "r"(m), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]));
+            }
+            break;
+        case 14: {  // operand-scanning step: w = lo(w) * b + hi(w) + lo(w)
+            uint64_t w[8];
+            for (int k = 0; k < 8; ++k) w[k] = ((uint64_t)c.v[k] << 32) | a.v[k];
+            for (int i = 0; i < iters; ++i)
+                for (int k = 0; k < 8; ++k) w[k] = (uint64_t)(uint32_t)w[k] * b.v[k] + (w[k] >> 32) + (uint32_t)w[k];
+            for (int k = 0; k < 8; ++k) a.v[k] = (uint32_t)w[k] ^ (uint32_t)(w[k] >> 32);
+            break;
+        }
+#endif
         default:
             break;
     }

@@ -249,7 +249,7 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int 
  *  8  k (32) -> (k*G).x | (k*G).y (64), zeros for infinity
  *  9  a|x|b (96) -> finite (1) | x (32) | y (32) of a*G + b*P, P = lift_x(x)
  * 10  r|p|m (96) -> BIP-340 challenge digest (32)
- * 11  a|b (64) -> a*b | a^2 | a+b | a-b mod p (128), through the field code
+ * 11  a|b (64) -> a*b | a^2 | a+b | a-b | 4a | 8a mod p (192), through the field code
  *     of the verify kernels (PTX carry chains), inputs any 256-bit values
  * All values big-endian. */
 #define UFSECP_EXT_DIAG_FE_MUL    1

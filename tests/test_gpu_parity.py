@@ -86,6 +86,13 @@ def _sub_paths(a, b):
     return int((r & (2**64 - 1)) < K), int(r < K)
 
 
+def _shift_paths(a, k):
+    """(carry past limb 1 after folding the shifted-out bits, wrap past 2^256)
+    of the device a * 2^k."""
+    r, top = (a << k) % 2**256, a >> (256 - k)
+    return int(((r & (2**64 - 1)) + top * K) >> 64), int(r + top * K >= 2**256)
+
+
 def _hard_field_pairs(rng):
     """Operand pairs that drive the device field code into its rare carry paths."""
     pairs = []
@@ -114,14 +121,21 @@ def _hard_field_pairs(rng):
         a = int(rng.integers(0, 2**20))
         pairs.append((a, (a - r) % 2**256))
     pairs += [(d, 2**256 - 1 - e) for d in range(0, 5) for e in range(0, 2000, 401)]
+    # shifts: a * 2^k with limb 1 of the shifted value all ones, and near 2^256
+    for k in (2, 3):
+        for _ in range(16):
+            r = (int.from_bytes(rng.bytes(32), "big") | (M32 << 32)) & ~((1 << k) - 1)
+            top = int(rng.integers(1, 1 << k))
+            pairs.append((((top << 256) | r) >> k, 1))
+    pairs += [(2**256 - 1 - d, 3) for d in range(0, 64, 5)]
     return pairs
 
 
 def test_diag_ptx_field_rare_paths(gpu_ctx):
     """The field code the verify kernels run (PTX carry chains) on random
     weakly reduced operands and on pairs built to reach every rare carry path
-    of the reduction, the add and the sub; the models above confirm that each
-    path is reached."""
+    of the reduction, the add, the sub and the shifts by 2 and 3; the models
+    above confirm that each path is reached."""
     rng = np.random.default_rng(11)
     pairs = _hard_field_pairs(rng)
     pairs += [(int.from_bytes(rng.bytes(32), "big"), int.from_bytes(rng.bytes(32), "big")) for _ in range(2000)]
@@ -131,10 +145,12 @@ def test_diag_ptx_field_rare_paths(gpu_ctx):
     assert all(any(f[k] for f in fold) for k in range(3)), "a reduction path is not reached"
     assert all(any(_add_paths(a, b)[k] for a, b in pairs) for k in range(2)), "an add path is not reached"
     assert all(any(_sub_paths(a, b)[k] for a, b in pairs) for k in range(2)), "a sub path is not reached"
+    for sh in (2, 3):
+        assert all(any(_shift_paths(a, sh)[k] for a, _ in pairs) for k in range(2)), "a shift path is not reached"
     data = np.frombuffer(b"".join(be(a) + be(b) for a, b in pairs), np.uint8)
     out = gpu_ctx.diag(11, data)
-    got = [[int.from_bytes(r[32 * k:32 * k + 32].tobytes(), "big") for k in range(4)] for r in out]
-    want = [[a * b % P, a * a % P, (a + b) % P, (a - b) % P] for a, b in pairs]
+    got = [[int.from_bytes(r[32 * k:32 * k + 32].tobytes(), "big") for k in range(6)] for r in out]
+    want = [[a * b % P, a * a % P, (a + b) % P, (a - b) % P, 4 * a % P, 8 * a % P] for a, b in pairs]
     bad = [(i, pairs[i]) for i in range(len(pairs)) if got[i] != want[i]]
     assert not bad, bad[:4]
 

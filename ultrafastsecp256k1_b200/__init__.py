@@ -385,7 +385,7 @@ class GpuContext:
         return ms.value
 
     _DIAG_IO = {1: (64, 32), 2: (32, 32), 3: (32, 32), 4: (32, 33), 5: (64, 32), 6: (32, 32), 7: (32, 34),
-                8: (32, 64), 9: (96, 65), 10: (96, 32), 11: (64, 128)}
+                8: (32, 64), 9: (96, 65), 10: (96, 32), 11: (64, 192)}
 
     def diag(self, op: int, data) -> np.ndarray:
         isz, osz = self._DIAG_IO[op]

@@ -596,7 +596,7 @@ ufsecp_error_t ufsecp_gpu_ext_diag(ufsecp_gpu_ctx* ctx, uint32_t op, const uint8
     if (n == 0) return UFSECP_OK;
     if (!in || !out) return UFSECP_ERR_NULL_ARG;
     static const int in_sz[12] = {0, 64, 32, 32, 32, 64, 32, 32, 32, 96, 96, 64};
-    static const int out_sz[12] = {0, 32, 32, 32, 33, 32, 32, 34, 64, 65, 32, 128};
+    static const int out_sz[12] = {0, 32, 32, 32, 33, 32, 32, 34, 64, 65, 32, 192};
     if (op < 1 || op > 11 || n > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
     return ctx->backend->diag(op, in, n, out, (size_t)in_sz[op], (size_t)out_sz[op]);
 }

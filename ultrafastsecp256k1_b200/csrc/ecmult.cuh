@@ -153,10 +153,7 @@ UF_HDI void dual_mul_c(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc
     jac_set_inf(R);
     UF_NOUNROLL
     for (int i = kNWP - 1; i >= 0; --i) {
-        if (i != kNWP - 1) {
-            UF_NOUNROLL
-            for (int j = 0; j < kWP; ++j) jac_dbl(R);
-        }
+        if (i != kNWP - 1) jac_dbl_n(R, kWP);
         add_ptab(R, tab, dp1[i], sb.neg1, false, beta);
         add_ptab(R, tab, dp2[i], sb.neg2, true, beta);
         if (i % kGEvery == 0) {

@@ -216,7 +216,7 @@ UF_HD void sqr256(uint32_t t[16], const uint32_t a[8]) {
 // operands in registers rather than through the stack.
 // UF_PTX_MUL selects the PTX carry-chain product / square of fe_ptx.cuh and
 // fe_ptx_sqr.cuh on the device (and the PTX add / sub above).
-UF_FIELD_FN Fe fe_mul_v(Fe a, Fe b) {
+UF_HD Fe fe_mul_c(Fe a, Fe b) {
     uint32_t t[16];
     Fe r;
 #if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
@@ -228,7 +228,7 @@ UF_FIELD_FN Fe fe_mul_v(Fe a, Fe b) {
     return r;
 }
 
-UF_FIELD_FN Fe fe_sqr_v(Fe a) {
+UF_HD Fe fe_sqr_c(Fe a) {
     uint32_t t[16];
     Fe r;
 #if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
@@ -238,6 +238,17 @@ UF_FIELD_FN Fe fe_sqr_v(Fe a) {
 #endif
     fe_reduce512(r, t);
     return r;
+}
+
+UF_FIELD_FN Fe fe_mul_v(Fe a, Fe b) { return fe_mul_c(a, b); }
+UF_FIELD_FN Fe fe_sqr_v(Fe a) { return fe_sqr_c(a); }
+
+// n >= 1 squarings in one out-of-line call (the square-root chain's runs of
+// up to 88 squarings pay one call, not one per squaring).
+UF_FIELD_FN Fe fe_sqr_n_v(Fe a, int n) {
+    UF_NOUNROLL
+    for (int i = 0; i < n; ++i) a = fe_sqr_c(a);
+    return a;
 }
 
 UF_HD void fe_mul(Fe& r, const Fe& a, const Fe& b) { r = fe_mul_v(a, b); }
@@ -266,6 +277,19 @@ UF_HD void fe_mul_small(Fe& r, const Fe& a, uint32_t m) {
     fe_add_k(s, hi32(c));
     UF_UNROLL
     for (int i = 0; i < 8; ++i) r.v[i] = s[i];
+}
+
+// r = a * 2^k mod p for k = 1..8 (a shift and one fold on the device).
+template <int k>
+UF_HD void fe_mul_pow2(Fe& r, const Fe& a) {
+#if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
+    uint32_t t[8];
+    fe_shl_ptx<k>(t, a.v);
+    UF_UNROLL
+    for (int i = 0; i < 8; ++i) r.v[i] = t[i];
+#else
+    fe_mul_small(r, a, 1u << k);
+#endif
 }
 
 // Canonical representative in [0, p).
@@ -302,11 +326,7 @@ UF_HD bool limbs_lt_p(const uint32_t v[8]) {
     return fe_add_k(t, 1) == 0;
 }
 
-UF_HD void fe_sqr_n(Fe& r, const Fe& a, int n) {
-    fe_sqr(r, a);
-    UF_NOUNROLL
-    for (int i = 1; i < n; ++i) fe_sqr(r, r);
-}
+UF_HD void fe_sqr_n(Fe& r, const Fe& a, int n) { r = fe_sqr_n_v(a, n); }
 
 // a^((p+1)/4): the square root when a is a square.  (p+1)/4 is, from the top,
 // 223 one-bits, a zero, 22 ones, four zeros, two ones, two zeros; the chain

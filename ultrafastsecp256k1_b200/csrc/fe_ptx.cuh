@@ -158,6 +158,47 @@ __device__ __forceinline__ void fold_top_ptx(uint32_t s[8], uint64_t top) {
     }
 }
 
+// r += c * K (K = 2^32 + 977) for the carry word c < 2^22 of a value that
+// overflowed 2^256 by c: c * 977 on limb 0 and c on limb 1.  A carry out of
+// limb 1 (limb 1 all ones) continues on the rare path; wrapping past 2^256
+// again leaves a value below c * K < 2^55 (limbs 2..7 zero), so the last
+// + K stays in limbs 0..1.
+__device__ __forceinline__ void fold_k_ptx(uint32_t r[8], uint32_t c) {
+    uint32_t c2;
+    asm("mad.lo.cc.u32 %0, %3, 977, %0;\n\t"
+        "addc.cc.u32 %1, %1, %3;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "+r"(r[0]), "+r"(r[1]), "=r"(c2)
+        : "r"(c));
+    if (__builtin_expect(c2 != 0, 0)) {
+        asm("add.cc.u32 %0, %0, 1;\n\t"
+            "addc.cc.u32 %1, %1, 0;\n\t"
+            "addc.cc.u32 %2, %2, 0;\n\t"
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.cc.u32 %4, %4, 0;\n\t"
+            "addc.cc.u32 %5, %5, 0;\n\t"
+            "addc.u32 %6, 0, 0;"
+            : "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(c2));
+        if (c2) {
+            asm("add.cc.u32 %0, %0, 977;\n\t"
+                "addc.u32 %1, %1, 1;"
+                : "+r"(r[0]), "+r"(r[1]));
+        }
+    }
+}
+
+// r = a * 2^k mod p (weakly reduced in and out), k = 1..8: a funnel shift of
+// the limbs and one fold of the k bits shifted out.
+template <int k>
+__device__ __forceinline__ void fe_shl_ptx(uint32_t r[8], const uint32_t a[8]) {
+    static_assert(k >= 1 && k <= 8, "shift of 1..8 bits");
+    const uint32_t top = a[7] >> (32 - k);
+#pragma unroll
+    for (int i = 7; i > 0; --i) r[i] = __funnelshift_l(a[i - 1], a[i], k);
+    r[0] = a[0] << k;
+    fold_k_ptx(r, top);
+}
+
 // r = a + b mod p (weakly reduced in and out).  The carry out of the 256-bit
 // add is folded back as +K (K = 2^32 + 977) on limbs 0..1; carrying further
 // (limb 1 all ones) and wrapping past 2^256 again (only when the sum is below
@@ -177,29 +218,7 @@ __device__ __forceinline__ void fe_add_ptx(uint32_t r[8], const uint32_t a[8], c
           "=&r"(c)
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
           "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
-    // + K on carry: 977 on limb 0, 1 on limb 1; a carry out of limb 1
-    // (limb 1 was 0xFFFFFFFF) continues on the rare path
-    uint32_t c2;
-    asm("mad.lo.cc.u32 %0, %3, 977, %0;\n\t"
-        "addc.cc.u32 %1, %1, %3;\n\t"
-        "addc.u32 %2, 0, 0;"
-        : "+r"(r[0]), "+r"(r[1]), "=r"(c2)
-        : "r"(c));
-    if (__builtin_expect(c2 != 0, 0)) {
-        asm("add.cc.u32 %0, %0, 1;\n\t"
-            "addc.cc.u32 %1, %1, 0;\n\t"
-            "addc.cc.u32 %2, %2, 0;\n\t"
-            "addc.cc.u32 %3, %3, 0;\n\t"
-            "addc.cc.u32 %4, %4, 0;\n\t"
-            "addc.cc.u32 %5, %5, 0;\n\t"
-            "addc.u32 %6, 0, 0;"
-            : "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "=r"(c2));
-        if (c2) {   // wrapped again: the sum is below K (limbs 2..7 zero, limb 1 <= 1): + K
-            asm("add.cc.u32 %0, %0, 977;\n\t"
-                "addc.u32 %1, %1, 1;"
-                : "+r"(r[0]), "+r"(r[1]));
-        }
-    }
+    fold_k_ptx(r, c);
 }
 
 // r = a - b mod p (weakly reduced in and out).  A borrow out of the 256-bit

@@ -143,7 +143,7 @@ cudaError_t launch_diag(uint32_t op, const uint8_t* in, uint32_t n, uint8_t* out
                         const void* d_gtab, cudaStream_t s);
 
 // Field multiply / square / add / sub as the verify kernels compile them
-// (diag op 11): a | b (64 B) -> a*b | a^2 | a+b | a-b (128 B, normalized).
+// (diag op 11): a | b (64 B) -> a*b | a^2 | a+b | a-b | 4a | 8a (192 B, normalized).
 cudaError_t launch_field_diag(const uint8_t* in, uint32_t n, uint8_t* out, int sms, cudaStream_t s);
 
 // Integer multiply-add issue-rate probe: every thread runs `iters` rounds of

@@ -126,15 +126,15 @@ k_tagged_hash(Mid mid, const uint8_t* __restrict__ msgs, const uint32_t* __restr
 
 // Field arithmetic exactly as the verify kernels compile it (this file is
 // built with their flags: PTX carry chains, out-of-line multiply): per item
-// a | b (any 256-bit values, i.e. weakly reduced) -> a*b, a^2, a+b, a-b, each
-// normalized, big-endian.
+// a | b (any 256-bit values, i.e. weakly reduced) -> a*b, a^2, a+b, a-b, 4a,
+// 8a, each normalized, big-endian.
 __global__ void __launch_bounds__(128)
 k_field_diag(const uint8_t* __restrict__ in, uint32_t n, uint8_t* __restrict__ out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         Fe a, b, r;
         be32_to_limbs(a.v, in + 64ull * i);
         be32_to_limbs(b.v, in + 64ull * i + 32);
-        uint8_t* o = out + 128ull * i;
+        uint8_t* o = out + 192ull * i;
         fe_mul(r, a, b);
         fe_normalize(r);
         limbs_to_be32(o, r.v);
@@ -147,6 +147,12 @@ k_field_diag(const uint8_t* __restrict__ in, uint32_t n, uint8_t* __restrict__ o
         fe_sub(r, a, b);
         fe_normalize(r);
         limbs_to_be32(o + 96, r.v);
+        fe_mul_pow2<2>(r, a);
+        fe_normalize(r);
+        limbs_to_be32(o + 128, r.v);
+        fe_mul_pow2<3>(r, a);
+        fe_normalize(r);
+        limbs_to_be32(o + 160, r.v);
     }
 }
 

@@ -27,7 +27,7 @@ UF_HD void jac_from_aff(Jac& a, const Fe& x, const Fe& y) {
 }
 
 // dbl-2009-l.  Y = 0 cannot occur on secp256k1 (no 2-torsion).
-UF_POINT_FN Jac jac_dbl_v(Jac a) {
+UF_HD Jac jac_dbl_c(Jac a) {
     if (a.inf) return a;
     Fe A, B, C, D, E, t;
     fe_mul(t, a.Y, a.Z);
@@ -47,14 +47,22 @@ UF_POINT_FN Jac jac_dbl_v(Jac a) {
     fe_sub(a.X, t, D);          // X3 = F - 2D
     fe_sub(t, D, a.X);
     fe_mul(a.Y, E, t);
-    fe_dbl(C, C);
-    fe_dbl(C, C);
-    fe_dbl(C, C);
+    fe_mul_pow2<3>(C, C);
     fe_sub(a.Y, a.Y, C);        // Y3 = E (D - X3) - 8C
     return a;
 }
 
+UF_POINT_FN Jac jac_dbl_v(Jac a) { return jac_dbl_c(a); }
+
+// n >= 1 doublings in one out-of-line call (a window's doublings).
+UF_POINT_FN Jac jac_dbl_n_v(Jac a, int n) {
+    UF_NOUNROLL
+    for (int i = 0; i < n; ++i) a = jac_dbl_c(a);
+    return a;
+}
+
 UF_HD void jac_dbl(Jac& a) { a = jac_dbl_v(a); }
+UF_HD void jac_dbl_n(Jac& a, int n) { a = jac_dbl_n_v(a, n); }
 
 // a += (x2, y2) affine (madd-2007-bl), exact in all cases.
 UF_POINT_FN Jac jac_add_aff_v(Jac a, Fe x2, Fe y2) {
@@ -73,8 +81,7 @@ UF_POINT_FN Jac jac_add_aff_v(Jac a, Fe x2, Fe y2) {
     }
     Fe HH, I, J, V;
     fe_sqr(HH, H);
-    fe_dbl(I, HH);
-    fe_dbl(I, I);               // I = 4 HH
+    fe_mul_pow2<2>(I, HH);      // I = 4 HH
     fe_mul(J, H, I);            // J = H I
     fe_dbl(r, r);               // r = 2 (S2 - Y1)
     fe_mul(V, a.X, I);          // V = X1 I

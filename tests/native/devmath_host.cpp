@@ -112,7 +112,7 @@ void hm_booth(const uint8_t* k16, int w, int32_t* out) {
     uint32_t v[8];
     be32_to_limbs(v, buf);
     if (w == 4) { int8_t d[kNWP]; booth_recode<kWP, kNWP>(d, v); for (int i = 0; i < kNWP; ++i) out[i] = d[i]; }
-    else { int16_t d[kNWG]; booth_recode<kWG, kNWG>(d, v); for (int i = 0; i < kNWG; ++i) out[i] = d[i]; }
+    else { GDigit d[kNWG]; booth_recode<kWG, kNWG>(d, v); for (int i = 0; i < kNWG; ++i) out[i] = d[i]; }
 }
 // a*G + b*P for P given by x (BE) with even y; affine result or 0 for infinity
 int hm_dual_mul(const uint8_t* a, const uint8_t* px32, const uint8_t* b, uint8_t* x_out, uint8_t* y_out) {

@@ -9,12 +9,12 @@
 #include <stdint.h>
 
 // Window width (bits) of the generator streams, library-wide: the per-context
-// G / lambda G tables hold 2^(UF_GWIN-1) multiples each.  12-bit windows (one
-// per three 4-bit P windows, 2 x 2048 entries, 256 KB) measured 6 % faster on
-// B200 than 8-bit ones (2 x 128 entries, 16 KB): 22 instead of 34 table
-// additions per verify, the tables served from L2.
+// G / lambda G tables hold 2^(UF_GWIN-1) multiples each.  16-bit windows (one
+// per four 4-bit P windows, 2 x 32768 entries, 4 MB, served from L2): 18
+// table additions per verify, against 22 for 12-bit windows (2 x 2048
+// entries, 256 KB) and 34 for 8-bit ones (16 KB).
 #ifndef UF_GWIN
-#define UF_GWIN 12
+#define UF_GWIN 16
 #endif
 
 #if defined(__CUDACC__)

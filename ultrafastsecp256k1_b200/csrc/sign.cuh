@@ -92,20 +92,18 @@ UF_HD void mid_challenge(uint32_t m[8]) {
     m[4] = 0x97c87550u; m[5] = 0x003cc765u; m[6] = 0x90f61164u; m[7] = 0x33e9b66au;
 }
 
-// k*G through the generator tables: GLV split, two 8-bit Booth streams.
+// k*G through the generator tables: GLV split, two UF_GWIN-bit Booth streams.
 template <class GT>
 UF_HDI void gen_mul(Jac& R, const Sc& k, const GT& gt) {
     GlvSplit s;
     glv_split(s, k);
-    int16_t d1[kNWG], d2[kNWG];
+    GDigit d1[kNWG], d2[kNWG];
     booth_recode<kWG, kNWG>(d1, s.k1);
     booth_recode<kWG, kNWG>(d2, s.k2);
     jac_set_inf(R);
     UF_NOUNROLL
     for (int i = kNWG - 1; i >= 0; --i) {
-        if (i != kNWG - 1) {
-            for (int j = 0; j < kWG; ++j) jac_dbl(R);
-        }
+        if (i != kNWG - 1) jac_dbl_n(R, kWG);
         add_gtab(R, gt, d1[i], s.neg1, 0);
         add_gtab(R, gt, d2[i], s.neg2, 1);
     }

@@ -236,7 +236,8 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* 
  * 9 BIP-340 challenge hash; integer multiply-add forms, 8 per round with
  * data-dependent multipliers: 10 mad.lo.u32, 11 mad.hi.u32, 12 mad.wide.u32,
  * 13 mad.lo.cc / madc.hi.cc carry chain, 14 operand-scanning step
- * (32x32 + 32 + 32 -> 64). */
+ * (32x32 + 32 + 32 -> 64); 15 two 256x256 PTX products (no reduction),
+ * 16 two inlined field multiplies (no call). */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int blocks, int threads, int iters,
                                                float* ms_out);
 

@@ -587,7 +587,7 @@ ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) 
 
 ufsecp_error_t ufsecp_gpu_ext_probe(ufsecp_gpu_ctx* ctx, int op, int blocks, int threads, int iters, float* ms_out) {
     if (!ctx || !ms_out) return UFSECP_ERR_NULL_ARG;
-    if (op < 1 || op > 14 || blocks < 1 || threads < 1 || threads > 1024 || iters < 1) return UFSECP_ERR_BAD_INPUT;
+    if (op < 1 || op > 16 || blocks < 1 || threads < 1 || threads > 1024 || iters < 1) return UFSECP_ERR_BAD_INPUT;
     return ctx->backend->probe(op, blocks, threads, iters, ms_out);
 }
 

@@ -220,7 +220,7 @@ UF_HD Fe fe_mul_c(Fe a, Fe b) {
     uint32_t t[16];
     Fe r;
 #if defined(__CUDA_ARCH__) && defined(UF_PTX_MUL)
-    mul256_ptx(t, a.v, b.v);
+    mul256_sel_ptx(t, a.v, b.v);
 #else
     mul256(t, a.v, b.v);
 #endif

@@ -71,6 +71,141 @@ __device__ __forceinline__ void mul256_ptx(uint32_t t[16], const uint32_t a[8], 
 #undef UF_ROW_EVEN
 #undef UF_ROW_ODD
 
+// 128 x 128 -> 256-bit product (4 x 4 limbs), the same even / odd row chains
+// as mul256_ptx: after rows 0..i the value is below 2^(32(i+5)), so limb i+4
+// is zero before row i's even chain deposits its carry there.
+#define UF_ROW4_EVEN(T0, T1, T2, T3, T4, BI)                                                     \
+    asm("mad.lo.cc.u32 %0, %5, %7, %0;\n\t"                                                      \
+        "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"                                                     \
+        "madc.lo.cc.u32 %2, %6, %7, %2;\n\t"                                                     \
+        "madc.hi.cc.u32 %3, %6, %7, %3;\n\t"                                                     \
+        "addc.u32 %4, %4, 0;"                                                                    \
+        : "+r"(T0), "+r"(T1), "+r"(T2), "+r"(T3), "+r"(T4)                                       \
+        : "r"(a[0]), "r"(a[2]), "r"(BI))
+#define UF_ROW4_ODD(T1, T2, T3, T4, BI)                                                          \
+    asm("mad.lo.cc.u32 %0, %4, %6, %0;\n\t"                                                      \
+        "madc.hi.cc.u32 %1, %4, %6, %1;\n\t"                                                     \
+        "madc.lo.cc.u32 %2, %5, %6, %2;\n\t"                                                     \
+        "madc.hi.u32 %3, %5, %6, %3;"                                                            \
+        : "+r"(T1), "+r"(T2), "+r"(T3), "+r"(T4)                                                 \
+        : "r"(a[1]), "r"(a[3]), "r"(BI))
+
+__device__ __forceinline__ void mul128_ptx(uint32_t t[8], const uint32_t a[4], const uint32_t b[4]) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0;
+    UF_ROW4_EVEN(t0, t1, t2, t3, t4, b[0]);
+    UF_ROW4_ODD(t1, t2, t3, t4, b[0]);
+    UF_ROW4_EVEN(t1, t2, t3, t4, t5, b[1]);
+    UF_ROW4_ODD(t2, t3, t4, t5, b[1]);
+    UF_ROW4_EVEN(t2, t3, t4, t5, t6, b[2]);
+    UF_ROW4_ODD(t3, t4, t5, t6, b[2]);
+    UF_ROW4_EVEN(t3, t4, t5, t6, t7, b[3]);
+    UF_ROW4_ODD(t4, t5, t6, t7, b[3]);
+    t[0] = t0; t[1] = t1; t[2] = t2; t[3] = t3; t[4] = t4; t[5] = t5; t[6] = t6; t[7] = t7;
+}
+
+#undef UF_ROW4_EVEN
+#undef UF_ROW4_ODD
+
+// 256 x 256 -> 512 by one level of Karatsuba on 128-bit halves:
+// a = a0 + a1 2^128, b = b0 + b1 2^128, z0 = a0 b0, z2 = a1 b1,
+// m = (a0 + a1)(b0 + b1) with the two sums' carry bits ca, cb handled as
+// m = sa sb + ca sb 2^128 + cb sa 2^128 + ca cb 2^256 (sa, sb their low 128
+// bits), z1 = m - z0 - z2 = a0 b1 + a1 b0 < 2^257, t = z0 + z1 2^128 + z2 2^256.
+// Three 4 x 4 products (96 multiply-adds) instead of 128, for about 60 adds,
+// which run on the integer ALU pipe rather than the multiply-add one.
+__device__ __forceinline__ void mul256_kara_ptx(uint32_t t[16], const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t z0[8], z2[8], p[8], sa[4], sb[4], ca, cb;
+    mul128_ptx(z0, a, b);
+    mul128_ptx(z2, a + 4, b + 4);
+    asm("add.cc.u32 %0, %5, %9;\n\t"
+        "addc.cc.u32 %1, %6, %10;\n\t"
+        "addc.cc.u32 %2, %7, %11;\n\t"
+        "addc.cc.u32 %3, %8, %12;\n\t"
+        "addc.u32 %4, 0, 0;"
+        : "=r"(sa[0]), "=r"(sa[1]), "=r"(sa[2]), "=r"(sa[3]), "=r"(ca)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]));
+    asm("add.cc.u32 %0, %5, %9;\n\t"
+        "addc.cc.u32 %1, %6, %10;\n\t"
+        "addc.cc.u32 %2, %7, %11;\n\t"
+        "addc.cc.u32 %3, %8, %12;\n\t"
+        "addc.u32 %4, 0, 0;"
+        : "=r"(sb[0]), "=r"(sb[1]), "=r"(sb[2]), "=r"(sb[3]), "=r"(cb)
+        : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+    mul128_ptx(p, sa, sb);
+    // m[0..8] = p + (ca ? sb : 0) 2^128 + (cb ? sa : 0) 2^128 + ca cb 2^256
+    const uint32_t ma = 0u - ca, mb = 0u - cb;
+    uint32_t m8;
+    asm("add.cc.u32 %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.cc.u32 %2, %2, %7;\n\t"
+        "addc.cc.u32 %3, %3, %8;\n\t"
+        "addc.u32 %4, 0, 0;"
+        : "+r"(p[4]), "+r"(p[5]), "+r"(p[6]), "+r"(p[7]), "=r"(m8)
+        : "r"(sb[0] & ma), "r"(sb[1] & ma), "r"(sb[2] & ma), "r"(sb[3] & ma));
+    asm("add.cc.u32 %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.cc.u32 %2, %2, %7;\n\t"
+        "addc.cc.u32 %3, %3, %8;\n\t"
+        "addc.u32 %4, %4, %9;"
+        : "+r"(p[4]), "+r"(p[5]), "+r"(p[6]), "+r"(p[7]), "+r"(m8)
+        : "r"(sa[0] & mb), "r"(sa[1] & mb), "r"(sa[2] & mb), "r"(sa[3] & mb), "r"(ca & cb));
+    // z1 = m - z0 - z2 (nonnegative, below 2^257)
+    asm("sub.cc.u32 %0, %0, %9;\n\t"
+        "subc.cc.u32 %1, %1, %10;\n\t"
+        "subc.cc.u32 %2, %2, %11;\n\t"
+        "subc.cc.u32 %3, %3, %12;\n\t"
+        "subc.cc.u32 %4, %4, %13;\n\t"
+        "subc.cc.u32 %5, %5, %14;\n\t"
+        "subc.cc.u32 %6, %6, %15;\n\t"
+        "subc.cc.u32 %7, %7, %16;\n\t"
+        "subc.u32 %8, %8, 0;"
+        : "+r"(p[0]), "+r"(p[1]), "+r"(p[2]), "+r"(p[3]), "+r"(p[4]), "+r"(p[5]), "+r"(p[6]), "+r"(p[7]),
+          "+r"(m8)
+        : "r"(z0[0]), "r"(z0[1]), "r"(z0[2]), "r"(z0[3]), "r"(z0[4]), "r"(z0[5]), "r"(z0[6]), "r"(z0[7]));
+    asm("sub.cc.u32 %0, %0, %9;\n\t"
+        "subc.cc.u32 %1, %1, %10;\n\t"
+        "subc.cc.u32 %2, %2, %11;\n\t"
+        "subc.cc.u32 %3, %3, %12;\n\t"
+        "subc.cc.u32 %4, %4, %13;\n\t"
+        "subc.cc.u32 %5, %5, %14;\n\t"
+        "subc.cc.u32 %6, %6, %15;\n\t"
+        "subc.cc.u32 %7, %7, %16;\n\t"
+        "subc.u32 %8, %8, 0;"
+        : "+r"(p[0]), "+r"(p[1]), "+r"(p[2]), "+r"(p[3]), "+r"(p[4]), "+r"(p[5]), "+r"(p[6]), "+r"(p[7]),
+          "+r"(m8)
+        : "r"(z2[0]), "r"(z2[1]), "r"(z2[2]), "r"(z2[3]), "r"(z2[4]), "r"(z2[5]), "r"(z2[6]), "r"(z2[7]));
+    // t = z0 | z2, then + z1 at limb 4
+    t[0] = z0[0]; t[1] = z0[1]; t[2] = z0[2]; t[3] = z0[3];
+    asm("add.cc.u32 %0, %12, %20;\n\t"
+        "addc.cc.u32 %1, %13, %21;\n\t"
+        "addc.cc.u32 %2, %14, %22;\n\t"
+        "addc.cc.u32 %3, %15, %23;\n\t"
+        "addc.cc.u32 %4, %16, %24;\n\t"
+        "addc.cc.u32 %5, %17, %25;\n\t"
+        "addc.cc.u32 %6, %18, %26;\n\t"
+        "addc.cc.u32 %7, %19, %27;\n\t"
+        "addc.cc.u32 %8, %29, %28;\n\t"
+        "addc.cc.u32 %9, %30, 0;\n\t"
+        "addc.cc.u32 %10, %31, 0;\n\t"
+        "addc.u32 %11, %32, 0;"
+        : "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7]), "=r"(t[8]), "=r"(t[9]), "=r"(t[10]), "=r"(t[11]),
+          "=r"(t[12]), "=r"(t[13]), "=r"(t[14]), "=r"(t[15])
+        : "r"(z0[4]), "r"(z0[5]), "r"(z0[6]), "r"(z0[7]), "r"(z2[0]), "r"(z2[1]), "r"(z2[2]), "r"(z2[3]),
+          "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]),
+          "r"(m8), "r"(z2[4]), "r"(z2[5]), "r"(z2[6]), "r"(z2[7]));
+}
+
+// The product the field multiply uses: Karatsuba (measured on B200: 157
+// instead of 178 IMAD issue slots per product, field multiply 253 -> 230),
+// or the plain rows with UF_MUL_ROWS.
+__device__ __forceinline__ void mul256_sel_ptx(uint32_t t[16], const uint32_t a[8], const uint32_t b[8]) {
+#if defined(UF_MUL_ROWS)
+    mul256_ptx(t, a, b);
+#else
+    mul256_kara_ptx(t, a, b);
+#endif
+}
+
 // First fold of the reduction mod p for the 512-bit t = H*2^256 + L:
 // s[0..7] + top*2^256 = L + 977*H + (H << 32), with top < 2^32 + 978.
 // Order matters for the carry bounds: L + 977*H < 2^266 fits limbs 0..8, then

@@ -126,6 +126,17 @@ __global__ void k_probe(int op, int iters, uint32_t* sink) {
             for (int k = 0; k < 8; ++k) a.v[k] = (uint32_t)w[k] ^ (uint32_t)(w[k] >> 32);
             break;
         }
+        case 15:  // two independent 256x256 PTX products, low halves fed back (no reduction, no call)
+            for (int i = 0; i < iters; ++i) {
+                uint32_t t[16], u[16];
+                mul256_sel_ptx(t, a.v, b.v);
+                mul256_sel_ptx(u, c.v, d.v);
+                for (int k = 0; k < 8; ++k) { a.v[k] = t[k] ^ t[k + 8]; c.v[k] = u[k] ^ u[k + 8]; }
+            }
+            break;
+        case 16:  // two independent inlined field multiplies (product + reduction, no call)
+            for (int i = 0; i < iters; ++i) { a = fe_mul_c(a, b); c = fe_mul_c(c, d); }
+            break;
 #endif
         default:
             break;

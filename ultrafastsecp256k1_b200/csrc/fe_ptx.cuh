@@ -106,17 +106,8 @@ __device__ __forceinline__ void mul128_ptx(uint32_t t[8], const uint32_t a[4], c
 #undef UF_ROW4_EVEN
 #undef UF_ROW4_ODD
 
-// 256 x 256 -> 512 by one level of Karatsuba on 128-bit halves:
-// a = a0 + a1 2^128, b = b0 + b1 2^128, z0 = a0 b0, z2 = a1 b1,
-// m = (a0 + a1)(b0 + b1) with the two sums' carry bits ca, cb handled as
-// m = sa sb + ca sb 2^128 + cb sa 2^128 + ca cb 2^256 (sa, sb their low 128
-// bits), z1 = m - z0 - z2 = a0 b1 + a1 b0 < 2^257, t = z0 + z1 2^128 + z2 2^256.
-// Three 4 x 4 products (96 multiply-adds) instead of 128, for about 60 adds,
-// which run on the integer ALU pipe rather than the multiply-add one.
-__device__ __forceinline__ void mul256_kara_ptx(uint32_t t[16], const uint32_t a[8], const uint32_t b[8]) {
-    uint32_t z0[8], z2[8], p[8], sa[4], sb[4], ca, cb;
-    mul128_ptx(z0, a, b);
-    mul128_ptx(z2, a + 4, b + 4);
+// s = x mod 2^128 + x >> 128 (4 limbs) and its carry bit c.
+__device__ __forceinline__ void kara_sum_ptx(uint32_t sa[4], uint32_t& ca, const uint32_t a[8]) {
     asm("add.cc.u32 %0, %5, %9;\n\t"
         "addc.cc.u32 %1, %6, %10;\n\t"
         "addc.cc.u32 %2, %7, %11;\n\t"
@@ -124,14 +115,14 @@ __device__ __forceinline__ void mul256_kara_ptx(uint32_t t[16], const uint32_t a
         "addc.u32 %4, 0, 0;"
         : "=r"(sa[0]), "=r"(sa[1]), "=r"(sa[2]), "=r"(sa[3]), "=r"(ca)
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]));
-    asm("add.cc.u32 %0, %5, %9;\n\t"
-        "addc.cc.u32 %1, %6, %10;\n\t"
-        "addc.cc.u32 %2, %7, %11;\n\t"
-        "addc.cc.u32 %3, %8, %12;\n\t"
-        "addc.u32 %4, 0, 0;"
-        : "=r"(sb[0]), "=r"(sb[1]), "=r"(sb[2]), "=r"(sb[3]), "=r"(cb)
-        : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
-    mul128_ptx(p, sa, sb);
+}
+
+// Karatsuba combination: t = z0 + (m - z0 - z2) 2^128 + z2 2^256 where
+// m = (sa + ca 2^128)(sb + cb 2^128) = p + ca sb 2^128 + cb sa 2^128 + ca cb 2^256
+// and p = sa sb (all exact; m - z0 - z2 < 2^257).
+__device__ __forceinline__ void kara_combine_ptx(uint32_t t[16], const uint32_t z0[8], const uint32_t z2[8],
+                                                 uint32_t p[8], const uint32_t sa[4], const uint32_t sb[4],
+                                                 uint32_t ca, uint32_t cb) {
     // m[0..8] = p + (ca ? sb : 0) 2^128 + (cb ? sa : 0) 2^128 + ca cb 2^256
     const uint32_t ma = 0u - ca, mb = 0u - cb;
     uint32_t m8;
@@ -193,6 +184,23 @@ __device__ __forceinline__ void mul256_kara_ptx(uint32_t t[16], const uint32_t a
         : "r"(z0[4]), "r"(z0[5]), "r"(z0[6]), "r"(z0[7]), "r"(z2[0]), "r"(z2[1]), "r"(z2[2]), "r"(z2[3]),
           "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]),
           "r"(m8), "r"(z2[4]), "r"(z2[5]), "r"(z2[6]), "r"(z2[7]));
+}
+
+// 256 x 256 -> 512 by one level of Karatsuba on 128-bit halves:
+// a = a0 + a1 2^128, b = b0 + b1 2^128, z0 = a0 b0, z2 = a1 b1,
+// m = (a0 + a1)(b0 + b1) with the two sums' carry bits ca, cb handled as
+// m = sa sb + ca sb 2^128 + cb sa 2^128 + ca cb 2^256 (sa, sb their low 128
+// bits), z1 = m - z0 - z2 = a0 b1 + a1 b0 < 2^257, t = z0 + z1 2^128 + z2 2^256.
+// Three 4 x 4 products (96 multiply-adds) instead of 128, for about 60 adds,
+// which run on the integer ALU pipe rather than the multiply-add one.
+__device__ __forceinline__ void mul256_kara_ptx(uint32_t t[16], const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t z0[8], z2[8], p[8], sa[4], sb[4], ca, cb;
+    mul128_ptx(z0, a, b);
+    mul128_ptx(z2, a + 4, b + 4);
+    kara_sum_ptx(sa, ca, a);
+    kara_sum_ptx(sb, cb, b);
+    mul128_ptx(p, sa, sb);
+    kara_combine_ptx(t, z0, z2, p, sa, sb, ca, cb);
 }
 
 // The product the field multiply uses: Karatsuba (measured on B200: 157

@@ -18,6 +18,7 @@ namespace uf {
 namespace {
 // Items per host->device chunk: bounds device memory at ~130 B x 2^22 = 0.5 GB.
 constexpr size_t kPipeChunk = size_t{1} << 17;   // items per staging slot of a host-buffer call
+constexpr size_t kPipeFirst = size_t{1} << 14;   // items in a host-buffer call's first chunk
 constexpr size_t kDeviceChunk = size_t{1} << 17; // items per launch of a large device-buffer call
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
@@ -163,7 +164,7 @@ Backend::~Backend() {
             cudaEventDestroy(djoin_);
             cudaStreamDestroy(dstream_);
         }
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < kPipeSlots; ++j) {
             if (pstream_[j]) cudaStreamSynchronize(pstream_[j]);
             pstage_[j].release();
             dstage_[j].release();
@@ -278,26 +279,27 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
     cudaError_t e = cudaSetDevice(dev_);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
     if (!pstream_[0]) {
-        for (int j = 0; j < 2 && e == cudaSuccess; ++j) {
+        for (int j = 0; j < kPipeSlots && e == cudaSuccess; ++j) {
             e = cudaStreamCreateWithFlags(&pstream_[j], cudaStreamNonBlocking);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pev_[j], cudaEventDisableTiming);
         }
         if (e != cudaSuccess) return cuda_error(e, "pipeline streams");
     }
-    // Chunks of up to kPipeChunk items alternate between two pinned staging
-    // slots: the CPU packs chunk k + 1 (and unpacks chunk k - 1's verdicts)
-    // while the device copies in and verifies chunk k.  Per chunk the slot is
+    // Chunks of up to kPipeChunk items rotate through kPipeSlots pinned
+    // staging slots: the CPU packs chunk k + 2 (and unpacks chunk k - 1's
+    // verdicts) while the device copies in and verifies chunks k and k + 1.  Per chunk the slot is
     // laid out msgs | keys | sigs (16-byte aligned) | verdicts, copied in and
     // out with one transfer each way.
     const size_t pub_sz = kind == 1 ? 32 : 33;
     const size_t sub = std::min(count, kPipeChunk);
     auto a16 = [](size_t v) { return (v + 15) & ~size_t{15}; };
     const size_t slot_bytes = a16(sub * (32 + pub_sz)) + sub * 64 + sub + 16;
-    for (int j = 0; j < 2; ++j) {
+    const int slots = count > kPipeFirst ? kPipeSlots : 1;   // chunks of the ramp below use every slot
+    for (int j = 0; j < slots; ++j) {
         if ((e = pstage_[j].ensure(slot_bytes)) != cudaSuccess) return cuda_error(e, "cudaHostAlloc(staging)");
         if ((e = dstage_[j].ensure(slot_bytes)) != cudaSuccess) return cuda_error(e, "cudaMalloc(staging)");
     }
-    size_t pend_off[2] = {0, 0}, pend_n[2] = {0, 0}, pend_out[2] = {0, 0};
+    size_t pend_off[kPipeSlots] = {}, pend_n[kPipeSlots] = {}, pend_out[kPipeSlots] = {};
     auto drain = [&](int j) -> cudaError_t {
         if (!pend_n[j]) return cudaSuccess;
         const cudaError_t r = cudaEventSynchronize(pev_[j]);
@@ -305,24 +307,32 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
         pend_n[j] = 0;
         return r;
     };
-    size_t k = 0;
-    for (size_t off = 0; off < count; off += sub, ++k) {
-        const int j = (int)(k & 1);
+    // Chunk sizes ramp up from kPipeFirst, doubling to kPipeChunk: the
+    // pipeline's fill (packing and copying the first chunk while the device
+    // is idle) costs a small chunk, and the device fills up while the CPU
+    // packs the next, larger ones.
+    size_t k = 0, m = 0;
+    for (size_t off = 0; off < count; off += m, ++k) {
+        const int j = (int)(k % kPipeSlots);
         if ((e = drain(j)) != cudaSuccess) return cuda_error(e, "verify");
-        const size_t m = std::min(sub, count - off);
+        m = std::min(std::min(sub, kPipeFirst << std::min<size_t>(k, 20)), count - off);
         const size_t o_p = m * 32, o_s = a16(o_p + m * pub_sz), o_o = o_s + m * 64;
         uint8_t* h = (uint8_t*)pstage_[j].p;
         uint8_t* d = (uint8_t*)dstage_[j].p;
-        auto pack = [m, off](uint8_t* dst, const uint8_t* src, size_t width, size_t stride) {
-            if (stride == width) {
-                memcpy(dst, src + off * width, m * width);
-            } else {
-                for (size_t i = 0; i < m; ++i) memcpy(dst + i * width, src + (off + i) * stride, width);
-            }
+        // items [lo, hi) of this chunk into the slot
+        auto pack = [&](size_t lo, size_t hi) {
+            auto one = [&](uint8_t* dst, const uint8_t* src, size_t width, size_t stride) {
+                if (stride == width) {
+                    memcpy(dst + lo * width, src + (off + lo) * width, (hi - lo) * width);
+                } else {
+                    for (size_t i = lo; i < hi; ++i) memcpy(dst + i * width, src + (off + i) * stride, width);
+                }
+            };
+            one(h, msgs, 32, m_stride);
+            one(h + o_p, pubs, pub_sz, p_stride);
+            one(h + o_s, sigs, 64, s_stride);
         };
-        pack(h, msgs, 32, m_stride);
-        pack(h + o_p, pubs, pub_sz, p_stride);
-        pack(h + o_s, sigs, 64, s_stride);
+        pack(0, m);
         if (collect) memcpy(h + o_o, out + off, m);
         const size_t in_bytes = o_o + (collect ? m : 0);
         if ((e = cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, pstream_[j])) != cudaSuccess)
@@ -336,7 +346,7 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
         pend_n[j] = m;
         pend_out[j] = o_o;
     }
-    for (int j = 0; j < 2; ++j)
+    for (int j = 0; j < kPipeSlots; ++j)
         if ((e = drain(j)) != cudaSuccess) return cuda_error(e, "verify");
     clear_error();
     return kOk;

@@ -118,12 +118,15 @@ private:
     cudaStream_t stream_ = nullptr;
     void* d_gtab_ = nullptr;
     DevBuf msgs_, pubs_, sigs_, out_, scratch_, ops_in_;
-    // host-buffer calls: two pinned staging slots, each with its own stream,
-    // so that packing chunk k + 1 on the CPU overlaps verifying chunk k
-    HostBuf pstage_[2];
-    DevBuf dstage_[2];
-    cudaStream_t pstream_[2] = {nullptr, nullptr};
-    cudaEvent_t pev_[2] = {nullptr, nullptr};
+    // host-buffer calls: kPipeSlots pinned staging slots, each with its own
+    // stream, so that the CPU packs chunk k + 2 while the device verifies
+    // chunks k and k + 1 (the next launch is always queued behind the running
+    // ones, and their last partial waves overlap)
+    static constexpr int kPipeSlots = 3;
+    HostBuf pstage_[kPipeSlots];
+    DevBuf dstage_[kPipeSlots];
+    cudaStream_t pstream_[kPipeSlots] = {};
+    cudaEvent_t pev_[kPipeSlots] = {};
     // large device-buffer calls: second stream with fork / join events
     cudaStream_t dstream_ = nullptr;
     cudaEvent_t dfork_ = nullptr, djoin_ = nullptr;

@@ -287,6 +287,25 @@ def test_chunked_host_call(gpu_ctx, oracle):
     assert (got == np.tile(want, reps)[:n]).all()
 
 
+@pytest.mark.parametrize("n", [16383, 16384, 16385, 49151, 49153, 114688, 131072, 131073, 245761, 393217])
+def test_host_pipeline_chunk_edges(gpu_ctx, oracle, n):
+    """Host-buffer calls are cut into chunks of 16384, 32768, 65536 and then
+    131072 items over three staging slots: sizes on and around those edges keep
+    every verdict in place (ECDSA with collect, BIP-340 plain)."""
+    base = 2048
+    m, x, s = schnorr_corpus(oracle, base, seed=300, tamper=0.1)
+    want = oracle.schnorr_verify_batch(m, x, s)
+    reps = -(-n // base)
+    tile = lambda a: np.ascontiguousarray(np.tile(a, (reps, 1))[:n])
+    assert (gpu_ctx.schnorr_verify_batch(tile(m), tile(x), tile(s)) == np.tile(want, reps)[:n]).all()
+    me, pe, se = ecdsa_corpus(oracle, base, seed=301, tamper=0.1)
+    we = oracle.ecdsa_verify_batch(me, pe, se)
+    kb = np.full(n, 0x5A, np.uint8)
+    gpu_ctx.ecdsa_verify_collect(tile(me), tile(pe), tile(se), kb)
+    w = np.tile(we, reps)[:n]
+    assert ((kb == 0) == (w == 1)).all() and (kb[w == 0] == 0x5A).all()
+
+
 @pytest.mark.parametrize("n", [1, 2, 31, 127, 129, 1000])
 def test_ragged_sizes(gpu_ctx, oracle, n):
     m, p, s = ecdsa_corpus(oracle, n, seed=100 + n, tamper=0.3)

@@ -9,12 +9,12 @@
 #include <stdint.h>
 
 // Window width (bits) of the generator streams, library-wide: the per-context
-// G / lambda G tables hold 2^(UF_GWIN-1) multiples each.  16-bit windows (one
-// per four 4-bit P windows, 2 x 32768 entries, 4 MB, served from L2): 18
-// table additions per verify, against 22 for 12-bit windows (2 x 2048
-// entries, 256 KB) and 34 for 8-bit ones (16 KB).
+// G / lambda G tables hold 2^(UF_GWIN-1) multiples each.  20-bit windows (one
+// per five 4-bit P windows, 2 x 2^19 entries, 64 MB, served from the 126 MB
+// L2): 14 table additions per verify, against 18 for 16-bit windows (4 MB),
+// 22 for 12-bit ones (256 KB) and 34 for 8-bit ones (16 KB).
 #ifndef UF_GWIN
-#define UF_GWIN 16
+#define UF_GWIN 20
 #endif
 
 #if defined(__CUDACC__)

@@ -3,8 +3,8 @@
 // SmemTab: a thread's 1P..8P table in dynamic shared memory, laid out
 // [entry][quad][thread] as uint4 so that each thread owns a bank column and a
 // warp's data-dependent reads never conflict.  GlobalGT: the per-context
-// 1..2^(UF_GWIN-1) multiples of G and lambda*G in global memory (4 MB for
-// 16-bit windows; L2-resident), read through the read-only L1 path.
+// 1..2^(UF_GWIN-1) multiples of G and lambda*G in global memory (64 MB for
+// 20-bit windows; served from L2), read through the read-only L1 path.
 #pragma once
 #include "fe.cuh"
 

@@ -12,7 +12,7 @@
 //    data-dependent positions would make the warp add at almost every bit);
 //  * P streams: 4-bit windows, table of 1P..8P (affine, one field inversion per
 //    signature through a batch-to-affine), lambda P via one beta multiplication;
-//  * G streams: UF_GWIN-bit windows (16: every fourth P window), tables of the 2^(UF_GWIN-1) multiples
+//  * G streams: UF_GWIN-bit windows (20: every fifth P window), tables of the 2^(UF_GWIN-1) multiples
 //    of G and of lambda G computed once per context and read through L1 / L2;
 //  * 33 P windows x 4 bits = 132 >= 129 bits, so 128 doublings in total.
 #pragma once
@@ -27,13 +27,13 @@ namespace uf {
 constexpr int kWP = 4;     // P window bits
 constexpr int kNWP = 33;   // P windows
 constexpr int kWG = UF_GWIN;                  // G window bits (a multiple of kWP)
-constexpr int kNWG = (129 + kWG - 1) / kWG;   // G windows: 9 for 16 bits (one per four P windows)
+constexpr int kNWG = (129 + kWG - 1) / kWG;   // G windows: 7 for 20 bits (one per five P windows)
 constexpr int kGEvery = kWG / kWP;            // P windows per G window
 static_assert(kWG % kWP == 0 && kNWG * kGEvery >= kNWP, "G windows must align with P windows");
 static_assert(kWG <= 30, "G Booth digits (up to 2^(kWG-1)) are stored as int32_t");
 typedef int32_t GDigit;   // a G-stream Booth digit, |d| <= 2^(kWG-1)
 constexpr int kPTab = 8;   // 1P..8P
-constexpr int kGTab = 1 << (kWG - 1); // 1G..32768G for 16-bit windows (and the same for lambda G)
+constexpr int kGTab = 1 << (kWG - 1); // 1G..2^19 G for 20-bit windows (and the same for lambda G)
 
 // Signed fixed-window (Booth) digits of a magnitude k < 2^129:
 // d_i = b_{wi-1} + sum_{t<w-1} b_{wi+t} 2^t - b_{wi+w-1} 2^(w-1), d_i in [-2^(w-1), 2^(w-1)],

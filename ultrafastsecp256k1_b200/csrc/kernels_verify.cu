@@ -6,7 +6,7 @@
 //   * dynamic shared memory holds each thread's 1P..8P table as
 //     [entry][quad][thread] uint4, so a warp's data-dependent table reads are
 //     bank-conflict free (each thread owns its own bank column);
-//   * the 1..2^(UF_GWIN-1) multiples of G and lambda*G (4 MB for 16-bit
+//   * the 1..2^(UF_GWIN-1) multiples of G and lambda*G (64 MB for 20-bit
 //     windows) stay in global memory, served from L2 through the read-only path;
 //   * Booth digits live in a small per-thread local array indexed uniformly
 //     across the warp (coalesced, L1 resident).

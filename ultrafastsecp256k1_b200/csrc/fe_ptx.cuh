@@ -1,6 +1,10 @@
-// 256 x 256 -> 512-bit product with PTX carry chains (device only).
+// Field building blocks in PTX carry chains (device only): the 256 x 256 ->
+// 512-bit product (rows below, and one level of Karatsuba on 128-bit halves,
+// the form the field multiply uses), the two folds of the reduction by
+// 2^256 = 2^32 + 977 (mod p), and add / sub / small shifts whose folds touch
+// only the limbs a fold reaches in the common case.
 //
-// Operand scanning, one row per limb b[i] of the multiplier.  Within a row the
+// Row product: operand scanning, one row per limb b[i] of the multiplier.  Within a row the
 // products a[j]*b[i] are split by the parity of j, because lo(a[j] b[i]) lands
 // on limb i+j and hi(a[j] b[i]) on i+j+1: the even products (j = 0,2,4,6) then
 // touch limbs i..i+7 exactly once each and form ONE unbroken carry chain

@@ -218,11 +218,20 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* 
  * variants compute the same verdicts; they differ in how much of the field /
  * point arithmetic is inlined (instruction-cache footprint vs. call overhead).
  * ultrafastsecp256k1_b200.autotune measures them and writes the tuning file
- * read at context creation (UFSECP_B200_TUNING). */
+ * read at context creation (UFSECP_B200_TUNING).  The tuning may also name a
+ * small-launch variant per kind, used by launches of at most `items` items
+ * (latency-bound launches with a few warps per SM, where inlining the field
+ * arithmetic wins); set_variant applies its variant to every launch size and
+ * clears the small-launch one.  get_small_variant reports -1 when none. */
 #define UFSECP_EXT_VERIFY_VARIANTS 9
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_variant(ufsecp_gpu_ctx* ctx, int kind, int variant);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out,
                                                      int* blocks_per_sm_out);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_small_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out,
+                                                           uint32_t* items_out);
+/* variant -1 removes the small-launch variant of `kind`. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_small_variant(ufsecp_gpu_ctx* ctx, int kind, int variant,
+                                                           uint32_t items);
 
 /* Measured 32-bit integer multiply-add issue rate of the device (ops / s):
  * every thread of a full grid runs 16 independent mad.lo.u32 chains. */

@@ -415,6 +415,7 @@ def test_every_kernel_variant_matches_oracle(gpu_ctx, oracle, variant):
     m, p, s = ecdsa_corpus(oracle, 700, seed=60 + variant, tamper=0.2)
     mx, x, sx = schnorr_corpus(oracle, 700, seed=70 + variant, tamper=0.2)
     old = (gpu_ctx.get_variant(0)[0], gpu_ctx.get_variant(1)[0])
+    old_small = (gpu_ctx.get_small_variant(0), gpu_ctx.get_small_variant(1))
     try:
         gpu_ctx.set_variant(0, variant)
         gpu_ctx.set_variant(1, variant)
@@ -428,3 +429,32 @@ def test_every_kernel_variant_matches_oracle(gpu_ctx, oracle, variant):
     finally:
         gpu_ctx.set_variant(0, old[0])
         gpu_ctx.set_variant(1, old[1])
+        for k in (0, 1):
+            gpu_ctx.set_small_variant(k, *old_small[k])
+
+
+def test_small_launch_variant_from_tuning(oracle, tmp_path, monkeypatch):
+    """A tuning file's small-launch variants apply to launches up to their item
+    limit and the main variant above it; verdicts match the oracle on both
+    sides, and set_variant removes the small-launch variant."""
+    import ultrafastsecp256k1_b200 as uf
+    tune = tmp_path / "tuning.txt"
+    tune.write_text("ecdsa_variant 4\necdsa_small_variant 6\necdsa_small_items 1000\n"
+                    "schnorr_variant 8\nschnorr_small_variant 0\nschnorr_small_items 500\n")
+    monkeypatch.setenv("UFSECP_B200_TUNING", str(tune))
+    monkeypatch.delenv("UFSECP_B200_VARIANT_ECDSA", raising=False)
+    monkeypatch.delenv("UFSECP_B200_VARIANT_SCHNORR", raising=False)
+    ctx = uf.GpuContext(0)
+    try:
+        assert ctx.get_variant(0)[0] == 4 and ctx.get_small_variant(0) == (6, 1000)
+        assert ctx.get_variant(1)[0] == 8 and ctx.get_small_variant(1) == (0, 500)
+        for n in (999, 1000, 1001):
+            m, p, s = ecdsa_corpus(oracle, n, seed=500 + n, tamper=0.2)
+            assert (ctx.ecdsa_verify_batch(m, p, s) == oracle.ecdsa_verify_batch(m, p, s)).all()
+        for n in (499, 500, 501):
+            m, x, s = schnorr_corpus(oracle, n, seed=600 + n, tamper=0.2)
+            assert (ctx.schnorr_verify_batch(m, x, s) == oracle.schnorr_verify_batch(m, x, s)).all()
+        ctx.set_variant(0, 4)
+        assert ctx.get_small_variant(0) == (-1, 0)
+    finally:
+        ctx.close()

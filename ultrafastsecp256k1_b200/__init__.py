@@ -107,6 +107,9 @@ _SIGS = {
     "ufsecp_gpu_ext_set_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "ufsecp_gpu_ext_get_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                   ctypes.POINTER(ctypes.c_int)]),
+    "ufsecp_gpu_ext_get_small_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                        ctypes.POINTER(ctypes.c_uint32)]),
+    "ufsecp_gpu_ext_set_small_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32]),
     "ufsecp_gpu_ext_imad_peak": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "ufsecp_gpu_ext_diag": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_probe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -372,6 +375,17 @@ class GpuContext:
         self._check(self.L.ufsecp_gpu_ext_get_variant(self._ctx, kind, ctypes.byref(v), ctypes.byref(b)),
                     "get_variant")
         return v.value, b.value
+
+    def get_small_variant(self, kind: int):
+        """(variant, items): launches of at most `items` items use `variant`; (-1, 0) when none."""
+        v, n = ctypes.c_int(), ctypes.c_uint32()
+        self._check(self.L.ufsecp_gpu_ext_get_small_variant(self._ctx, kind, ctypes.byref(v), ctypes.byref(n)),
+                    "get_small_variant")
+        return v.value, n.value
+
+    def set_small_variant(self, kind: int, variant: int, items: int = 0) -> None:
+        """Launches of at most `items` items use `variant` (-1: none)."""
+        self._check(self.L.ufsecp_gpu_ext_set_small_variant(self._ctx, kind, variant, items), "set_small_variant")
 
     def imad_peak(self) -> float:
         v = ctypes.c_double()

@@ -6,7 +6,8 @@ For each signature kind (ECDSA, BIP-340) it times every verify-kernel variant
 (ufsecp_gpu_ext_set_variant; the variants differ in how much field / point
 arithmetic is inlined, i.e. instruction-cache footprint against call
 overhead) on a GPU-signed batch, checks that all variants return identical
-verdicts, and picks them; then, for RLC batch verification, it times the
+verdicts, and picks them, plus a small-launch variant and its item limit for
+latency-bound launches (a few warps per SM); then, for RLC batch verification, it times the
 Pippenger window width (the MSM bucket width, 2^(c-1) buckets per window)
 for each batch size of 64 / 512 / 4096 / 16384 over the model's choice and
 its neighbours and picks the fastest.  The winners go to a tuning file of
@@ -76,6 +77,32 @@ def time_variant(ctx, torch, kind, bufs, n, reps=3):
     return n / (ms * 1e-3), out.cpu().numpy()
 
 
+SMALL_SIZES = (4096, 16384, 32768, 65536)
+
+
+def tune_small(ctx, torch, kind, bufs, main: int, reps: int = 10) -> dict:
+    """Small launches (a few warps per SM) are latency-bound, where inlining
+    the field arithmetic can beat the variant that is fastest at full
+    occupancy.  Times every variant at SMALL_SIZES; the fastest at the
+    smallest size becomes the small-launch variant, used up to the largest
+    size at which it still beats `main` (none if it never does)."""
+    rates = {v: {} for v in range(VARIANTS)}
+    for v in range(VARIANTS):
+        ctx.set_variant(kind, v)
+        for n in SMALL_SIZES:
+            rates[v][n] = time_variant(ctx, torch, kind, bufs, n, reps)[0]
+    ctx.set_variant(kind, main)
+    small = max(range(VARIANTS), key=lambda v: rates[v][SMALL_SIZES[0]])
+    items = 0
+    for n in SMALL_SIZES:
+        if small != main and rates[small][n] > rates[main][n]:
+            items = n
+        else:
+            break
+    return {"variant": small if items else None, "items": items,
+            "sigs_per_s": {str(v): {str(n): r for n, r in rs.items()} for v, rs in rates.items()}}
+
+
 def model_window(n: int) -> int:
     """The backend's cost model (rlc_window_bits in csrc/rlc.cu)."""
     best, cost = 4, float("inf")
@@ -133,15 +160,19 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
                 rates[v] = rate
             best = max(rates, key=rates.get)
             res["kinds"][label] = {"sigs_per_s": {str(k): r for k, r in rates.items()}, "best": best,
-                                   "valid": int(ref.sum())}
+                                   "valid": int(ref.sum()), "small": tune_small(ctx, torch, kind, bufs, best)}
             ctx.set_variant(kind, best)
         res["rlc_window"] = tune_rlc(ctx, torch)
     if write:
         path = out_path or tuning_path(name, info.compute_units)
         os.makedirs(os.path.dirname(path), exist_ok=True)
         with open(path, "w") as f:
-            f.write(f"ecdsa_variant {res['kinds']['ecdsa']['best']}\n")
-            f.write(f"schnorr_variant {res['kinds']['schnorr']['best']}\n")
+            for label in ("ecdsa", "schnorr"):
+                k = res["kinds"][label]
+                f.write(f"{label}_variant {k['best']}\n")
+                if k["small"]["variant"] is not None:
+                    f.write(f"{label}_small_variant {k['small']['variant']}\n")
+                    f.write(f"{label}_small_items {k['small']['items']}\n")
             for size, r in res["rlc_window"].items():
                 f.write(f"rlc_window_{size} {r['best']}\n")
         res["tuning_file"] = path

@@ -580,6 +580,20 @@ ufsecp_error_t ufsecp_gpu_ext_get_variant(ufsecp_gpu_ctx* ctx, int kind, int* va
     return UFSECP_OK;
 }
 
+ufsecp_error_t ufsecp_gpu_ext_get_small_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out,
+                                                uint32_t* items_out) {
+    if (!ctx || !variant_out) return UFSECP_ERR_NULL_ARG;
+    if (kind < 0 || kind > 1) return UFSECP_ERR_BAD_INPUT;
+    *variant_out = ctx->backend->small_variant(kind);
+    if (items_out) *items_out = *variant_out >= 0 ? ctx->backend->small_items(kind) : 0;
+    return UFSECP_OK;
+}
+
+ufsecp_error_t ufsecp_gpu_ext_set_small_variant(ufsecp_gpu_ctx* ctx, int kind, int variant, uint32_t items) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->set_small_variant(kind, variant, items);
+}
+
 ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) {
     if (!ctx || !ops_per_s) return UFSECP_ERR_NULL_ARG;
     return ctx->backend->imad_peak(ops_per_s);

@@ -38,22 +38,34 @@ int env_int(const char* name, int dflt) {
 
 cudaError_t Backend::launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
                                    uint8_t* out, int collect, cudaStream_t st) {
-    const int v = variant_[kind & 1];
-    return kLaunchers[v](kind, m, p, s, n, d_gtab_, out, collect, grid_[v][kind & 1], st);
+    const int k = kind & 1;
+    const int v = small_variant_[k] >= 0 && n <= small_items_[k] ? small_variant_[k] : variant_[k];
+    return kLaunchers[v](kind, m, p, s, n, d_gtab_, out, collect, grid_[v][k], st);
 }
 
 int Backend::set_variant(int kind, int v) {
     if (kind < 0 || kind > 1 || v < 0 || v >= kVerifyVariants) return set_error(kErrBadInput, "bad variant");
     variant_[kind] = v;
+    small_variant_[kind] = -1;   // an explicit choice applies to every launch size
+    clear_error();
+    return kOk;
+}
+
+int Backend::set_small_variant(int kind, int v, uint32_t items) {
+    if (kind < 0 || kind > 1 || v < -1 || v >= kVerifyVariants) return set_error(kErrBadInput, "bad variant");
+    small_variant_[kind] = v;
+    small_items_[kind] = v >= 0 ? items : 0;
     clear_error();
     return kOk;
 }
 
 // Per-device tuning: a file of "key value" lines (ecdsa_variant,
-// schnorr_variant) written by ultrafastsecp256k1_b200.autotune.  It is the file
-// named by UFSECP_B200_TUNING, else tuning/<device name>_<SMs>sm.txt beside the
-// library's lib/ directory.  UFSECP_B200_VARIANT_ECDSA / _SCHNORR override
-// single entries.
+// schnorr_variant, their small-launch counterparts ecdsa_small_variant /
+// ecdsa_small_items and schnorr_small_variant / schnorr_small_items, and
+// rlc_window_<batch>) written by ultrafastsecp256k1_b200.autotune.  It is the
+// file named by UFSECP_B200_TUNING, else tuning/<device name>_<SMs>sm.txt
+// beside the library's lib/ directory.  UFSECP_B200_VARIANT_ECDSA / _SCHNORR
+// override a kind's variant for every launch size.
 void Backend::load_tuning() {
     std::string path_s;
     const char* env = getenv("UFSECP_B200_TUNING");
@@ -89,6 +101,11 @@ void Backend::load_tuning() {
             while (fscanf(f, "%63s %d", key, &val) == 2) {
                 if (!strcmp(key, "ecdsa_variant") && val >= 0 && val < kVerifyVariants) variant_[0] = val;
                 if (!strcmp(key, "schnorr_variant") && val >= 0 && val < kVerifyVariants) variant_[1] = val;
+                if (!strcmp(key, "ecdsa_small_variant") && val >= 0 && val < kVerifyVariants) small_variant_[0] = val;
+                if (!strcmp(key, "schnorr_small_variant") && val >= 0 && val < kVerifyVariants)
+                    small_variant_[1] = val;
+                if (!strcmp(key, "ecdsa_small_items") && val > 0) small_items_[0] = (uint32_t)val;
+                if (!strcmp(key, "schnorr_small_items") && val > 0) small_items_[1] = (uint32_t)val;
                 unsigned size = 0;
                 if (sscanf(key, "rlc_window_%u", &size) == 1 && size > 0 && val >= 4 && val <= 16)
                     rlc_window_[size] = val;
@@ -97,8 +114,14 @@ void Backend::load_tuning() {
         }
     }
     const int ve = env_int("UFSECP_B200_VARIANT_ECDSA", -1), vs = env_int("UFSECP_B200_VARIANT_SCHNORR", -1);
-    if (ve >= 0 && ve < kVerifyVariants) variant_[0] = ve;
-    if (vs >= 0 && vs < kVerifyVariants) variant_[1] = vs;
+    if (ve >= 0 && ve < kVerifyVariants) {
+        variant_[0] = ve;
+        small_variant_[0] = -1;
+    }
+    if (vs >= 0 && vs < kVerifyVariants) {
+        variant_[1] = vs;
+        small_variant_[1] = -1;
+    }
 }
 
 cudaError_t DevBuf::ensure(size_t bytes) {

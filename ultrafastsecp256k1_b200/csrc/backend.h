@@ -97,7 +97,10 @@ public:
 
     // Kernel variant per signature kind (0 ECDSA, 1 BIP-340) and its grid.
     int variant(int kind) const { return variant_[kind & 1]; }
+    int small_variant(int kind) const { return small_variant_[kind & 1]; }
+    uint32_t small_items(int kind) const { return small_items_[kind & 1]; }
     int set_variant(int kind, int v);
+    int set_small_variant(int kind, int v, uint32_t items);   // v = -1: none
     int verify_grid(int kind) const { return grid_[variant_[kind & 1]][kind & 1]; }
     int blocks_per_sm(int kind, int v) const { return sms_ ? grid_[v][kind & 1] / sms_ : 0; }
 
@@ -112,6 +115,11 @@ private:
     std::string dev_name_;
     int grid_[9][2] = {};        // [variant][kind] resident-grid size
     int variant_[2] = {4, 4};    // chosen variant per kind (4: out-of-line field / point ops, PTX chains)
+    // Launches of at most small_items_[kind] items (latency-bound: a few warps
+    // per SM) use small_variant_[kind] instead, when the tuning names one; an
+    // explicit set_variant / environment override clears it.
+    int small_variant_[2] = {-1, -1};
+    uint32_t small_items_[2] = {0, 0};
     cudaError_t launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
                               uint8_t* out, int collect, cudaStream_t st);
     void load_tuning();

@@ -219,9 +219,9 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* 
  * point arithmetic is inlined (instruction-cache footprint vs. call overhead).
  * ultrafastsecp256k1_b200.autotune measures them and writes the tuning file
  * read at context creation (UFSECP_B200_TUNING).  The tuning may also name a
- * small-launch variant per kind, used by launches of at most `items` items
- * (latency-bound launches with a few warps per SM, where inlining the field
- * arithmetic wins); set_variant applies its variant to every launch size and
+ * small-launch variant per kind, used by verify calls of at most `items`
+ * items (latency-bound launches with a few warps per SM, where inlining the
+ * field arithmetic wins; the chunks of a larger call keep the main variant); set_variant applies its variant to every launch size and
  * clears the small-launch one.  get_small_variant reports -1 when none. */
 #define UFSECP_EXT_VERIFY_VARIANTS 9
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_variant(ufsecp_gpu_ctx* ctx, int kind, int variant);

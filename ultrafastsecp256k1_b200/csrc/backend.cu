@@ -37,9 +37,9 @@ int env_int(const char* name, int dflt) {
 }  // namespace
 
 cudaError_t Backend::launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
-                                   uint8_t* out, int collect, cudaStream_t st) {
+                                   uint8_t* out, int collect, cudaStream_t st, size_t call_items) {
     const int k = kind & 1;
-    const int v = small_variant_[k] >= 0 && n <= small_items_[k] ? small_variant_[k] : variant_[k];
+    const int v = small_variant_[k] >= 0 && call_items <= small_items_[k] ? small_variant_[k] : variant_[k];
     return kLaunchers[v](kind, m, p, s, n, d_gtab_, out, collect, grid_[v][k], st);
 }
 
@@ -258,7 +258,7 @@ int Backend::verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pub
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
     cudaStream_t s = stream ? stream : stream_;
     if (count < 2 * kDeviceChunk) {
-        e = launch_verify(kind, d_msgs, d_pubs, d_sigs, (uint32_t)count, d_out, 0, s);
+        e = launch_verify(kind, d_msgs, d_pubs, d_sigs, (uint32_t)count, d_out, 0, s, count);
         if (e != cudaSuccess) return cuda_error(e, "verify launch");
         clear_error();
         return kOk;
@@ -280,7 +280,7 @@ int Backend::verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pub
     for (size_t off = 0; off < count; off += kDeviceChunk, ++k) {
         const size_t m = std::min(kDeviceChunk, count - off);
         e = launch_verify(kind, d_msgs + 32 * off, d_pubs + pub_sz * off, d_sigs + 64 * off, (uint32_t)m, d_out + off,
-                          0, (k & 1) ? dstream_ : s);
+                          0, (k & 1) ? dstream_ : s, count);
         if (e != cudaSuccess) return cuda_error(e, "verify launch");
     }
     if ((e = cudaEventRecord(djoin_, dstream_)) != cudaSuccess || (e = cudaStreamWaitEvent(s, djoin_, 0)) != cudaSuccess)
@@ -360,7 +360,7 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
         const size_t in_bytes = o_o + (collect ? m : 0);
         if ((e = cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, pstream_[j])) != cudaSuccess)
             return cuda_error(e, "host->device copy");
-        e = launch_verify(kind, d, d + o_p, d + o_s, (uint32_t)m, d + o_o, collect, pstream_[j]);
+        e = launch_verify(kind, d, d + o_p, d + o_s, (uint32_t)m, d + o_o, collect, pstream_[j], count);
         if (e != cudaSuccess) return cuda_error(e, "verify launch");
         if ((e = cudaMemcpyAsync(h + o_o, d + o_o, m, cudaMemcpyDeviceToHost, pstream_[j])) != cudaSuccess)
             return cuda_error(e, "device->host copy");

@@ -115,13 +115,16 @@ private:
     std::string dev_name_;
     int grid_[9][2] = {};        // [variant][kind] resident-grid size
     int variant_[2] = {4, 4};    // chosen variant per kind (4: out-of-line field / point ops, PTX chains)
-    // Launches of at most small_items_[kind] items (latency-bound: a few warps
-    // per SM) use small_variant_[kind] instead, when the tuning names one; an
-    // explicit set_variant / environment override clears it.
+    // Verify calls of at most small_items_[kind] items (latency-bound: a few
+    // warps per SM) use small_variant_[kind] instead, when the tuning names
+    // one; an explicit set_variant / environment override clears it.
     int small_variant_[2] = {-1, -1};
     uint32_t small_items_[2] = {0, 0};
+    // call_items: the size of the whole call this launch belongs to; the
+    // small-launch variant is used only when the whole call is small (the
+    // chunks of a large call run beside one another at full occupancy).
     cudaError_t launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
-                              uint8_t* out, int collect, cudaStream_t st);
+                              uint8_t* out, int collect, cudaStream_t st, size_t call_items);
     void load_tuning();
     cudaStream_t stream_ = nullptr;
     void* d_gtab_ = nullptr;

@@ -233,6 +233,17 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_small_variant(ufsecp_gpu_ctx* ctx, 
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_small_variant(ufsecp_gpu_ctx* ctx, int kind, int variant,
                                                            uint32_t items);
 
+/* Lanes per signature (kind 0 ECDSA, 1 BIP-340): with lanes = 2, calls of at
+ * most `items` items run two threads per signature, each over half of the
+ * four GLV streams, their partial sums added at the end: a shorter verify
+ * latency for 1.6x the arithmetic, which pays while the device has idle
+ * capacity (small calls).  lanes = 1 turns it off.  The tuning file sets it
+ * per kind (ecdsa_pair_items / schnorr_pair_items); set_variant turns it off.
+ * The opaque-row / column surfaces always use one lane. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_lanes(ufsecp_gpu_ctx* ctx, int kind, int lanes, uint32_t items);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_lanes(ufsecp_gpu_ctx* ctx, int kind, int* lanes_out,
+                                                   uint32_t* items_out);
+
 /* Measured 32-bit integer multiply-add issue rate of the device (ops / s):
  * every thread of a full grid runs 16 independent mad.lo.u32 chains. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s);

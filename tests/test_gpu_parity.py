@@ -433,6 +433,36 @@ def test_every_kernel_variant_matches_oracle(gpu_ctx, oracle, variant):
             gpu_ctx.set_small_variant(k, *old_small[k])
 
 
+def test_two_lanes_per_signature_match_oracle(gpu_ctx, oracle):
+    """Two threads per signature (ufsecp_gpu_ext_set_lanes): the golden sets,
+    the edge corpus, tampered corpora of odd sizes (partial warps) and the
+    collect form give the one-lane verdicts."""
+    _, wy, e = load_golden()
+    old = [gpu_ctx.get_lanes(k) for k in (0, 1)]
+    try:
+        for k in (0, 1):
+            gpu_ctx.set_lanes(k, 2, 1 << 22)
+            assert gpu_ctx.get_lanes(k) == (2, 1 << 22)
+        assert (gpu_ctx.ecdsa_verify_batch(wy["msgs"], wy["pubs"], wy["sigs"]) == wy["ref_valid"]).all()
+        assert (gpu_ctx.ecdsa_verify_batch(e["ecdsa_msgs"], e["ecdsa_pubs"], e["ecdsa_sigs"])
+                == e["ecdsa_ref_valid"]).all()
+        assert (gpu_ctx.schnorr_verify_batch(e["schnorr_msgs"], e["schnorr_pubs"], e["schnorr_sigs"])
+                == e["schnorr_ref_valid"]).all()
+        for n in (1, 17, 700):
+            m, p, s = ecdsa_corpus(oracle, n, seed=800 + n, tamper=0.25)
+            assert (gpu_ctx.ecdsa_verify_batch(m, p, s) == oracle.ecdsa_verify_batch(m, p, s)).all()
+            m, x, s = schnorr_corpus(oracle, n, seed=900 + n, tamper=0.25)
+            assert (gpu_ctx.schnorr_verify_batch(m, x, s) == oracle.schnorr_verify_batch(m, x, s)).all()
+        m, p, s = ecdsa_corpus(oracle, 333, seed=33, tamper=0.3)
+        want = oracle.ecdsa_verify_batch(m, p, s)
+        kb = np.full(333, 0x77, np.uint8)
+        gpu_ctx.ecdsa_verify_collect(m, p, s, kb)
+        assert ((kb == 0) == (want == 1)).all() and (kb[want == 0] == 0x77).all()
+    finally:
+        for k in (0, 1):
+            gpu_ctx.set_lanes(k, *((2, old[k][1]) if old[k][0] == 2 else (1, 0)))
+
+
 def test_small_launch_variant_from_tuning(oracle, tmp_path, monkeypatch):
     """A tuning file's small-launch variants apply to launches up to their item
     limit and the main variant above it; verdicts match the oracle on both

@@ -110,6 +110,9 @@ _SIGS = {
     "ufsecp_gpu_ext_get_small_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                         ctypes.POINTER(ctypes.c_uint32)]),
     "ufsecp_gpu_ext_set_small_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_set_lanes": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_get_lanes": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_uint32)]),
     "ufsecp_gpu_ext_imad_peak": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "ufsecp_gpu_ext_diag": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_probe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -382,6 +385,16 @@ class GpuContext:
         self._check(self.L.ufsecp_gpu_ext_get_small_variant(self._ctx, kind, ctypes.byref(v), ctypes.byref(n)),
                     "get_small_variant")
         return v.value, n.value
+
+    def set_lanes(self, kind: int, lanes: int, items: int = 0) -> None:
+        """lanes 2: calls of at most `items` items run two threads per signature; 1: off."""
+        self._check(self.L.ufsecp_gpu_ext_set_lanes(self._ctx, kind, lanes, items), "set_lanes")
+
+    def get_lanes(self, kind: int):
+        """(lanes, items) for signature kind 0 ECDSA / 1 BIP-340."""
+        l, n = ctypes.c_int(), ctypes.c_uint32()
+        self._check(self.L.ufsecp_gpu_ext_get_lanes(self._ctx, kind, ctypes.byref(l), ctypes.byref(n)), "get_lanes")
+        return l.value, n.value
 
     def set_small_variant(self, kind: int, variant: int, items: int = 0) -> None:
         """Launches of at most `items` items use `variant` (-1: none)."""

@@ -7,7 +7,8 @@ For each signature kind (ECDSA, BIP-340) it times every verify-kernel variant
 arithmetic is inlined, i.e. instruction-cache footprint against call
 overhead) on a GPU-signed batch, checks that all variants return identical
 verdicts, and picks them, plus a small-launch variant and its item limit for
-latency-bound launches (a few warps per SM); then, for RLC batch verification, it times the
+latency-bound launches (a few warps per SM) and the call size up to which two
+lanes per signature beat one; then, for RLC batch verification, it times the
 Pippenger window width (the MSM bucket width, 2^(c-1) buckets per window)
 for each batch size of 64 / 512 / 4096 / 16384 over the model's choice and
 its neighbours and picks the fastest.  The winners go to a tuning file of
@@ -77,7 +78,7 @@ def time_variant(ctx, torch, kind, bufs, n, reps=3):
     return n / (ms * 1e-3), out.cpu().numpy()
 
 
-SMALL_SIZES = (4096, 16384, 32768, 65536)
+SMALL_SIZES = (4096, 8192, 16384, 32768, 65536)
 
 
 def tune_small(ctx, torch, kind, bufs, main: int, reps: int = 10) -> dict:
@@ -101,6 +102,25 @@ def tune_small(ctx, torch, kind, bufs, main: int, reps: int = 10) -> dict:
             break
     return {"variant": small if items else None, "items": items,
             "sigs_per_s": {str(v): {str(n): r for n, r in rs.items()} for v, rs in rates.items()}}
+
+
+def tune_lanes(ctx, torch, kind, bufs, reps: int = 10) -> dict:
+    """Two lanes per signature against one, with the tuned (small-launch)
+    variants in place: the limit is the largest SMALL_SIZES entry up to which
+    two lanes stay faster (0: never)."""
+    rates = {1: {}, 2: {}}
+    for lanes in (1, 2):
+        ctx.set_lanes(kind, lanes, 1 << 30)
+        for n in SMALL_SIZES:
+            rates[lanes][n] = time_variant(ctx, torch, kind, bufs, n, reps)[0]
+    ctx.set_lanes(kind, 1)
+    items = 0
+    for n in SMALL_SIZES:
+        if rates[2][n] > rates[1][n]:
+            items = n
+        else:
+            break
+    return {"items": items, "sigs_per_s": {str(l): {str(n): r for n, r in rs.items()} for l, rs in rates.items()}}
 
 
 def model_window(n: int) -> int:
@@ -159,9 +179,13 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
                     raise RuntimeError(f"variant {v} disagrees with variant 0 on {label}")
                 rates[v] = rate
             best = max(rates, key=rates.get)
-            res["kinds"][label] = {"sigs_per_s": {str(k): r for k, r in rates.items()}, "best": best,
-                                   "valid": int(ref.sum()), "small": tune_small(ctx, torch, kind, bufs, best)}
+            small = tune_small(ctx, torch, kind, bufs, best)
             ctx.set_variant(kind, best)
+            if small["variant"] is not None:
+                ctx.set_small_variant(kind, small["variant"], small["items"])
+            res["kinds"][label] = {"sigs_per_s": {str(k): r for k, r in rates.items()}, "best": best,
+                                   "valid": int(ref.sum()), "small": small,
+                                   "lanes": tune_lanes(ctx, torch, kind, bufs)}
         res["rlc_window"] = tune_rlc(ctx, torch)
     if write:
         path = out_path or tuning_path(name, info.compute_units)
@@ -173,6 +197,8 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
                 if k["small"]["variant"] is not None:
                     f.write(f"{label}_small_variant {k['small']['variant']}\n")
                     f.write(f"{label}_small_items {k['small']['items']}\n")
+                if k["lanes"]["items"]:
+                    f.write(f"{label}_pair_items {k['lanes']['items']}\n")
             for size, r in res["rlc_window"].items():
                 f.write(f"rlc_window_{size} {r['best']}\n")
         res["tuning_file"] = path

@@ -594,6 +594,20 @@ ufsecp_error_t ufsecp_gpu_ext_set_small_variant(ufsecp_gpu_ctx* ctx, int kind, i
     return ctx->backend->set_small_variant(kind, variant, items);
 }
 
+ufsecp_error_t ufsecp_gpu_ext_set_lanes(ufsecp_gpu_ctx* ctx, int kind, int lanes, uint32_t items) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->set_lanes(kind, lanes, items);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_get_lanes(ufsecp_gpu_ctx* ctx, int kind, int* lanes_out, uint32_t* items_out) {
+    if (!ctx || !lanes_out) return UFSECP_ERR_NULL_ARG;
+    if (kind < 0 || kind > 1) return UFSECP_ERR_BAD_INPUT;
+    const uint32_t items = ctx->backend->pair_items(kind);
+    *lanes_out = items ? 2 : 1;
+    if (items_out) *items_out = items;
+    return UFSECP_OK;
+}
+
 ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) {
     if (!ctx || !ops_per_s) return UFSECP_ERR_NULL_ARG;
     return ctx->backend->imad_peak(ops_per_s);

@@ -39,6 +39,8 @@ int env_int(const char* name, int dflt) {
 cudaError_t Backend::launch_verify(int kind, const uint8_t* m, const uint8_t* p, const uint8_t* s, uint32_t n,
                                    uint8_t* out, int collect, cudaStream_t st, size_t call_items) {
     const int k = kind & 1;
+    if (kind != 2 && call_items <= pair_items_[k])
+        return launch_verify_pair(kind, m, p, s, n, d_gtab_, out, collect, st);
     const int v = small_variant_[k] >= 0 && call_items <= small_items_[k] ? small_variant_[k] : variant_[k];
     return kLaunchers[v](kind, m, p, s, n, d_gtab_, out, collect, grid_[v][k], st);
 }
@@ -47,6 +49,14 @@ int Backend::set_variant(int kind, int v) {
     if (kind < 0 || kind > 1 || v < 0 || v >= kVerifyVariants) return set_error(kErrBadInput, "bad variant");
     variant_[kind] = v;
     small_variant_[kind] = -1;   // an explicit choice applies to every launch size
+    pair_items_[kind] = 0;
+    clear_error();
+    return kOk;
+}
+
+int Backend::set_lanes(int kind, int lanes, uint32_t items) {
+    if (kind < 0 || kind > 1 || lanes < 1 || lanes > 2) return set_error(kErrBadInput, "bad lanes");
+    pair_items_[kind] = lanes == 2 ? items : 0;
     clear_error();
     return kOk;
 }
@@ -61,7 +71,8 @@ int Backend::set_small_variant(int kind, int v, uint32_t items) {
 
 // Per-device tuning: a file of "key value" lines (ecdsa_variant,
 // schnorr_variant, their small-launch counterparts ecdsa_small_variant /
-// ecdsa_small_items and schnorr_small_variant / schnorr_small_items, and
+// ecdsa_small_items and schnorr_small_variant / schnorr_small_items, the
+// two-lane limits ecdsa_pair_items / schnorr_pair_items, and
 // rlc_window_<batch>) written by ultrafastsecp256k1_b200.autotune.  It is the
 // file named by UFSECP_B200_TUNING, else tuning/<device name>_<SMs>sm.txt
 // beside the library's lib/ directory.  UFSECP_B200_VARIANT_ECDSA / _SCHNORR
@@ -106,6 +117,8 @@ void Backend::load_tuning() {
                     small_variant_[1] = val;
                 if (!strcmp(key, "ecdsa_small_items") && val > 0) small_items_[0] = (uint32_t)val;
                 if (!strcmp(key, "schnorr_small_items") && val > 0) small_items_[1] = (uint32_t)val;
+                if (!strcmp(key, "ecdsa_pair_items") && val >= 0) pair_items_[0] = (uint32_t)val;
+                if (!strcmp(key, "schnorr_pair_items") && val >= 0) pair_items_[1] = (uint32_t)val;
                 unsigned size = 0;
                 if (sscanf(key, "rlc_window_%u", &size) == 1 && size > 0 && val >= 4 && val <= 16)
                     rlc_window_[size] = val;
@@ -117,10 +130,12 @@ void Backend::load_tuning() {
     if (ve >= 0 && ve < kVerifyVariants) {
         variant_[0] = ve;
         small_variant_[0] = -1;
+        pair_items_[0] = 0;
     }
     if (vs >= 0 && vs < kVerifyVariants) {
         variant_[1] = vs;
         small_variant_[1] = -1;
+        pair_items_[1] = 0;
     }
 }
 
@@ -240,6 +255,7 @@ int Backend::init(int device_index) {
     for (int v = 0; v < kVerifyVariants; ++v)
         for (int k = 0; k < 2; ++k) grid_[v][k] = std::max(1, kOccupancy[v](k)) * sms_;
     queue_grid_ = std::max(1, verify_queue_occupancy()) * sms_;
+    (void)verify_pair_occupancy();   // shared-memory opt-in of the two-lane kernels
     load_tuning();
     (void)cudaGetLastError();
     ready_ = true;

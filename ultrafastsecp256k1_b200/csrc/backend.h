@@ -101,6 +101,8 @@ public:
     uint32_t small_items(int kind) const { return small_items_[kind & 1]; }
     int set_variant(int kind, int v);
     int set_small_variant(int kind, int v, uint32_t items);   // v = -1: none
+    int set_lanes(int kind, int lanes, uint32_t items);       // lanes 2 for calls of <= items, 1: never
+    uint32_t pair_items(int kind) const { return pair_items_[kind & 1]; }
     int verify_grid(int kind) const { return grid_[variant_[kind & 1]][kind & 1]; }
     int blocks_per_sm(int kind, int v) const { return sms_ ? grid_[v][kind & 1] / sms_ : 0; }
 
@@ -120,6 +122,10 @@ private:
     // one; an explicit set_variant / environment override clears it.
     int small_variant_[2] = {-1, -1};
     uint32_t small_items_[2] = {0, 0};
+    // Calls of at most pair_items_[kind] items (kinds 0 and 1) run two lanes
+    // per signature (kernels_pair.cu); 0 = never.  Also cleared by an explicit
+    // variant choice.
+    uint32_t pair_items_[2] = {0, 0};
     // call_items: the size of the whole call this launch belongs to; the
     // small-launch variant is used only when the whole call is small (the
     // chunks of a large call run beside one another at full occupancy).

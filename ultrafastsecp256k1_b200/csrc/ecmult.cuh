@@ -164,6 +164,40 @@ UF_HDI void dual_mul_c(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc
     }
 }
 
+// One lane's half of R = a*G + b*P when two lanes share a signature: half 0
+// sums the a1*G and b1*P streams, half 1 the a2*(lambda G) and b2*(lambda P)
+// streams (the GLV halves), each with the full 128 doublings, so that the two
+// partial sums add up to R.  Both lanes build the same P table in their own
+// shared-memory slots (the same instruction stream, so no divergence).
+template <class Tab, class GT>
+UF_HDI void dual_mul_half(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt,
+                          int half) {
+    GlvSplit sa, sb;
+    glv_split(sa, a);
+    glv_split(sb, b);
+    uint32_t kp[4], kg[4];
+    UF_UNROLL
+    for (int i = 0; i < 4; ++i) {
+        kp[i] = half ? sb.k2[i] : sb.k1[i];
+        kg[i] = half ? sa.k2[i] : sa.k1[i];
+    }
+    const bool negp = half ? sb.neg2 : sb.neg1, negg = half ? sa.neg2 : sa.neg1;
+    int8_t dp[kNWP];
+    GDigit dg[kNWG];
+    booth_recode<kWP, kNWP>(dp, kp);
+    booth_recode<kWG, kNWG>(dg, kg);
+    build_ptable(tab, px, py);
+    Fe beta;
+    fe_beta(beta);
+    jac_set_inf(R);
+    UF_NOUNROLL
+    for (int i = kNWP - 1; i >= 0; --i) {
+        if (i != kNWP - 1) jac_dbl_n(R, kWP);
+        add_ptab(R, tab, dp[i], negp, half != 0, beta);
+        if (i % kGEvery == 0) add_gtab(R, gt, dg[i / kGEvery], negg, half);
+    }
+}
+
 template <class Tab, class GT>
 UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt) {
     dual_mul_c(R, a, px, py, b, tab, gt, false, NoPubCache(), false);

@@ -118,6 +118,13 @@ cudaError_t launch_verify_queue(const QueueArgs& a, const void* d_gtab, unsigned
                                 cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
 int verify_queue_occupancy();
 
+// Two lanes per signature (kernels_pair.cu), kind 0 ECDSA (compact) or 1
+// BIP-340, for small calls; verify_pair_occupancy() also opts the kernels in
+// to their shared memory (call once per device).
+cudaError_t launch_verify_pair(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs, uint32_t n,
+                               const void* d_gtab, uint8_t* out, int collect, cudaStream_t s);
+int verify_pair_occupancy();
+
 // Allocation-free mixed verification (kernels_noalloc.cu): jobs hold
 // device-accessible buffers; the queue head and the job table live in a
 // static device array of the library, nothing is allocated.

@@ -28,6 +28,40 @@ UF_HD bool r_below_p_minus_n(const uint32_t r[8]) {
     return lt256(r, pmn);
 }
 
+// x(R) == r or, when r + n < p, x(R) == r + n, checked projectively as
+// r Z^2 == X (ecdsa_check_xcoord, src/cpu/src/ecdsa.cpp:764); false for R = inf.
+UF_HDI bool ecdsa_check_x(const Jac& R, const Sc& r) {
+    if (R.inf) return false;
+    Fe z2, t, rf;
+    fe_sqr(z2, R.Z);
+    UF_UNROLL
+    for (int i = 0; i < 8; ++i) rf.v[i] = r.v[i];
+    fe_mul(t, rf, z2);
+    if (fe_equal(t, R.X)) return true;
+    if (!r_below_p_minus_n(r.v)) return false;
+    uint32_t n[8];
+    sc_n(n);
+    uint64_t c = 0;
+    UF_UNROLL
+    for (int i = 0; i < 8; ++i) {
+        c = (uint64_t)r.v[i] + n[i] + (c >> 32);
+        rf.v[i] = lo32(c);
+    }
+    fe_mul(t, rf, z2);
+    return fe_equal(t, R.X);
+}
+
+// BIP-340's final check: R finite, y(R) even, x(R) == r (src/cpu/src/schnorr.cpp:595-610).
+UF_HDI bool schnorr_check(const Jac& R, const uint32_t r[8]) {
+    Aff A;
+    if (!jac_to_aff(A, R)) return false;
+    if (A.y.v[0] & 1u) return false;
+    uint32_t diff = 0;
+    UF_UNROLL
+    for (int i = 0; i < 8; ++i) diff |= A.x.v[i] ^ r[i];
+    return diff == 0;
+}
+
 // ECDSA after the signature's scalars are parsed (r, s in [1, n-1]).  `cache`
 // (PubCache / NoPubCache) may supply the key's table instead of decompressing
 // the key and building it.
@@ -49,24 +83,7 @@ UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const
     sc_mul(u2, r, w);
     Jac R;
     dual_mul_c(R, u1, qx, qy, u2, tab, gt, cached, cache, prefix == 0x03);
-    if (R.inf) return false;
-    Fe z2, t, rf;
-    fe_sqr(z2, R.Z);
-    UF_UNROLL
-    for (int i = 0; i < 8; ++i) rf.v[i] = r.v[i];
-    fe_mul(t, rf, z2);
-    if (fe_equal(t, R.X)) return true;
-    if (!r_below_p_minus_n(r.v)) return false;
-    uint32_t n[8];
-    sc_n(n);
-    uint64_t c = 0;
-    UF_UNROLL
-    for (int i = 0; i < 8; ++i) {
-        c = (uint64_t)r.v[i] + n[i] + (c >> 32);
-        rf.v[i] = lo32(c);
-    }
-    fe_mul(t, rf, z2);
-    return fe_equal(t, R.X);
+    return ecdsa_check_x(R, r);
 }
 
 // msg_w / sig_w: the 32 / 64 input bytes as words loaded little-endian;
@@ -132,13 +149,7 @@ UF_HDI bool schnorr_verify_one(const uint32_t msg_w[8], const uint32_t px_w[8], 
     sc_neg(ne, e);
     Jac R;
     dual_mul_c(R, s, px, py, ne, tab, gt, cached, cache, false);
-    Aff A;
-    if (!jac_to_aff(A, R)) return false;
-    if (A.y.v[0] & 1u) return false;
-    uint32_t diff = 0;
-    UF_UNROLL
-    for (int i = 0; i < 8; ++i) diff |= A.x.v[i] ^ r[i];
-    return diff == 0;
+    return schnorr_check(R, r);
 }
 
 }  // namespace uf

@@ -49,6 +49,26 @@ def test_mixed_uneven_batches(gpu_ctx, corpora):
         assert (g == w).all()
 
 
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_queue_lanes_per_signature(gpu_ctx, corpora, lanes):
+    """Small mixed layouts run the one-lane or the two-lane queue kernels
+    (ufsecp_gpu_ext_set_lanes for both kinds); both give the oracle's verdicts
+    over every bucket shape, and switching back and forth replays no stale
+    graph."""
+    (e, s, we, ws) = corpora
+    old = [gpu_ctx.get_lanes(k) for k in (0, 1)]
+    try:
+        for k in (0, 1):
+            gpu_ctx.set_lanes(k, lanes, 1 << 16)
+        for n_e, n_s in [(1, 0), (0, 1), (17, 33), (255, 257), (1000, 3000), (6000, 6000)]:
+            jobs = [(0,) + _slice(e, 0, n_e), (1,) + _slice(s, 0, n_s)]
+            ge, gs = gpu_ctx.verify_jobs(jobs)
+            assert (ge == we[:n_e]).all() and (gs == ws[:n_s]).all()
+    finally:
+        for k in (0, 1):
+            gpu_ctx.set_lanes(k, *((2, old[k][1]) if old[k][0] == 2 else (1, 0)))
+
+
 def test_graph_buckets_replay(gpu_ctx, corpora):
     """Repeated calls hitting the same and different capacity buckets stay exact."""
     (e, s, we, ws) = corpora

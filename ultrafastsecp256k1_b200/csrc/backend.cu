@@ -255,7 +255,7 @@ int Backend::init(int device_index) {
     for (int v = 0; v < kVerifyVariants; ++v)
         for (int k = 0; k < 2; ++k) grid_[v][k] = std::max(1, kOccupancy[v](k)) * sms_;
     queue_grid_ = std::max(1, verify_queue_occupancy()) * sms_;
-    (void)verify_pair_occupancy();   // shared-memory opt-in of the two-lane kernels
+    queue_pair_grid_ = std::max(1, verify_pair_occupancy()) * sms_;   // also the two-lane kernels' shared-memory opt-in
     load_tuning();
     (void)cudaGetLastError();
     ready_ = true;

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <algorithm>
 #include <map>
 #include <memory>
 #include <string>
@@ -83,6 +84,10 @@ public:
     // else the cost model.
     int rlc_window(uint32_t len) const;
     int queue_grid() const { return queue_grid_; }
+    int queue_pair_grid() const { return queue_pair_grid_; }
+    // Mixed-job launches of at most this many items (both kinds together) run
+    // the two-lane queue kernels: the smaller of the kinds' two-lane limits.
+    uint32_t queue_pair_items() const { return std::min(pair_items_[0], pair_items_[1]); }
     // Per-item batch operations (ops.cpp): host buffers, synchronous.
     int xonly_validate(const uint8_t* keys32, size_t n, uint8_t* out);
     int pubkey_validate(const uint8_t* pubs33, size_t n, uint8_t* out);
@@ -148,6 +153,7 @@ private:
     cudaStream_t dstream_ = nullptr;
     cudaEvent_t dfork_ = nullptr, djoin_ = nullptr;
     int queue_grid_ = 0;
+    int queue_pair_grid_ = 0;
     std::unique_ptr<BatchSlot> batch_;   // slot of the synchronous mixed-batch call
     std::unique_ptr<RlcVerifier> rlc_;
     std::map<uint32_t, int> rlc_window_;   // tuned window bits per RLC batch size

@@ -80,6 +80,17 @@ int BatchSlot::init(Backend* be, bool use_graphs) {
     return kOk;
 }
 
+// Small layouts without the key cache run two lanes per signature (the
+// backend's tuned limit); the choice is part of the graph key, so a changed
+// limit never replays a graph captured with the other kernels.
+bool BatchSlot::two_lanes(const QueueArgs& a) const {
+    return !a.cache && (uint64_t)a.cap_e + a.cap_s <= be_->queue_pair_items();
+}
+
+uint64_t BatchSlot::graph_key(const QueueArgs& a) const {
+    return ((uint64_t)a.cap_e << 32) | a.cap_s | (two_lanes(a) ? (1ull << 63) : 0);
+}
+
 QueueArgs BatchSlot::args_for(uint8_t* d) const {
     QueueArgs a;
     a.counts = reinterpret_cast<const uint32_t*>(d);
@@ -103,7 +114,11 @@ int BatchSlot::run_direct(const QueueArgs& a) {
     uint8_t* h = staged_big_ ? (uint8_t*)big_pinned_.p : (uint8_t*)pinned_.p;
     uint8_t* d = staged_big_ ? (uint8_t*)big_dev_.p : (uint8_t*)dev_.p;
     cudaError_t e = cudaMemcpyAsync(d, h, layout_.in_bytes, cudaMemcpyHostToDevice, stream_);
-    if (e == cudaSuccess) e = launch_verify_queue(a, be_->gtab(), d_head_, be_->queue_grid(), stream_, stream2_, fork_, join_);
+    if (e == cudaSuccess)
+        e = two_lanes(a) ? launch_verify_queue_pair(a, be_->gtab(), d_head_, be_->queue_pair_grid(), stream_, stream2_,
+                                                    fork_, join_)
+                         : launch_verify_queue(a, be_->gtab(), d_head_, be_->queue_grid(), stream_, stream2_, fork_,
+                                               join_);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(h + layout_.e_out, d + layout_.e_out, layout_.out_bytes, cudaMemcpyDeviceToHost, stream_);
     if (e != cudaSuccess) return be_->cuda_error(e, "batch enqueue");
@@ -171,7 +186,7 @@ int BatchSlot::enqueue(const VerifyJob* jobs, size_t n_jobs) {
     uint8_t* d = staged_big_ ? (uint8_t*)big_dev_.p : (uint8_t*)dev_.p;
     const QueueArgs a = args_for(d);
     last_graph_ = graph;
-    const int rc = graph ? run_graph(a, ((uint64_t)layout_.cap_e << 32) | layout_.cap_s) : run_direct(a);
+    const int rc = graph ? run_graph(a, graph_key(a)) : run_direct(a);
     if (rc != kOk) return rc;
     if ((e = cudaEventRecord(done_, stream_)) != cudaSuccess) return be_->cuda_error(e, "event record");
     return kOk;
@@ -191,7 +206,8 @@ int BatchSlot::prewarm(uint32_t max_items) {
             uint32_t* hdr = reinterpret_cast<uint32_t*>(pinned_.p);
             hdr[0] = 0;
             hdr[1] = 0;
-            const int rc = run_graph(args_for((uint8_t*)dev_.p), ((uint64_t)ce << 32) | cs);
+            const QueueArgs a = args_for((uint8_t*)dev_.p);
+            const int rc = run_graph(a, graph_key(a));
             if (rc != kOk) return rc;
         }
     }

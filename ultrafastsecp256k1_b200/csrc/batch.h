@@ -71,6 +71,8 @@ public:
 
 private:
     int run_direct(const QueueArgs& a);
+    bool two_lanes(const QueueArgs& a) const;
+    uint64_t graph_key(const QueueArgs& a) const;
     int run_graph(const QueueArgs& a, uint64_t key);
     QueueArgs args_for(uint8_t* dev_base) const;
 

@@ -124,6 +124,10 @@ int verify_queue_occupancy();
 cudaError_t launch_verify_pair(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs, uint32_t n,
                                const void* d_gtab, uint8_t* out, int collect, cudaStream_t s);
 int verify_pair_occupancy();
+// The work-queue form of the two-lane kernels (no key cache), same contract as
+// launch_verify_queue; `grid` from verify_pair_occupancy().
+cudaError_t launch_verify_queue_pair(const QueueArgs& a, const void* d_gtab, unsigned int* d_head, int grid,
+                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
 
 // Allocation-free mixed verification (kernels_noalloc.cu): jobs hold
 // device-accessible buffers; the queue head and the job table live in a

@@ -79,7 +79,8 @@ def test_graph_buckets_replay(gpu_ctx, corpora):
 
 
 def test_direct_path_large(gpu_ctx, oracle):
-    """Above the graph capacity (65,536 per kind) the same sequence runs directly."""
+    """A call above 65,536 items is cut into sub-calls on two batch slots (a
+    job split across them keeps its verdicts in place)."""
     base = 4096
     m, x, s = schnorr_corpus(oracle, base, seed=83, tamper=0.1)
     w = oracle.schnorr_verify_batch(m, x, s)
@@ -89,6 +90,29 @@ def test_direct_path_large(gpu_ctx, oracle):
     we = oracle.ecdsa_verify_batch(me, pe, se)
     gs, ge = gpu_ctx.verify_jobs([big, (0, me, pe, se)])
     assert (gs == np.tile(w, reps)).all() and (ge == we).all()
+
+
+def test_large_call_many_subcalls(gpu_ctx, oracle):
+    """Large jobs of both kinds and small ones between them, over more than two
+    65,536-item sub-calls (each slot reused), keep every verdict in place."""
+    base = 2048
+    m, x, s = schnorr_corpus(oracle, base, seed=85, tamper=0.1)
+    ws = oracle.schnorr_verify_batch(m, x, s)
+    me, pe, se = ecdsa_corpus(oracle, base, seed=86, tamper=0.1)
+    we = oracle.ecdsa_verify_batch(me, pe, se)
+    tile = lambda a, n: np.ascontiguousarray(np.tile(a, (-(-n // base), 1))[:n])
+    sizes = [(0, 40_000), (1, 70_001), (0, 3), (1, 0), (0, 30_001), (1, 65_536), (0, 1), (1, 17)]
+    jobs, want = [], []
+    for kind, n in sizes:
+        if kind == 0:
+            jobs.append((0, tile(me, n), tile(pe, n), tile(se, n)))
+            want.append(np.tile(we, -(-n // base) if n else 1)[:n])
+        else:
+            jobs.append((1, tile(m, n), tile(x, n), tile(s, n)))
+            want.append(np.tile(ws, -(-n // base) if n else 1)[:n])
+    got = gpu_ctx.verify_jobs(jobs)
+    for g, w in zip(got, want):
+        assert g.shape == w.shape and (g == w).all()
 
 
 def test_same_verdicts_as_plain_calls(gpu_ctx, corpora):

@@ -4,6 +4,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <vector>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -19,6 +20,7 @@ namespace {
 // Items per host->device chunk: bounds device memory at ~130 B x 2^22 = 0.5 GB.
 constexpr size_t kPipeChunk = size_t{1} << 17;   // items per staging slot of a host-buffer call
 constexpr size_t kPipeFirst = size_t{1} << 14;   // items in a host-buffer call's first chunk
+constexpr size_t kJobsPipeItems = size_t{1} << 16;   // items per sub-call of a large mixed-job call
 constexpr size_t kDeviceChunk = size_t{1} << 17; // items per launch of a large device-buffer call
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
@@ -184,7 +186,8 @@ RlcVerifier& Backend::rlc() {
 }
 
 Backend::~Backend() {
-    batch_.reset();
+    batch_[0].reset();
+    batch_[1].reset();
     if (dev_ >= 0) cudaSetDevice(dev_);
     rlc_.reset();
     if (dev_ >= 0) {
@@ -407,14 +410,65 @@ int Backend::sign_device(int kind, const uint8_t* d_msgs, const uint8_t* d_sks, 
 
 int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
     if (!ready_) return set_error(kErrGpuDevice, "context not ready");
-    if (!batch_) {
-        auto slot = std::make_unique<BatchSlot>();
-        const int rc = slot->init(this);
-        if (rc != kOk) return rc;
-        batch_ = std::move(slot);
+    for (int q = 0; q < 2; ++q) {
+        if (!batch_[q]) {
+            auto slot = std::make_unique<BatchSlot>();
+            const int rc = slot->init(this);
+            if (rc != kOk) return rc;
+            batch_[q] = std::move(slot);
+        }
+        if (q == 0) {
+            size_t total = 0;
+            for (size_t j = 0; j < n_jobs; ++j) total += jobs[j].count;
+            if (total <= kJobsPipeItems) {
+                int rc = batch_[0]->enqueue(jobs, n_jobs);
+                if (rc == kOk) rc = batch_[0]->finish(jobs, n_jobs);
+                if (rc == kOk) clear_error();
+                return rc;
+            }
+        }
     }
-    int rc = batch_->enqueue(jobs, n_jobs);
-    if (rc == kOk) rc = batch_->finish(jobs, n_jobs);
+    // A large call: sub-calls of at most kJobsPipeItems items (jobs cut at the
+    // boundaries; verdicts are per item) alternate between the two slots, so
+    // the CPU packs sub-call k + 1 while the device verifies sub-call k.
+    std::vector<VerifyJob> part[2];
+    bool pending[2] = {false, false};
+    int rc = kOk;
+    size_t j = 0, off = 0;
+    for (int k = 0; j < n_jobs && rc == kOk; ++k) {
+        const int q = k & 1;
+        if (pending[q]) {
+            pending[q] = false;
+            if ((rc = batch_[q]->finish(part[q].data(), part[q].size())) != kOk) break;
+        }
+        part[q].clear();
+        size_t n = 0;
+        while (j < n_jobs && n < kJobsPipeItems) {
+            const VerifyJob& J = jobs[j];
+            if (off >= J.count) {
+                ++j;
+                off = 0;
+                continue;
+            }
+            const size_t take = std::min(J.count - off, kJobsPipeItems - n);
+            VerifyJob P = J;
+            P.count = take;
+            P.msgs = J.msgs + 32 * off;
+            P.pubs = J.pubs + (J.kind == 0 ? 33 : 32) * off;
+            P.sigs = J.sigs + 64 * off;
+            P.out = J.out + off;
+            part[q].push_back(P);
+            n += take;
+            off += take;
+        }
+        if (part[q].empty()) break;
+        if ((rc = batch_[q]->enqueue(part[q].data(), part[q].size())) == kOk) pending[q] = true;
+    }
+    for (int q = 0; q < 2; ++q) {
+        if (!pending[q]) continue;
+        const int r = batch_[q]->finish(part[q].data(), part[q].size());
+        if (rc == kOk) rc = r;
+    }
     if (rc == kOk) clear_error();
     return rc;
 }

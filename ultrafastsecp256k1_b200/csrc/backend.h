@@ -154,7 +154,7 @@ private:
     cudaEvent_t dfork_ = nullptr, djoin_ = nullptr;
     int queue_grid_ = 0;
     int queue_pair_grid_ = 0;
-    std::unique_ptr<BatchSlot> batch_;   // slot of the synchronous mixed-batch call
+    std::unique_ptr<BatchSlot> batch_[2];   // slots of the synchronous mixed-batch call (two for large calls)
     std::unique_ptr<RlcVerifier> rlc_;
     std::map<uint32_t, int> rlc_window_;   // tuned window bits per RLC batch size
     int last_err_ = kOk;

@@ -155,18 +155,24 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     return L
 
 
-def _buf(x, n_bytes: int, name: str) -> np.ndarray:
+def _u8(x) -> np.ndarray:
+    """x as a flat contiguous uint8 array (no copy when it already is one)."""
+    if isinstance(x, np.ndarray) and x.dtype == np.uint8 and x.flags.c_contiguous:
+        return x.reshape(-1)
     if isinstance(x, (bytes, bytearray, memoryview)):
-        a = np.frombuffer(bytes(x), dtype=np.uint8)
-    else:
-        a = np.ascontiguousarray(np.asarray(x, dtype=np.uint8)).reshape(-1)
+        return np.frombuffer(bytes(x), dtype=np.uint8)
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint8)).reshape(-1)
+
+
+def _buf(x, n_bytes: int, name: str) -> np.ndarray:
+    a = _u8(x)
     if a.size != n_bytes:
         raise ValueError(f"{name}: expected {n_bytes} bytes, got {a.size}")
     return a
 
 
 def _ptr(a: np.ndarray) -> int:
-    return a.ctypes.data
+    return a.__array_interface__["data"][0]
 
 
 def backend_count() -> int:
@@ -275,17 +281,19 @@ class GpuContext:
     def verify_jobs(self, jobs):
         """ufsecp_gpu_ext_verify_jobs: jobs = [(kind, msgs, pubs, sigs), ...] with kind 0
         ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys); returns one verdict array per job."""
-        keep, arr, outs = [], (Job * max(1, len(jobs)))(), []
-        for k, (kind, msgs, pubs, sigs) in enumerate(jobs):
-            m = np.ascontiguousarray(np.asarray(msgs, np.uint8)).reshape(-1)
-            n = m.size // 32
+        keep, arr = [], (Job * max(1, len(jobs)))()
+        msgs_l = [_u8(j[1]) for j in jobs]
+        counts = [m.size // 32 for m in msgs_l]
+        out_all = np.zeros(max(1, sum(counts)), np.uint8)     # one verdict buffer, one view per job
+        o_base, off, outs = _ptr(out_all), 0, []
+        for k, ((kind, _, pubs, sigs), m, n) in enumerate(zip(jobs, msgs_l, counts)):
             p = _buf(pubs, (33 if kind == 0 else 32) * n, "pubkeys")
             s = _buf(sigs, 64 * n, "sigs64")
-            o = np.zeros(n, np.uint8)
             keep += [m, p, s]
-            outs.append(o)
+            outs.append(out_all[off:off + n])
             arr[k] = Job(kind, 0, n, _ptr(m) if n else None, _ptr(p) if n else None, _ptr(s) if n else None,
-                         _ptr(o) if n else None)
+                         o_base + off if n else None)
+            off += n
         self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, arr, len(jobs)), "verify_jobs")
         return outs
 

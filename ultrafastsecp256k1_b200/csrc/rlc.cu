@@ -249,15 +249,20 @@ k_rlc_tsum(RoundGeo g, const uint32_t* __restrict__ tsc, const uint8_t* __restri
 // One thread per (point, window): pass 0 counts the non-zero digits of every
 // bucket key, pass 1 writes entry = point index | sign << 31 at the bucket's
 // cursor.  Key = (segment * W + window) * B + |digit| - 1.
+// One thread per point of the round: its segment (one search), magnitude and
+// sign are read once and all W of its c-bit digits go to their buckets.
+// pass 0 counts entries per (segment, window, |digit|) key, pass 1 writes
+// them at the scanned offsets (order within a bucket is arbitrary: bucket sums
+// do not depend on it).
 __global__ void __launch_bounds__(256)
 k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint4* __restrict__ segmag,
              const uint8_t* __restrict__ segneg, uint32_t total, uint32_t* __restrict__ counts,
              uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries, int pass) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const uint32_t s = upper_index(g.pwf, g.n_seg, t);
-    const uint32_t local = t - g.pwf[s];
-    const uint32_t p = local / (uint32_t)g.W, w = local - p * (uint32_t)g.W;
+    const uint32_t W = (uint32_t)g.W;
+    const uint32_t tp = blockIdx.x * blockDim.x + threadIdx.x;     // point of the round
+    if (tp >= total / W) return;
+    const uint32_t s = upper_index(g.pwf, g.n_seg, tp * W);
+    const uint32_t p = tp - g.pwf[s] / W;
     const uint32_t len = g.seg[2 * s + 1];
     uint32_t pidx;
     uint4 m;
@@ -271,14 +276,17 @@ k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint4* __restrict
         m = segmag[j];
         neg = segneg[j] != 0;
     }
-    const int d = booth_digit(m, (int)w, g.c);
-    if (d == 0) return;
-    const uint32_t key = (s * (uint32_t)g.W + w) * (uint32_t)g.B + (uint32_t)((d < 0 ? -d : d) - 1);
-    if (pass == 0) {
-        atomicAdd(&counts[key], 1u);
-    } else {
-        const uint32_t pos = atomicAdd(&cursor[key], 1u);
-        entries[pos] = pidx | (((d < 0) != neg) ? 0x80000000u : 0u);
+    const uint32_t key0 = s * W * (uint32_t)g.B;
+    for (uint32_t w = 0; w < W; ++w) {
+        const int d = booth_digit(m, (int)w, g.c);
+        if (d == 0) continue;
+        const uint32_t key = key0 + w * (uint32_t)g.B + (uint32_t)((d < 0 ? -d : d) - 1);
+        if (pass == 0) {
+            atomicAdd(&counts[key], 1u);
+        } else {
+            const uint32_t pos = atomicAdd(&cursor[key], 1u);
+            entries[pos] = pidx | (((d < 0) != neg) ? 0x80000000u : 0u);
+        }
     }
 }
 
@@ -587,13 +595,13 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC round set-up");
     k_rlc_tsum<<<n_seg, 256, 0, s>>>(g, (const uint32_t*)tsc_.p, (const uint8_t*)okb_.p, (uint4*)segmag_.p,
                                      (uint8_t*)segneg_.p, (uint32_t*)segbad_.p);
-    k_rlc_digits<<<grid_for(total, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
+    k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
                                                      (uint32_t)total, counts, nullptr, nullptr, 0);
     size_t tb = scan_tmp_.cap;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, counts, offsets, (int)(K + 1), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(cursor, offsets, K * 4, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC scan");
-    k_rlc_digits<<<grid_for(total, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
+    k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
                                                      (uint32_t)total, nullptr, cursor, (uint32_t*)entries_.p, 1);
     k_rlc_nchunks<<<grid_for(K + 1, 256), 256, 0, s>>>(counts, (uint32_t)K, nch);
     tb = scan_tmp_.cap;

@@ -244,6 +244,15 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_lanes(ufsecp_gpu_ctx* ctx, int kind
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_lanes(ufsecp_gpu_ctx* ctx, int kind, int* lanes_out,
                                                    uint32_t* items_out);
 
+/* RLC bucket chunk: the number of bucket points one thread sums before the
+ * per-bucket merge.  The tuning file sets it per batch size (rlc_chunk_<n>;
+ * the nearest tuned size in log scale applies, else 16).  set: 2..256 fixes it
+ * for every segment length, 0 restores the tuned values (the environment
+ * variable UFSECP_B200_RLC_CHUNK sets the same override at context creation).
+ * get: the chunk a segment of `len` items uses.  Verdicts do not depend on it. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_rlc_chunk(ufsecp_gpu_ctx* ctx, uint32_t chunk);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_rlc_chunk(ufsecp_gpu_ctx* ctx, uint32_t len, uint32_t* chunk_out);
+
 /* Measured 32-bit integer multiply-add issue rate of the device (ops / s):
  * every thread of a full grid runs 16 independent mad.lo.u32 chains. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s);

@@ -136,6 +136,34 @@ def test_rlc_repeated_items(gpu_ctx, oracle):
     assert (out == want).all()
 
 
+@pytest.mark.parametrize("chunk", [2, 3, 7, 16, 256])
+def test_rlc_chunk_sizes(gpu_ctx, oracle, chunk):
+    """Any bucket chunk (one point per thread up to whole buckets) gives the same verdicts."""
+    m, x, s = schnorr_corpus(oracle, 60, seed=82, tamper=0.0)
+    _flip(m, 11)
+    idx = np.array([i % 60 for i in range(1500)] + [3] * 200)
+    m, x, s = m[idx].copy(), x[idx].copy(), s[idx].copy()
+    want = oracle.schnorr_verify_batch(m, x, s)
+    tuned = gpu_ctx.get_rlc_chunk(4096)
+    gpu_ctx.set_rlc_chunk(chunk)
+    try:
+        assert gpu_ctx.get_rlc_chunk(4096) == chunk and gpu_ctx.get_rlc_chunk(64) == chunk
+        for wbits in (4, 0):
+            for bs in (0, 256):
+                out, bok = gpu_ctx.schnorr_verify_rlc(m, x, s, batch_size=bs, seed32=SEED, window_bits=wbits)
+                assert (out == want).all(), (wbits, bs)
+    finally:
+        gpu_ctx.set_rlc_chunk(0)
+    assert gpu_ctx.get_rlc_chunk(4096) == tuned
+
+
+def test_rlc_chunk_bounds(gpu_ctx):
+    for bad in (1, 257):
+        with pytest.raises(uf.UfsecpError):
+            gpu_ctx.set_rlc_chunk(bad)
+    assert 2 <= gpu_ctx.get_rlc_chunk(4096) <= 256
+
+
 def test_rlc_seed_does_not_change_verdicts(gpu_ctx, oracle):
     m, x, s = schnorr_corpus(oracle, 3000, seed=81, tamper=0.003)
     want = oracle.schnorr_verify_batch(m, x, s)

@@ -113,6 +113,8 @@ _SIGS = {
     "ufsecp_gpu_ext_set_lanes": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32]),
     "ufsecp_gpu_ext_get_lanes": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_uint32)]),
+    "ufsecp_gpu_ext_set_rlc_chunk": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_get_rlc_chunk": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     "ufsecp_gpu_ext_imad_peak": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "ufsecp_gpu_ext_diag": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_probe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -403,6 +405,16 @@ class GpuContext:
         l, n = ctypes.c_int(), ctypes.c_uint32()
         self._check(self.L.ufsecp_gpu_ext_get_lanes(self._ctx, kind, ctypes.byref(l), ctypes.byref(n)), "get_lanes")
         return l.value, n.value
+
+    def set_rlc_chunk(self, chunk: int) -> None:
+        """Bucket points per RLC chunk thread for every segment (2..256); 0 restores the tuned values."""
+        self._check(self.L.ufsecp_gpu_ext_set_rlc_chunk(self._ctx, chunk), "set_rlc_chunk")
+
+    def get_rlc_chunk(self, length: int) -> int:
+        """Bucket points per RLC chunk thread for a segment of `length` items."""
+        v = ctypes.c_uint32()
+        self._check(self.L.ufsecp_gpu_ext_get_rlc_chunk(self._ctx, length, ctypes.byref(v)), "get_rlc_chunk")
+        return v.value
 
     def set_small_variant(self, kind: int, variant: int, items: int = 0) -> None:
         """Launches of at most `items` items use `variant` (-1: none)."""

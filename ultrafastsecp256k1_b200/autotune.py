@@ -161,6 +161,41 @@ def tune_rlc(ctx, torch, total: int = 1 << 18, reps: int = 2) -> dict:
     return res
 
 
+RLC_CHUNKS = (4, 6, 8, 12, 16, 24, 32)
+
+
+def tune_rlc_chunk(ctx, torch, windows: dict, total: int = 1 << 18, reps: int = 2) -> dict:
+    """Bucket points per chunk thread per RLC batch size, at the tuned window."""
+    import time
+    d_m, d_p, d_s = signed_batch(ctx, torch, 1, total, seed=92)
+    d_s.view(total, 64)[::50, 40] ^= 0x04        # an all-valid corpus
+    torch.cuda.synchronize()
+    out = torch.zeros(total, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    res = {}
+    try:
+        for size in RLC_SIZES:
+            c = windows[str(size)]["best"]
+            rates = {}
+            for chunk in RLC_CHUNKS:
+                ctx.set_rlc_chunk(chunk)
+                call = lambda: ctx.schnorr_verify_rlc_device(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), total,
+                                                             out.data_ptr(), batch_size=size, seed32=bytes(32),
+                                                             window_bits=c, stream=st.cuda_stream)
+                call()
+                t0 = time.perf_counter()
+                for _ in range(reps):
+                    call()
+                rates[chunk] = total * reps / (time.perf_counter() - t0)
+                if not bool(out.all()):
+                    raise RuntimeError("RLC rejected a valid corpus while tuning the chunk")
+            best = max(rates, key=rates.get)
+            res[str(size)] = {"best": best, "sigs_per_s": {str(k): v for k, v in rates.items()}}
+    finally:
+        ctx.set_rlc_chunk(0)
+    return res
+
+
 def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = True) -> dict:
     import torch
     info = uf.device_info(0)
@@ -187,6 +222,7 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
                                    "valid": int(ref.sum()), "small": small,
                                    "lanes": tune_lanes(ctx, torch, kind, bufs)}
         res["rlc_window"] = tune_rlc(ctx, torch)
+        res["rlc_chunk"] = tune_rlc_chunk(ctx, torch, res["rlc_window"])
     if write:
         path = out_path or tuning_path(name, info.compute_units)
         os.makedirs(os.path.dirname(path), exist_ok=True)
@@ -201,6 +237,8 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
                     f.write(f"{label}_pair_items {k['lanes']['items']}\n")
             for size, r in res["rlc_window"].items():
                 f.write(f"rlc_window_{size} {r['best']}\n")
+            for size, r in res["rlc_chunk"].items():
+                f.write(f"rlc_chunk_{size} {r['best']}\n")
         res["tuning_file"] = path
     return res
 

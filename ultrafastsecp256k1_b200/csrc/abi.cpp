@@ -608,6 +608,17 @@ ufsecp_error_t ufsecp_gpu_ext_get_lanes(ufsecp_gpu_ctx* ctx, int kind, int* lane
     return UFSECP_OK;
 }
 
+ufsecp_error_t ufsecp_gpu_ext_set_rlc_chunk(ufsecp_gpu_ctx* ctx, uint32_t chunk) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->set_rlc_chunk(chunk);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_get_rlc_chunk(ufsecp_gpu_ctx* ctx, uint32_t len, uint32_t* chunk_out) {
+    if (!ctx || !chunk_out) return UFSECP_ERR_NULL_ARG;
+    *chunk_out = ctx->backend->rlc_chunk(len);
+    return UFSECP_OK;
+}
+
 ufsecp_error_t ufsecp_gpu_ext_imad_peak(ufsecp_gpu_ctx* ctx, double* ops_per_s) {
     if (!ctx || !ops_per_s) return UFSECP_ERR_NULL_ARG;
     return ctx->backend->imad_peak(ops_per_s);

@@ -124,10 +124,14 @@ void Backend::load_tuning() {
                 unsigned size = 0;
                 if (sscanf(key, "rlc_window_%u", &size) == 1 && size > 0 && val >= 4 && val <= 16)
                     rlc_window_[size] = val;
+                if (sscanf(key, "rlc_chunk_%u", &size) == 1 && size > 0 && val >= 2 && val <= 256)
+                    rlc_chunk_[size] = (uint32_t)val;
             }
             fclose(f);
         }
     }
+    const int rc_env = env_int("UFSECP_B200_RLC_CHUNK", 0);
+    if (rc_env >= 2 && rc_env <= 256) rlc_chunk_fixed_ = (uint32_t)rc_env;
     const int ve = env_int("UFSECP_B200_VARIANT_ECDSA", -1), vs = env_int("UFSECP_B200_VARIANT_SCHNORR", -1);
     if (ve >= 0 && ve < kVerifyVariants) {
         variant_[0] = ve;
@@ -178,6 +182,28 @@ int Backend::rlc_window(uint32_t len) const {
         }
     }
     return best;
+}
+
+uint32_t Backend::rlc_chunk(uint32_t len) const {
+    // a fixed override, else the tuned batch size nearest in log scale
+    if (rlc_chunk_fixed_) return rlc_chunk_fixed_;
+    if (rlc_chunk_.empty() || len == 0) return RlcVerifier::kChunk;
+    uint32_t best = RlcVerifier::kChunk;
+    double dist = 1e300;
+    for (const auto& kv : rlc_chunk_) {
+        const double d = fabs(log2((double)kv.first) - log2((double)len));
+        if (d < dist) {
+            dist = d;
+            best = kv.second;
+        }
+    }
+    return best;
+}
+
+int Backend::set_rlc_chunk(uint32_t chunk) {
+    if (chunk != 0 && (chunk < 2 || chunk > 256)) return set_error(kErrBadInput, "RLC chunk must be 0 or 2..256");
+    rlc_chunk_fixed_ = chunk;
+    return kOk;
 }
 
 RlcVerifier& Backend::rlc() {

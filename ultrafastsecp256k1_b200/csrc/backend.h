@@ -83,6 +83,12 @@ public:
     // of the nearest tuned batch size (tuning file lines "rlc_window_<n> <c>"),
     // else the cost model.
     int rlc_window(uint32_t len) const;
+    // Bucket points summed by one RLC chunk thread for segments of `len`
+    // items: the fixed override if set, else the value of the nearest tuned
+    // batch size (tuning file lines "rlc_chunk_<n> <points>"), else 16.
+    uint32_t rlc_chunk(uint32_t len) const;
+    // 2..256 fixes the chunk for every segment length; 0 restores the tuned values.
+    int set_rlc_chunk(uint32_t chunk);
     int queue_grid() const { return queue_grid_; }
     int queue_pair_grid() const { return queue_pair_grid_; }
     // Mixed-job launches of at most this many items (both kinds together) run
@@ -157,6 +163,8 @@ private:
     std::unique_ptr<BatchSlot> batch_[2];   // slots of the synchronous mixed-batch call (two for large calls)
     std::unique_ptr<RlcVerifier> rlc_;
     std::map<uint32_t, int> rlc_window_;   // tuned window bits per RLC batch size
+    std::map<uint32_t, uint32_t> rlc_chunk_;  // tuned bucket points per chunk thread per RLC batch size
+    uint32_t rlc_chunk_fixed_ = 0;            // set_rlc_chunk / UFSECP_B200_RLC_CHUNK override, 0 = tuned
     int last_err_ = kOk;
     std::string last_msg_ = "OK";
 };

@@ -5,7 +5,7 @@
 // c-bit windows (W = ceil(129 / c) windows, B = 2^(c-1) buckets per window):
 // one 4-byte entry per non-zero digit (at most (3 len + 2) W per segment),
 // counters and offsets over the K = S W B bucket keys, a Jacobian sum (112 B)
-// per bucket and per chunk of kChunk entries, two per bucket sub-range and one
+// per bucket and per chunk of chunk() entries, two per bucket sub-range and one
 // per window.
 #include "rlc.h"
 
@@ -291,24 +291,25 @@ k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint4* __restrict
 }
 
 // chunks per key, for the chunk scan; nch[K] = 0
-__global__ void k_rlc_nchunks(const uint32_t* __restrict__ counts, uint32_t K, uint32_t* __restrict__ nch) {
+__global__ void k_rlc_nchunks(const uint32_t* __restrict__ counts, uint32_t K, uint32_t chunk,
+                              uint32_t* __restrict__ nch) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < K) nch[k] = (counts[k] + RlcVerifier::kChunk - 1) / RlcVerifier::kChunk;
+    if (k < K) nch[k] = (counts[k] + chunk - 1) / chunk;
     else if (k == K) nch[k] = 0;
 }
 
-// One thread per chunk of at most kChunk entries of one bucket.  A bucket
+// One thread per chunk of at most `chunk` entries of one bucket.  A bucket
 // with a single chunk is written straight to its bucket slot.
 __global__ void __launch_bounds__(128)
-k_rlc_chunks(const uint32_t* __restrict__ coff, uint32_t K, const uint32_t* __restrict__ offsets,
+k_rlc_chunks(const uint32_t* __restrict__ coff, uint32_t K, uint32_t chunk, const uint32_t* __restrict__ offsets,
              const uint32_t* __restrict__ entries, const RlcItem* __restrict__ items, uint32_t n3,
              const uint4* __restrict__ gt, uint4* __restrict__ partials, uint4* __restrict__ buckets) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= coff[K]) return;
     const uint32_t key = upper_index(coff, K, t);
     const uint32_t j = t - coff[key];
-    const uint32_t e0 = offsets[key] + j * RlcVerifier::kChunk;
-    const uint32_t e1 = min(e0 + RlcVerifier::kChunk, offsets[key + 1]);
+    const uint32_t e0 = offsets[key] + j * chunk;
+    const uint32_t e1 = min(e0 + chunk, offsets[key + 1]);
     Jac acc;
     jac_set_inf(acc);
     for (uint32_t e = e0; e < e1; ++e) {
@@ -563,7 +564,10 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     host[3 * (size_t)n_seg] = (uint32_t)total;
     const uint64_t K = (uint64_t)n_seg * W * B;
     if (K >= 0x7FFFFFFFull) return be_->set_error(kErrBadInput, "RLC round too large");
-    const uint64_t chunk_cap = total / kChunk + K + 1;
+    uint32_t maxlen = 0;
+    for (uint32_t k = 0; k < n_seg; ++k) maxlen = std::max(maxlen, seg[2 * k + 1]);
+    const uint32_t chunk = be_->rlc_chunk(maxlen);
+    const uint64_t chunk_cap = total / chunk + K + 1;
     size_t scan_bytes = 0;
     cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
                                                   (int)(K + 1), s);
@@ -603,11 +607,11 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC scan");
     k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
                                                      (uint32_t)total, nullptr, cursor, (uint32_t*)entries_.p, 1);
-    k_rlc_nchunks<<<grid_for(K + 1, 256), 256, 0, s>>>(counts, (uint32_t)K, nch);
+    k_rlc_nchunks<<<grid_for(K + 1, 256), 256, 0, s>>>(counts, (uint32_t)K, chunk, nch);
     tb = scan_tmp_.cap;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, nch, coff, (int)(K + 1), s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC chunk scan");
-    k_rlc_chunks<<<grid_for(chunk_cap, 128), 128, 0, s>>>(coff, (uint32_t)K, offsets, (const uint32_t*)entries_.p,
+    k_rlc_chunks<<<grid_for(chunk_cap, 128), 128, 0, s>>>(coff, (uint32_t)K, chunk, offsets, (const uint32_t*)entries_.p,
                                                           (const RlcItem*)items_.p, 3u * n_,
                                                           (const uint4*)be_->gtab(), (uint4*)partials_.p,
                                                           (uint4*)buckets_.p);

@@ -18,8 +18,9 @@
 //    -sum a_i s_i), every scalar below 2^128;
 //  * signed c-bit windows: a counting sort places every (point, window) with a
 //    non-zero digit into bucket (segment, window, |digit|); each bucket is
-//    summed in chunks of kChunk points, each window reduced by running sums
-//    over sub-ranges of buckets, windows combined by Horner's rule;
+//    summed in chunks of a tuned number of points (16 by default), each
+//    window reduced by running sums over sub-ranges of buckets, windows
+//    combined by Horner's rule;
 //  * a failing segment is split into kFanout near-equal children, all checked
 //    again in the next round (the per-item data is computed once; eight-way
 //    splits need half the rounds of halving and less MSM work in total: about
@@ -47,11 +48,12 @@ struct RlcStats {
 class RlcVerifier {
 public:
     static constexpr uint32_t kLeaf = 32;      // segments this small are verified per signature
-    static constexpr uint32_t kChunk = 16;     // bucket points summed by one thread
+    static constexpr uint32_t kChunk = 16;     // default bucket points summed by one thread
     static constexpr uint32_t kFanout = 8;     // children of a failing segment
     static constexpr uint32_t kMaxItems = 1u << 24;
 
     explicit RlcVerifier(Backend* be) : be_(be) {}
+
     ~RlcVerifier();
 
     // Device-resident BIP-340 items (32-byte messages, 32-byte x-only keys,

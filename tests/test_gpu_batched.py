@@ -115,6 +115,16 @@ def test_large_call_many_subcalls(gpu_ctx, oracle):
         assert g.shape == w.shape and (g == w).all()
 
 
+def test_jobs_buffer_forms(gpu_ctx, corpora):
+    """Jobs given as read-only arrays, bytes, 2-D arrays and lists verify like flat arrays."""
+    (e, s, we, ws) = corpora
+    ro = [np.frombuffer(a.tobytes(), np.uint8) for a in e]
+    jobs = [(0,) + tuple(ro), (1, bytes(s[0]), bytearray(s[1]), s[2].reshape(-1, 64)),
+            (1, s[0][:3].tolist(), s[1][:3], s[2][:3]), (0, e[0][:0], e[1][:0], e[2][:0])]
+    got = gpu_ctx.verify_jobs(jobs)
+    assert (got[0] == we).all() and (got[1] == ws).all() and (got[2] == ws[:3]).all() and got[3].size == 0
+
+
 def test_same_verdicts_as_plain_calls(gpu_ctx, corpora):
     (e, s, we, ws) = corpora
     ge, gs = gpu_ctx.verify_jobs([(0,) + e, (1,) + s])

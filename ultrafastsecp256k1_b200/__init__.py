@@ -157,6 +157,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     return L
 
 
+_U8 = np.dtype(np.uint8)
+# ufsecp_gpu_ext_job_t as a numpy record (the Job structure's layout, 48 bytes)
+_JOB_DTYPE = np.dtype([("kind", "<u4"), ("reserved", "<u4"), ("count", "<u8"), ("msg_hashes32", "<u8"),
+                       ("pubkeys", "<u8"), ("sigs64", "<u8"), ("out_results", "<u8")])
+assert _JOB_DTYPE.itemsize == ctypes.sizeof(Job)
+
+
 def _u8(x) -> np.ndarray:
     """x as a flat contiguous uint8 array (no copy when it already is one)."""
     if isinstance(x, np.ndarray) and x.dtype == np.uint8 and x.flags.c_contiguous:
@@ -175,6 +182,18 @@ def _buf(x, n_bytes: int, name: str) -> np.ndarray:
 
 def _ptr(a: np.ndarray) -> int:
     return a.__array_interface__["data"][0]
+
+
+_CCHAR = ctypes.c_char
+
+
+def _addr(a: np.ndarray) -> int:
+    """Address of a non-empty contiguous array: through the buffer protocol
+    (a third of __array_interface__'s cost), read-only arrays through _ptr."""
+    try:
+        return ctypes.addressof(_CCHAR.from_buffer(a))
+    except (TypeError, ValueError):
+        return _ptr(a)
 
 
 def backend_count() -> int:
@@ -282,22 +301,37 @@ class GpuContext:
     # ---- ufsecp_gpu_ext.h -------------------------------------------------------
     def verify_jobs(self, jobs):
         """ufsecp_gpu_ext_verify_jobs: jobs = [(kind, msgs, pubs, sigs), ...] with kind 0
-        ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys); returns one verdict array per job."""
-        keep, arr = [], (Job * max(1, len(jobs)))()
-        msgs_l = [_u8(j[1]) for j in jobs]
-        counts = [m.size // 32 for m in msgs_l]
-        out_all = np.zeros(max(1, sum(counts)), np.uint8)     # one verdict buffer, one view per job
-        o_base, off, outs = _ptr(out_all), 0, []
-        for k, ((kind, _, pubs, sigs), m, n) in enumerate(zip(jobs, msgs_l, counts)):
-            p = _buf(pubs, (33 if kind == 0 else 32) * n, "pubkeys")
-            s = _buf(sigs, 64 * n, "sigs64")
-            keep += [m, p, s]
-            outs.append(out_all[off:off + n])
-            arr[k] = Job(kind, 0, n, _ptr(m) if n else None, _ptr(p) if n else None, _ptr(s) if n else None,
-                         o_base + off if n else None)
-            off += n
-        self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, arr, len(jobs)), "verify_jobs")
-        return outs
+        ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys); returns one verdict array per job.
+        The job table is one numpy record array laid out as ufsecp_gpu_ext_job_t
+        (the per-job Python work is little more than the three buffer addresses)."""
+        nj = len(jobs)
+        keep, meta = [], []
+        total = 0
+        for kind, m, p, s in jobs:
+            if not (type(m) is np.ndarray and m.dtype is _U8 and m.flags.c_contiguous):
+                m = _u8(m)
+            if not (type(p) is np.ndarray and p.dtype is _U8 and p.flags.c_contiguous):
+                p = _u8(p)
+            if not (type(s) is np.ndarray and s.dtype is _U8 and s.flags.c_contiguous):
+                s = _u8(s)
+            n = m.size >> 5
+            if p.size != (33 if kind == 0 else 32) * n:
+                raise ValueError(f"pubkeys: expected {(33 if kind == 0 else 32) * n} bytes, got {p.size}")
+            if s.size != 64 * n:
+                raise ValueError(f"sigs64: expected {64 * n} bytes, got {s.size}")
+            keep.append((m, p, s))
+            meta.append((kind, 0, n, _addr(m) if n else 0, _addr(p) if n else 0, _addr(s) if n else 0, total))
+            total += n
+        out_all = np.zeros(max(1, total), np.uint8)     # one verdict buffer, one view per job
+        tab = np.array(meta, _JOB_DTYPE) if nj else np.zeros(1, _JOB_DTYPE)
+        if nj:
+            o = tab["out_results"]
+            o += _ptr(out_all)
+            o[tab["count"] == 0] = 0
+        self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, tab.ctypes.data_as(ctypes.POINTER(Job)), nj),
+                    "verify_jobs")
+        offs = [t[6] for t in meta]
+        return [out_all[o:o + t[2]] for o, t in zip(offs, meta)]
 
     def schnorr_verify_rlc(self, msg_hashes32, pubkeys_x32, sigs64, batch_size: int = 0, seed32=None,
                            window_bits: int = 0):

@@ -456,7 +456,17 @@ int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
     }
     // A large call: sub-calls of at most kJobsPipeItems items (jobs cut at the
     // boundaries; verdicts are per item) alternate between the two slots, so
-    // the CPU packs sub-call k + 1 while the device verifies sub-call k.
+    // the CPU packs sub-call k + 1 while the device verifies sub-call k.  The
+    // jobs are taken ECDSA first, then BIP-340 (each in call order): a
+    // sub-call holding one kind runs one queue kernel over the whole device,
+    // where interleaved kinds split every sub-call between two kernels, each
+    // with its own tail (4000 mixed jobs: 65 -> 54 ms).  Verdicts go through
+    // each job's own output pointer, so the order is free.
+    std::vector<size_t> order;
+    order.reserve(n_jobs);
+    for (int kind = 0; kind < 2; ++kind)
+        for (size_t i = 0; i < n_jobs; ++i)
+            if ((jobs[i].kind == 0) == (kind == 0)) order.push_back(i);
     std::vector<VerifyJob> part[2];
     bool pending[2] = {false, false};
     int rc = kOk;
@@ -468,15 +478,18 @@ int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
             if ((rc = batch_[q]->finish(part[q].data(), part[q].size())) != kOk) break;
         }
         part[q].clear();
+        // the first sub-calls ramp up from kPipeFirst items, so the device
+        // starts while the CPU packs the next one
+        const size_t cap = std::min(kJobsPipeItems, kPipeFirst << std::min(k, 8));
         size_t n = 0;
-        while (j < n_jobs && n < kJobsPipeItems) {
-            const VerifyJob& J = jobs[j];
+        while (j < n_jobs && n < cap) {
+            const VerifyJob& J = jobs[order[j]];
             if (off >= J.count) {
                 ++j;
                 off = 0;
                 continue;
             }
-            const size_t take = std::min(J.count - off, kJobsPipeItems - n);
+            const size_t take = std::min(J.count - off, cap - n);
             VerifyJob P = J;
             P.count = take;
             P.msgs = J.msgs + 32 * off;

@@ -142,7 +142,7 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_identify_invalid(ufsecp_g
  * budget covers the slots' fixed staging (pinned + device) and the key cache,
  * reserved at creation (fewer slots are made if they do not fit), plus the
  * staged bytes of the items in flight; pending requests wait for room.
- * Config NULL = defaults: 4 slots, 65,536 items per launch, an 8 GiB budget,
+ * Config NULL = defaults: 8 slots, 65,536 items per launch, an 8 GiB budget,
  * no batch window, no key cache. */
 typedef struct ufsecp_gpu_ext_server ufsecp_gpu_ext_server;
 typedef struct {

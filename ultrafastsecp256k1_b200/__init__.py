@@ -196,6 +196,38 @@ def _addr(a: np.ndarray) -> int:
         return _ptr(a)
 
 
+def _flat_u8(x) -> np.ndarray:
+    if type(x) is np.ndarray and x.dtype is _U8 and x.flags.c_contiguous:
+        return x
+    return _u8(x)
+
+
+def _job_table(jobs):
+    """The ufsecp_gpu_ext_job_t table of `jobs` as one numpy record array, the
+    input arrays it points into (to keep alive), one verdict buffer for all
+    jobs and each job's (offset, count) in it.  The per-job Python work is
+    little more than the three buffer addresses."""
+    keep, meta = [], []
+    total = 0
+    for kind, m, p, s in jobs:
+        m, p, s = _flat_u8(m), _flat_u8(p), _flat_u8(s)
+        n = m.size >> 5
+        if p.size != (33 if kind == 0 else 32) * n:
+            raise ValueError(f"pubkeys: expected {(33 if kind == 0 else 32) * n} bytes, got {p.size}")
+        if s.size != 64 * n:
+            raise ValueError(f"sigs64: expected {64 * n} bytes, got {s.size}")
+        keep.append((m, p, s))
+        meta.append((kind, 0, n, _addr(m) if n else 0, _addr(p) if n else 0, _addr(s) if n else 0, total))
+        total += n
+    out_all = np.zeros(max(1, total), np.uint8)
+    tab = np.array(meta, _JOB_DTYPE) if meta else np.zeros(1, _JOB_DTYPE)
+    if meta:
+        o = tab["out_results"]
+        o += _addr(out_all)
+        o[tab["count"] == 0] = 0
+    return tab, keep, out_all, [(t[6], t[2]) for t in meta]
+
+
 def backend_count() -> int:
     return load_library().ufsecp_gpu_backend_count(None, 0)
 
@@ -301,37 +333,11 @@ class GpuContext:
     # ---- ufsecp_gpu_ext.h -------------------------------------------------------
     def verify_jobs(self, jobs):
         """ufsecp_gpu_ext_verify_jobs: jobs = [(kind, msgs, pubs, sigs), ...] with kind 0
-        ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys); returns one verdict array per job.
-        The job table is one numpy record array laid out as ufsecp_gpu_ext_job_t
-        (the per-job Python work is little more than the three buffer addresses)."""
-        nj = len(jobs)
-        keep, meta = [], []
-        total = 0
-        for kind, m, p, s in jobs:
-            if not (type(m) is np.ndarray and m.dtype is _U8 and m.flags.c_contiguous):
-                m = _u8(m)
-            if not (type(p) is np.ndarray and p.dtype is _U8 and p.flags.c_contiguous):
-                p = _u8(p)
-            if not (type(s) is np.ndarray and s.dtype is _U8 and s.flags.c_contiguous):
-                s = _u8(s)
-            n = m.size >> 5
-            if p.size != (33 if kind == 0 else 32) * n:
-                raise ValueError(f"pubkeys: expected {(33 if kind == 0 else 32) * n} bytes, got {p.size}")
-            if s.size != 64 * n:
-                raise ValueError(f"sigs64: expected {64 * n} bytes, got {s.size}")
-            keep.append((m, p, s))
-            meta.append((kind, 0, n, _addr(m) if n else 0, _addr(p) if n else 0, _addr(s) if n else 0, total))
-            total += n
-        out_all = np.zeros(max(1, total), np.uint8)     # one verdict buffer, one view per job
-        tab = np.array(meta, _JOB_DTYPE) if nj else np.zeros(1, _JOB_DTYPE)
-        if nj:
-            o = tab["out_results"]
-            o += _ptr(out_all)
-            o[tab["count"] == 0] = 0
-        self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, tab.ctypes.data_as(ctypes.POINTER(Job)), nj),
+        ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys); returns one verdict array per job."""
+        tab, keep, out_all, offs = _job_table(jobs)
+        self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, tab.ctypes.data_as(ctypes.POINTER(Job)), len(jobs)),
                     "verify_jobs")
-        offs = [t[6] for t in meta]
-        return [out_all[o:o + t[2]] for o, t in zip(offs, meta)]
+        return [out_all[o:o + n] for o, n in offs]
 
     def schnorr_verify_rlc(self, msg_hashes32, pubkeys_x32, sigs64, batch_size: int = 0, seed32=None,
                            window_bits: int = 0):
@@ -482,7 +488,7 @@ class Server:
     """Serving loop over one context (ufsecp_gpu_ext_server_*): submit requests
     of ECDSA / BIP-340 jobs from any thread, wait for their verdicts."""
 
-    def __init__(self, ctx: GpuContext, slots: int = 4, max_launch_items: int = 1 << 16,
+    def __init__(self, ctx: GpuContext, slots: int = 8, max_launch_items: int = 1 << 16,
                  memory_budget_bytes: int = 8 << 30, batch_window_us: int = 0, key_cache_log2: int = 0):
         """key_cache_log2: 0 or 1 = no resident key cache (default), 8..24 = a cache of 2^k slots."""
         self.L = ctx.L
@@ -498,23 +504,13 @@ class Server:
     def submit(self, jobs) -> int:
         """jobs = [(kind, msgs, pubs, sigs), ...]; returns the request id.  The verdict
         arrays are returned by wait()."""
-        arr = (Job * max(1, len(jobs)))()
-        keep, outs = [], []
-        for k, (kind, msgs, pubs, sigs) in enumerate(jobs):
-            m = np.ascontiguousarray(np.asarray(msgs, np.uint8)).reshape(-1)
-            n = m.size // 32
-            p = _buf(pubs, (33 if kind == 0 else 32) * n, "pubkeys")
-            s = _buf(sigs, 64 * n, "sigs64")
-            o = np.zeros(n, np.uint8)
-            keep += [m, p, s]
-            outs.append(o)
-            arr[k] = Job(kind, 0, n, _ptr(m) if n else None, _ptr(p) if n else None, _ptr(s) if n else None,
-                         _ptr(o) if n else None)
+        tab, keep, out_all, offs = _job_table(jobs)
         rid = ctypes.c_uint64()
-        rc = self.L.ufsecp_gpu_ext_server_submit(self._h, arr, len(jobs), ctypes.byref(rid))
+        rc = self.L.ufsecp_gpu_ext_server_submit(self._h, tab.ctypes.data_as(ctypes.POINTER(Job)), len(jobs),
+                                                 ctypes.byref(rid))
         if rc != UFSECP_OK:
             raise UfsecpError(rc, "server_submit")
-        self._keep[rid.value] = (keep, outs, arr)
+        self._keep[rid.value] = (keep, [out_all[o:o + n] for o, n in offs], tab)
         return rid.value
 
     def wait(self, rid: int, timeout_ms: int = 60_000):

@@ -35,7 +35,7 @@
 namespace uf {
 
 struct ServerConfig {
-    uint32_t slots = 4;
+    uint32_t slots = 8;
     uint32_t max_launch_items = 1u << 16;
     uint64_t memory_budget_bytes = 8ull << 30;
     uint32_t batch_window_us = 0;     // wait this long for more work before launching a small batch

@@ -4,6 +4,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <thread>
 #include <vector>
 #include <math.h>
 #include <stdio.h>
@@ -12,6 +13,7 @@
 
 #include "batch.h"
 #include "kernels.h"
+#include "pack_pool.h"
 #include "rlc.h"
 
 namespace uf {
@@ -21,6 +23,7 @@ namespace {
 constexpr size_t kPipeChunk = size_t{1} << 17;   // items per staging slot of a host-buffer call
 constexpr size_t kPipeFirst = size_t{1} << 14;   // items in a host-buffer call's first chunk
 constexpr size_t kJobsPipeItems = size_t{1} << 16;   // items per sub-call of a large mixed-job call
+constexpr size_t kPackSplitItems = size_t{1} << 13;  // chunks at least this large are packed by the pool
 constexpr size_t kDeviceChunk = size_t{1} << 17; // items per launch of a large device-buffer call
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
@@ -130,6 +133,12 @@ void Backend::load_tuning() {
             fclose(f);
         }
     }
+    // staging copies: 4 threads on hosts of 8+ cores (one core's memcpy rate is
+    // near what the device consumes at full speed), 2 on 4+ cores
+    const unsigned hw = std::thread::hardware_concurrency();
+    pack_threads_ = hw >= 8 ? 4 : (hw >= 4 ? 2 : 1);
+    const int pt = env_int("UFSECP_B200_PACK_THREADS", 0);
+    if (pt >= 1 && pt <= 16) pack_threads_ = pt;
     const int rc_env = env_int("UFSECP_B200_RLC_CHUNK", 0);
     if (rc_env >= 2 && rc_env <= 256) rlc_chunk_fixed_ = (uint32_t)rc_env;
     const int ve = env_int("UFSECP_B200_VARIANT_ECDSA", -1), vs = env_int("UFSECP_B200_VARIANT_SCHNORR", -1);
@@ -400,7 +409,13 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
             one(h + o_p, pubs, pub_sz, p_stride);
             one(h + o_s, sigs, 64, s_stride);
         };
-        pack(0, m);
+        if (pack_threads_ > 1 && m >= kPackSplitItems) {
+            if (!pack_pool_) pack_pool_.reset(new PackPool(pack_threads_));
+            const int parts = pack_pool_->threads();
+            pack_pool_->run(parts, [&](int p) { pack(m * p / parts, m * (p + 1) / parts); });
+        } else {
+            pack(0, m);
+        }
         if (collect) memcpy(h + o_o, out + off, m);
         const size_t in_bytes = o_o + (collect ? m : 0);
         if ((e = cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, pstream_[j])) != cudaSuccess)

@@ -43,6 +43,7 @@ struct HostBuf {
 struct VerifyJob;
 class BatchSlot;
 class RlcVerifier;
+class PackPool;
 
 class Backend {
 public:
@@ -155,6 +156,11 @@ private:
     DevBuf dstage_[kPipeSlots];
     cudaStream_t pstream_[kPipeSlots] = {};
     cudaEvent_t pev_[kPipeSlots] = {};
+    // threads that copy one chunk into its staging slot (the caller and
+    // pack_threads_ - 1 helpers; by core count, or UFSECP_B200_PACK_THREADS),
+    // made on first use
+    int pack_threads_ = 1;
+    std::unique_ptr<PackPool> pack_pool_;
     // large device-buffer calls: second stream with fork / join events
     cudaStream_t dstream_ = nullptr;
     cudaEvent_t dfork_ = nullptr, djoin_ = nullptr;

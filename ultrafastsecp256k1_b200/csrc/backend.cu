@@ -22,7 +22,7 @@ namespace {
 // Items per host->device chunk: bounds device memory at ~130 B x 2^22 = 0.5 GB.
 constexpr size_t kPipeChunk = size_t{1} << 17;   // items per staging slot of a host-buffer call
 constexpr size_t kPipeFirst = size_t{1} << 14;   // items in a host-buffer call's first chunk
-constexpr size_t kJobsPipeItems = size_t{1} << 16;   // items per sub-call of a large mixed-job call
+constexpr size_t kJobsPipeItems = size_t{1} << 16;   // most items per sub-call of a large mixed-job call
 constexpr size_t kPackSplitItems = size_t{1} << 13;  // chunks at least this large are packed by the pool
 constexpr size_t kDeviceChunk = size_t{1} << 17; // items per launch of a large device-buffer call
 
@@ -494,8 +494,12 @@ int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
         }
         part[q].clear();
         // the first sub-calls ramp up from kPipeFirst items, so the device
-        // starts while the CPU packs the next one
-        const size_t cap = std::min(kJobsPipeItems, kPipeFirst << std::min(k, 8));
+        // starts while the CPU packs the next one, to one wave of the queue
+        // kernel's resident grid (56,832 items on a 148-SM B200): a sub-call
+        // of 65,536 items was 1.15 waves and ran its tail alone (mixed jobs in
+        // one call 28.8 -> 30.0 M sigs/s, one BIP-340 job 32.2 -> 33.7 M)
+        const size_t wave = std::max<size_t>(kPipeFirst, std::min(kJobsPipeItems, (size_t)queue_grid_ * kVerifyThreads));
+        const size_t cap = std::min(wave, kPipeFirst << std::min(k, 8));
         size_t n = 0;
         while (j < n_jobs && n < cap) {
             const VerifyJob& J = jobs[order[j]];

@@ -7,9 +7,16 @@
  * reference header links against libufsecp_gpu.so unchanged.
  *
  * Implemented on the sm_100a kernels of this library:
- *   discovery / lifecycle, ecdsa_verify_batch, schnorr_verify_batch,
- *   ecdsa_verify_collect, schnorr_verify_collect, error_str.
- * Every other operation of the reference surface is present for link
+ *   discovery / lifecycle / errors: backend_count, backend_name, is_available,
+ *     device_count, device_info, ctx_create, ctx_destroy, is_ready, last_error,
+ *     last_error_msg, error_str;
+ *   verification: ecdsa_verify_batch, schnorr_verify_batch, ecdsa_verify_collect,
+ *     schnorr_verify_collect, ecdsa_verify_opaque_rows, ecdsa_verify_lbtc_rows,
+ *     ecdsa_verify_lbtc_columns, schnorr_verify_lbtc_columns;
+ *   adjacent operations on the same math: msm, xonly_validate, pubkey_validate,
+ *     commitment_verify, tagged_hash, tagged_hash_var.
+ * Every other operation of the reference surface (key generation, ECDH,
+ * hashing, BIP-324 / BIP-352, ZK, FROST, recovery) is present for link
  * compatibility and returns UFSECP_ERR_GPU_UNSUPPORTED (104), which the
  * reference header allows for operations a backend does not implement.
  *

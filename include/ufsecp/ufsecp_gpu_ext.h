@@ -61,15 +61,19 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const 
  * allocate).  No counterpart in the reference.  The jobs' buffers are DEVICE
  * (device-accessible) memory the caller owns: msgs / signatures / x-only keys
  * 16-byte aligned, outputs one byte per item.  The call allocates nothing: the
- * work-queue kernel's scratch (queue head and job table) is a static device
- * array of the library, at most UFSECP_GPU_EXT_NOALLOC_MAX_JOBS jobs per call
- * (more -> UFSECP_ERR_BAD_INPUT with an explanatory last_error_msg).  The
- * first call on a device looks up that array's device address; make it before
- * any stream capture.  The call returns after enqueueing the kernel on
- * `stream` (NULL = the context's stream); the verdicts are ready when the
- * stream reaches that point.  All calls share the array and the queue head is
- * reset by every call, so calls whose work overlaps on the GPU race: serialise
- * them (one stream, or wait for the previous call). */
+ * work-queue kernel's scratch (queue head and job table, 49,408 bytes) is a
+ * static device array of the library, at most UFSECP_GPU_EXT_NOALLOC_MAX_JOBS
+ * jobs per call (more -> UFSECP_ERR_BAD_INPUT with an explanatory
+ * last_error_msg).  The first call on a device looks up that array's device
+ * address; make that first call before any stream capture.  The job table is
+ * copied to the device from the library's own pageable host staging, so the
+ * call may wait until those bytes are staged; it then enqueues the kernel on
+ * `stream` (NULL = the context's stream) and returns; the verdicts are ready
+ * when the stream reaches that point.  If the copy or the launch fails, every
+ * job's verdict bytes are cleared on `stream` and the error is returned.  All
+ * calls share the array and the queue head is reset by every call, so calls
+ * whose work overlaps on the GPU race: serialise them (one stream, or wait for
+ * the previous call). */
 #define UFSECP_GPU_EXT_NOALLOC_MAX_JOBS 1024
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs_noalloc(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
                                                              size_t n_jobs, void* stream);
@@ -105,6 +109,19 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc_device(ufsecp_gpu_ct
  * plus one per bisection level), out[1] segments checked, out[2] items
  * verified one by one, out[3] window bits of the first round. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_stats(ufsecp_gpu_ctx* ctx, uint64_t out[4]);
+
+/* Input binding of the reference-shaped batch API's seed: the SHA-256 tree
+ * digest of n BIP-340 items (host buffers, layouts as above).  Per item
+ * d_i = SHA-256(r || s || x(P) || m) (the 128 bytes the reference hashes per
+ * entry, src/cpu/src/batch_verify.cpp:361-369); then, while more than one
+ * digest remains, groups of 16 consecutive digests are replaced by the
+ * SHA-256 of their concatenation (a short last group hashes what it has);
+ * out32 = SHA-256(root || le32 n).  ufsecp_gpu_ext_schnorr_batch_verify and
+ * _identify_invalid take their RLC seed as this digest XOR 32 fresh random
+ * bytes, as the reference mixes its input hash with CSPRNG bytes (:355-380). */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_input_digest(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32,
+                                                          const uint8_t* pubkeys_x32, const uint8_t* sigs64,
+                                                          size_t count, uint8_t out32[32]);
 
 /* The reference's batch API on the GPU, same rows, gating and results:
  * ufsecp_schnorr_batch_verify (src/cpu/src/impl/ufsecp_taproot.cpp:703) and

@@ -1,8 +1,8 @@
 """Generate the committed golden fixtures for the verify path.
 
-Run here (where the reference tree and oracle/_ref exist), never on the GPU box:
+Run where the reference source tree and oracle/_ref exist, never on the GPU box:
 
-    make -C oracle -j8 && python tests/golden/make_golden.py
+    make -C oracle ref REF=<tree> -j8 && UFSECP_REFERENCE=<tree> python tests/golden/make_golden.py
 
 Outputs (all verdicts come from RUNNING the reference's own CPU library,
 oracle/_ref/libufsecp_ref.so, through its C ABI ufsecp_ecdsa_verify /
@@ -38,7 +38,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from oracle import RefLib  # noqa: E402
 
-REF = os.environ.get("UFSECP_REFERENCE", "/root/reference")
+# the reference source tree (its test files hold the vectors); no default
+REF = os.environ.get("UFSECP_REFERENCE", "")
 P = 2**256 - 2**32 - 977
 N = 0xFFFFFFFFFFFFFFFFFFFFFFFFFFFFFFFEBAAEDCE6AF48A03BBFD25E8CD0364141
 
@@ -294,4 +295,6 @@ def main():
 
 
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(os.path.join(REF, "src")):
+        sys.exit("set UFSECP_REFERENCE to the reference source tree")
     main()

@@ -258,3 +258,26 @@ def test_batch_api_parse_gate_order(gpu_ctx, oracle, reflib):
         assert gpu_ctx.schnorr_batch_verify(r) == want
         assert gpu_ctx.schnorr_batch_identify_invalid(r)[0] == reflib.schnorr_batch_identify_invalid_rows(r)[0]
     assert gpu_ctx.schnorr_batch_verify(base[:0]) == uf.UFSECP_OK
+
+
+def _tree_digest(m, x, s):
+    """The RLC seed's input binding written out with hashlib: per item
+    SHA-256(r || s || x || m), 16-way tree, then SHA-256(root || le32 n)."""
+    import hashlib
+    n = len(m)
+    level = [hashlib.sha256(s[i].tobytes() + x[i].tobytes() + m[i].tobytes()).digest() for i in range(n)]
+    while len(level) > 1:
+        level = [hashlib.sha256(b"".join(level[k:k + 16])).digest() for k in range(0, len(level), 16)]
+    root = level[0] if level else bytes(32)
+    return hashlib.sha256(root + n.to_bytes(4, "little")).digest()
+
+
+@pytest.mark.parametrize("n", [0, 1, 15, 16, 17, 257, 4099])
+def test_rlc_input_digest_matches_hashlib(gpu_ctx, oracle, n):
+    m, x, s = schnorr_corpus(oracle, max(n, 1), seed=777 + n, tamper=0.05)
+    m, x, s = m[:n], x[:n], s[:n]
+    assert gpu_ctx.rlc_input_digest(m, x, s) == _tree_digest(m, x, s)
+    if n:
+        m2 = m.copy()
+        m2[n - 1, 0] ^= 1
+        assert gpu_ctx.rlc_input_digest(m2, x, s) != gpu_ctx.rlc_input_digest(m, x, s)

@@ -36,14 +36,19 @@ def _device_jobs(torch, specs):
 
 
 def _run_noalloc(gpu_ctx, torch, specs):
+    """Runs the entry point on device copies of `specs`; returns the verdicts and
+    the device's free bytes just before and just after the call (inputs, outputs
+    and the stream are created before the first reading)."""
     keep, arr = _device_jobs(torch, specs)
     L = uf.load_library()
-    torch.cuda.synchronize()
     stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
     rc = L.ufsecp_gpu_ext_verify_jobs_noalloc(gpu_ctx.handle, arr, len(specs), stream.cuda_stream)
     assert rc == uf.UFSECP_OK, gpu_ctx.last_error_msg()
     stream.synchronize()
-    return [keep[k][3][:len(specs[k][1])].cpu().numpy() for k in range(len(specs))]
+    free_after = torch.cuda.mem_get_info()[0]
+    return [keep[k][3][:len(specs[k][1])].cpu().numpy() for k in range(len(specs))], free_before, free_after
 
 
 def test_no_alloc_matches_existing_entry_point_twice(gpu_ctx, oracle):
@@ -53,8 +58,12 @@ def test_no_alloc_matches_existing_entry_point_twice(gpu_ctx, oracle):
     first = [(1,) + tuple(x[:1000] for x in s), (0,) + tuple(x[:700] for x in e), (1,) + tuple(x[1000:1001] for x in s),
              (0,) + tuple(x[700:700] for x in e), (0,) + tuple(x[700:1500] for x in e)]
     second = [(0,) + tuple(x[:33] for x in e), (1,) + tuple(x[1001:2500] for x in s)]
-    for specs in (first, second):
-        got = _run_noalloc(gpu_ctx, torch, specs)
+    for call, specs in enumerate((first, second)):
+        got, free_before, free_after = _run_noalloc(gpu_ctx, torch, specs)
+        if call == 1:
+            # the point of this entry point: once a device has seen its first
+            # call, a call takes no device memory at all
+            assert free_after == free_before, (free_before, free_after)
         want = gpu_ctx.verify_jobs(specs)                      # the existing entry point
         for g, w, (kind, m, p, sg) in zip(got, want, specs):
             assert g.shape == w.shape

@@ -130,6 +130,7 @@ _SIGS = {
     "ufsecp_gpu_ext_server_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats), ctypes.c_int]),
     "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "ufsecp_gpu_ext_rlc_input_digest": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_schnorr_batch_verify": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
     "ufsecp_gpu_ext_schnorr_batch_identify_invalid": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t,
                                                                      ctypes.POINTER(ctypes.c_size_t),
@@ -373,6 +374,19 @@ class GpuContext:
         v = (ctypes.c_uint64 * 4)()
         self._check(self.L.ufsecp_gpu_ext_rlc_stats(self._ctx, v), "rlc_stats")
         return {"rounds": v[0], "segments": v[1], "leaf_items": v[2], "window_bits": v[3]}
+
+    def rlc_input_digest(self, msg_hashes32, pubkeys_x32, sigs64) -> bytes:
+        """ufsecp_gpu_ext_rlc_input_digest: the SHA-256 tree digest that binds the
+        reference-shaped batch API's RLC seed to its inputs."""
+        n = len(np.asarray(msg_hashes32, np.uint8).reshape(-1)) // 32
+        m = _buf(msg_hashes32, 32 * n, "msg_hashes32")
+        p = _buf(pubkeys_x32, 32 * n, "pubkeys_x32")
+        s = _buf(sigs64, 64 * n, "sigs64")
+        out = np.zeros(32, np.uint8)
+        rc = self.L.ufsecp_gpu_ext_rlc_input_digest(self._ctx, _ptr(m) if n else None, _ptr(p) if n else None,
+                                                    _ptr(s) if n else None, n, _ptr(out))
+        self._check(rc, "rlc_input_digest")
+        return out.tobytes()
 
     def schnorr_batch_verify(self, entries) -> int:
         """ufsecp_gpu_ext_schnorr_batch_verify on rows [x 32 | msg 32 | sig 64]; returns the

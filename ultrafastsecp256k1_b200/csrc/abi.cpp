@@ -524,14 +524,10 @@ ufsecp_error_t ufsecp_gpu_ext_verify_jobs_noalloc(ufsecp_gpu_ctx* ctx, const ufs
     }
     if (total > kMaxBatch) return be.set_error(UFSECP_ERR_BAD_INPUT, "more than 2^26 items");
     if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
-    uf::NoAllocJobDesc desc[uf::kNoAllocJobLimit];
-    for (size_t j = 0; j < n_jobs; ++j)
-        desc[j] = uf::NoAllocJobDesc{jobs[j].kind, jobs[j].count, jobs[j].msg_hashes32, jobs[j].pubkeys,
-                                     jobs[j].sigs64, jobs[j].out_results};
     cudaError_t e = cudaSetDevice(be.device());
     int limit = 0;
     if (e == cudaSuccess)
-        e = uf::verify_jobs_noalloc(be.device(), desc, n_jobs, be.gtab(),
+        e = uf::verify_jobs_noalloc(be.device(), jobs, n_jobs, be.gtab(),
                                     stream ? (cudaStream_t)stream : be.stream(), &limit);
     if (limit) return be.set_error(UFSECP_ERR_BAD_INPUT, "job limits of the allocation-free path exceeded");
     if (e != cudaSuccess) return be.cuda_error(e, "allocation-free verify");
@@ -649,6 +645,8 @@ namespace {
 constexpr size_t kMaxRlcItems = size_t{1} << 24;
 constexpr size_t kMaxRefBatch = size_t{1} << 20;   // the reference batch API's cap
 
+// 32 bytes from the host's random device; the reference batch API mixes them
+// into a digest of the batch's inputs (RlcVerifier::verify_entries).
 void fresh_seed(uint8_t seed[32]) {
     std::random_device rd;
     for (int k = 0; k < 8; ++k) {
@@ -741,6 +739,24 @@ ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc_device(ufsecp_gpu_ctx* ctx, con
         const int rc = be.rlc().verify(d_msg_hashes32, d_pubkeys_x32, d_sigs64, (uint32_t)count,
                                        (uint32_t)std::min(batch_size, count), seed32, window_bits, d_out_results,
                                        out_batch_ok, stream ? (cudaStream_t)stream : be.stream(), &ctx->rlc_stats);
+        if (rc != UFSECP_OK) return rc;
+        be.clear_error();
+        return UFSECP_OK;
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_rlc_input_digest(ufsecp_gpu_ctx* ctx, const uint8_t* msg_hashes32,
+                                               const uint8_t* pubkeys_x32, const uint8_t* sigs64, size_t count,
+                                               uint8_t out32[32]) {
+    if (!ctx || !out32) return UFSECP_ERR_NULL_ARG;
+    if (count > kMaxRlcItems) return ctx->backend->set_error(UFSECP_ERR_BAD_INPUT, "RLC: more than 2^24 items");
+    if (count && (!msg_hashes32 || !pubkeys_x32 || !sigs64)) return UFSECP_ERR_NULL_ARG;
+    return guarded([&]() -> ufsecp_error_t {
+        uf::Backend& be = *ctx->backend;
+        if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
+        cudaError_t e = cudaSetDevice(be.device());
+        if (e != cudaSuccess) return be.cuda_error(e, "cudaSetDevice");
+        const int rc = be.rlc().input_digest_host(msg_hashes32, pubkeys_x32, sigs64, (uint32_t)count, out32);
         if (rc != UFSECP_OK) return rc;
         be.clear_error();
         return UFSECP_OK;

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "ufsecp/ufsecp_gpu_ext.h"
 
 namespace uf {
 
@@ -129,19 +130,17 @@ int verify_pair_occupancy();
 cudaError_t launch_verify_queue_pair(const QueueArgs& a, const void* d_gtab, unsigned int* d_head, int grid,
                                      cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
 
-// Allocation-free mixed verification (kernels_noalloc.cu): jobs hold
-// device-accessible buffers; the queue head and the job table live in a
-// static device array of the library, nothing is allocated.
-struct NoAllocJobDesc {
-    uint32_t kind;
-    size_t count;
-    const uint8_t* msgs;
-    const uint8_t* pubs;
-    const uint8_t* sigs;
-    uint8_t* out;
-};
+// Allocation-free mixed verification (kernels_noalloc.cu): the jobs' buffers
+// are device-accessible memory the caller owns; the queue head and the job
+// table live in a static device array of the library (kNoAllocScratchBytes,
+// 49,408 bytes), nothing is allocated.  The descriptor table is built
+// straight into a per-thread staging array (no large stack frame).  On a
+// failed launch every job's verdict bytes are cleared with cudaMemsetAsync.
 constexpr size_t kNoAllocJobLimit = 1024;
-cudaError_t verify_jobs_noalloc(int device, const NoAllocJobDesc* jobs, size_t n_jobs, const void* d_gtab,
+constexpr size_t kNoAllocHeaderBytes = 256;
+constexpr size_t kNoAllocJobBytes = 48;
+constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocJobLimit * kNoAllocJobBytes;
+cudaError_t verify_jobs_noalloc(int device, const ufsecp_gpu_ext_job_t* jobs, size_t n_jobs, const void* d_gtab,
                                 cudaStream_t s, int* limit_hit);
 
 // Batch signer (workload generator): kind 0 = ECDSA (pubs 33 B), 1 = BIP-340

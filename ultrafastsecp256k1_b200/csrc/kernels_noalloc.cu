@@ -8,8 +8,8 @@
 // verifier from allocating behind their back.  They pass inputs and outputs
 // they already own (device-accessible pointers); this path allocates nothing.
 //
-// The scratch is kNoAllocScratchBytes of static device memory: the queue head
-// and a table of at most kNoAllocMaxJobs job descriptors.  Every GPU that loads
+// The scratch is kNoAllocScratchBytes (49,408 bytes) of static device memory:
+// the queue head and a table of at most kNoAllocJobLimit job descriptors.  Every GPU that loads
 // the library holds it until the process exits.  All calls share it and it
 // keeps the last call's contents: the queue head is cleared on every call, and
 // calls whose work overlaps on the GPU (different streams, or different host
@@ -18,7 +18,11 @@
 // In host code `g_noalloc_scratch` is only a host-side stand-in for the symbol,
 // not a device address; its device address is looked up once per device with
 // cudaGetSymbolAddress (with that device current) on the first call on that
-// device, so that first call should come before any stream capture.
+// device, so that first call should come before any stream capture.  The
+// descriptor table is copied from a per-thread host staging array (pageable
+// memory the library owns, not an allocation per call); cudaMemcpyAsync has
+// staged those bytes when it returns, so the array is free for the next call
+// on the thread without waiting for the stream.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -41,9 +45,8 @@ struct NoAllocJob {
     uint32_t pad;
 };
 
-constexpr uint32_t kNoAllocMaxJobs = 1024;
-constexpr size_t kNoAllocHeader = 256;   // queue head, job count, total items
-constexpr size_t kNoAllocScratchBytes = kNoAllocHeader + kNoAllocMaxJobs * sizeof(NoAllocJob);
+static_assert(sizeof(NoAllocJob) == kNoAllocJobBytes, "descriptor layout");
+constexpr size_t kNoAllocHeader = kNoAllocHeaderBytes;   // queue head, job count, total items
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -95,13 +98,13 @@ void* g_noalloc_addr[64] = {};   // device address of the scratch, per device or
 int g_noalloc_grid[64] = {};
 }  // namespace
 
-// Host part of the entry point.  `jobs` is a host array of descriptors whose
-// buffers are device-accessible; returns a cudaError_t, or cudaErrorInvalidValue
-// (with *limit_hit set) when a limit is exceeded.
-cudaError_t verify_jobs_noalloc(int device, const NoAllocJobDesc* jobs, size_t n_jobs, const void* d_gtab,
+// Host part of the entry point.  `jobs` is the caller's host array of
+// descriptors whose buffers are device-accessible; returns a cudaError_t, or
+// cudaErrorInvalidValue (with *limit_hit set) when a limit is exceeded.
+cudaError_t verify_jobs_noalloc(int device, const ufsecp_gpu_ext_job_t* jobs, size_t n_jobs, const void* d_gtab,
                                 cudaStream_t s, int* limit_hit) {
     *limit_hit = 0;
-    if (n_jobs > kNoAllocMaxJobs) {
+    if (n_jobs > kNoAllocJobLimit) {
         *limit_hit = 1;
         return cudaErrorInvalidValue;
     }
@@ -133,8 +136,9 @@ cudaError_t verify_jobs_noalloc(int device, const NoAllocJobDesc* jobs, size_t n
         grid = g_noalloc_grid[device];
     }
     if (total == 0) return cudaSuccess;
-    // header + descriptor table, built on the host stack and copied in one piece
-    static thread_local uint8_t staged[kNoAllocScratchBytes];
+    // header + descriptor table, built straight into this thread's staging
+    // array and copied in one piece
+    alignas(16) static thread_local uint8_t staged[kNoAllocScratchBytes];
     memset(staged, 0, kNoAllocHeader);
     uint32_t* hdr = reinterpret_cast<uint32_t*>(staged);
     hdr[0] = 0;                        // queue head starts at zero on every call
@@ -143,21 +147,26 @@ cudaError_t verify_jobs_noalloc(int device, const NoAllocJobDesc* jobs, size_t n
     NoAllocJob* tab = reinterpret_cast<NoAllocJob*>(staged + kNoAllocHeader);
     uint32_t first = 0;
     for (size_t j = 0; j < n_jobs; ++j) {
-        tab[j] = NoAllocJob{jobs[j].msgs, jobs[j].pubs, jobs[j].sigs, jobs[j].out, jobs[j].kind,
-                            (uint32_t)jobs[j].count, first, 0};
-        first += (uint32_t)jobs[j].count;
+        const ufsecp_gpu_ext_job_t& J = jobs[j];
+        tab[j] = NoAllocJob{J.msg_hashes32, J.pubkeys, J.sigs64, J.out_results, J.kind, (uint32_t)J.count, first, 0};
+        first += (uint32_t)J.count;
     }
     const size_t bytes = kNoAllocHeader + n_jobs * sizeof(NoAllocJob);
     cudaError_t e = cudaMemcpyAsync(addr, staged, bytes, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return e;
-    // the staging array is reused by the next call on this thread: wait for the copy to leave it
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-    const int need = (int)((total + kVerifyThreads - 1) / kVerifyThreads);
-    const int g = grid < need ? grid : need;
-    const size_t smem = kVerifyThreads * kVerifySmemPerThread;
-    k_verify_jobs_noalloc<<<g, kVerifyThreads, smem, s>>>(reinterpret_cast<uint8_t*>(addr),
-                                                          reinterpret_cast<const uint4*>(d_gtab));
-    return cudaGetLastError();
+    if (e == cudaSuccess) {
+        const int need = (int)((total + kVerifyThreads - 1) / kVerifyThreads);
+        const int g = grid < need ? grid : need;
+        const size_t smem = kVerifyThreads * kVerifySmemPerThread;
+        k_verify_jobs_noalloc<<<g, kVerifyThreads, smem, s>>>(reinterpret_cast<uint8_t*>(addr),
+                                                              reinterpret_cast<const uint4*>(d_gtab));
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        // fail closed: no verdict byte of this call may read as valid
+        for (size_t j = 0; j < n_jobs; ++j)
+            if (jobs[j].count && jobs[j].out_results) (void)cudaMemsetAsync(jobs[j].out_results, 0, jobs[j].count, s);
+    }
+    return e;
 }
 
 }  // namespace uf

@@ -427,6 +427,61 @@ __global__ void k_rlc_scatter(const uint32_t* __restrict__ idx, uint32_t m, cons
     if (k < m) out[idx[k]] = v[k];
 }
 
+// Input binding of the batch seed.  The reference hashes every entry's
+// r || s || x(P) || m into its batch seed before mixing in CSPRNG bytes
+// (src/cpu/src/batch_verify.cpp:355-380).  Here the same 128 bytes per item
+// are hashed on the device as a tree: k_rlc_leafhash gives one SHA-256 digest
+// per item, k_rlc_treehash hashes groups of kTreeFan consecutive digests
+// until one remains; the host then takes SHA-256(root || le32 n).
+constexpr uint32_t kTreeFan = 16;
+
+__global__ void k_rlc_leafhash(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ xs,
+                               const uint8_t* __restrict__ sigs, uint32_t n, uint32_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t w[16], t[8], h[8];
+    sha256_iv(h);
+    load_words8(t, sigs + 64ull * i);
+    for (int k = 0; k < 8; ++k) w[k] = bswap32(t[k]);
+    load_words8(t, sigs + 64ull * i + 32);
+    for (int k = 0; k < 8; ++k) w[8 + k] = bswap32(t[k]);
+    sha256_compress(h, w);
+    load_words8(t, xs + 32ull * i);
+    for (int k = 0; k < 8; ++k) w[k] = bswap32(t[k]);
+    load_words8(t, msgs + 32ull * i);
+    for (int k = 0; k < 8; ++k) w[8 + k] = bswap32(t[k]);
+    sha256_compress(h, w);
+    w[0] = 0x80000000u;
+    for (int k = 1; k < 15; ++k) w[k] = 0;
+    w[15] = 1024;   // 128 bytes
+    sha256_compress(h, w);
+    for (int k = 0; k < 8; ++k) out[8ull * i + k] = h[k];
+}
+
+// Node j: SHA-256 of digests [j*kTreeFan, min(n, (j+1)*kTreeFan)) concatenated.
+__global__ void k_rlc_treehash(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ out) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lo = j * kTreeFan;
+    if (lo >= n) return;
+    const uint32_t cnt = min(kTreeFan, n - lo);
+    uint32_t w[16], h[8];
+    sha256_iv(h);
+    uint32_t k = 0;
+    for (; k + 2 <= cnt; k += 2) {
+        for (int q = 0; q < 16; ++q) w[q] = in[8ull * (lo + k) + q];
+        sha256_compress(h, w);
+    }
+    int q = 0;
+    if (k < cnt) {
+        for (; q < 8; ++q) w[q] = in[8ull * (lo + k) + q];
+    }
+    w[q++] = 0x80000000u;
+    for (; q < 15; ++q) w[q] = 0;
+    w[15] = cnt * 256;   // bits
+    sha256_compress(h, w);
+    for (int t = 0; t < 8; ++t) out[8ull * j + t] = h[t];
+}
+
 // Rows [x 32 | msg 32 | sig 64] -> three arrays, and the reference's parse
 // gate: *first = min over failing rows of (row << 2 | code - 3), code 3 for
 // x >= p, 4 for r >= p or s outside [1, n-1] (the x test comes first).
@@ -545,7 +600,7 @@ RlcVerifier::~RlcVerifier() {
     for (DevBuf* b : {&items_, &mags_, &tsc_, &okb_, &segs_, &segmag_, &segneg_, &segbad_, &counts_, &offsets_,
                       &cursor_, &nch_, &coff_, &entries_, &partials_, &buckets_, &wu_, &wt_, &wins_, &segok_,
                       &scan_tmp_, &leaf_idx_, &leaf_m_, &leaf_x_, &leaf_s_, &leaf_out_, &in_m_, &in_x_, &in_s_,
-                      &in_out_, &in_rows_, &gate_, &segpt_})
+                      &in_out_, &in_rows_, &gate_, &segpt_, &dig_a_, &dig_b_})
         b->release();
 }
 
@@ -749,7 +804,57 @@ int RlcVerifier::verify_host(const uint8_t* msgs, const uint8_t* xs, const uint8
     return kOk;
 }
 
-int RlcVerifier::verify_entries(const uint8_t* rows, uint32_t n, const uint8_t seed[32], uint8_t* h_out,
+int RlcVerifier::input_digest(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_t* d_sigs, uint32_t n,
+                              cudaStream_t s, uint8_t out[32]) {
+    // two ping-pong digest arrays: n leaves, then n / kTreeFan nodes per level
+    const uint64_t cap = std::max<uint64_t>(n, 1);
+    cudaError_t e;
+    if ((e = dig_a_.ensure(32 * cap)) != cudaSuccess || (e = dig_b_.ensure(32 * (cap / kTreeFan + 1))) != cudaSuccess)
+        return be_->cuda_error(e, "RLC digest buffers");
+    uint32_t* a = (uint32_t*)dig_a_.p;
+    uint32_t* b = (uint32_t*)dig_b_.p;
+    uint32_t root[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // n == 0: the all-zero root
+    if (n) k_rlc_leafhash<<<grid_for(n, 128), 128, 0, s>>>(d_msgs, d_xs, d_sigs, n, a);
+    uint32_t m = n;
+    while (m > 1) {
+        const uint32_t nodes = (m + kTreeFan - 1) / kTreeFan;
+        k_rlc_treehash<<<grid_for(nodes, 128), 128, 0, s>>>(a, m, b);
+        std::swap(a, b);
+        m = nodes;
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess && n) e = cudaMemcpyAsync(root, a, 32, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC input digest");
+    // SHA-256(root || le32 n)
+    uint8_t buf[36];
+    words_to_bytes(buf, root);
+    for (int k = 0; k < 4; ++k) buf[32 + k] = (uint8_t)(n >> (8 * k));
+    uint32_t h[8];
+    sha256_iv(h);
+    sha256_tail(h, buf, 36, 0);
+    words_to_bytes(out, h);
+    return kOk;
+}
+
+int RlcVerifier::input_digest_host(const uint8_t* msgs, const uint8_t* xs, const uint8_t* sigs, uint32_t n,
+                                   uint8_t out[32]) {
+    const cudaStream_t s = be_->stream();
+    const uint64_t cap = std::max<uint32_t>(n, 1);
+    cudaError_t e;
+    if ((e = in_m_.ensure(32 * cap)) != cudaSuccess || (e = in_x_.ensure(32 * cap)) != cudaSuccess ||
+        (e = in_s_.ensure(64 * cap)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC staging buffers");
+    if (n) {
+        e = cudaMemcpyAsync(in_m_.p, msgs, 32ull * n, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(in_x_.p, xs, 32ull * n, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(in_s_.p, sigs, 64ull * n, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return be_->cuda_error(e, "RLC copy in");
+    }
+    return input_digest((const uint8_t*)in_m_.p, (const uint8_t*)in_x_.p, (const uint8_t*)in_s_.p, n, s, out);
+}
+
+int RlcVerifier::verify_entries(const uint8_t* rows, uint32_t n, const uint8_t rand32[32], uint8_t* h_out,
                                 int* gate_code, uint32_t* gate_index, RlcStats* stats) {
     *gate_code = 0;
     *gate_index = 0;
@@ -776,8 +881,13 @@ int RlcVerifier::verify_entries(const uint8_t* rows, uint32_t n, const uint8_t s
         *gate_index = first >> 2;
         return kOk;
     }
-    const int rc = verify((const uint8_t*)in_m_.p, (const uint8_t*)in_x_.p, (const uint8_t*)in_s_.p, n, n, seed, 0,
-                          (uint8_t*)in_out_.p, nullptr, s, stats);
+    // batch seed = digest of every row's r || s || x(P) || m, XOR fresh random bytes
+    uint8_t seed[32];
+    int rc = input_digest((const uint8_t*)in_m_.p, (const uint8_t*)in_x_.p, (const uint8_t*)in_s_.p, n, s, seed);
+    if (rc != kOk) return rc;
+    for (int k = 0; k < 32; ++k) seed[k] ^= rand32[k];
+    rc = verify((const uint8_t*)in_m_.p, (const uint8_t*)in_x_.p, (const uint8_t*)in_s_.p, n, n, seed, 0,
+                (uint8_t*)in_out_.p, nullptr, s, stats);
     if (rc != kOk) return rc;
     e = cudaMemcpyAsync(h_out, in_out_.p, n, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

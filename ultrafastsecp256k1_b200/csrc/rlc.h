@@ -77,9 +77,19 @@ public:
     // x(P) >= p sets *gate_code = 3 (BAD_PUBKEY), one with r >= p or s outside
     // [1, n-1] sets 4 (BAD_SIG), and *gate_index to that row; then nothing is
     // verified.  Otherwise *gate_code = 0 and h_out[i] = 1 / 0 per row, all rows
-    // in one RLC batch.
-    int verify_entries(const uint8_t* entries, uint32_t n, const uint8_t seed[32], uint8_t* h_out, int* gate_code,
+    // in one RLC batch whose seed binds the inputs as the reference's does
+    // (src/cpu/src/batch_verify.cpp:355-380): input_digest() of the rows XOR
+    // the 32 random bytes rand32.
+    int verify_entries(const uint8_t* entries, uint32_t n, const uint8_t rand32[32], uint8_t* h_out, int* gate_code,
                        uint32_t* gate_index, RlcStats* stats);
+
+    // SHA-256 tree digest of n device-resident items: one digest of
+    // r || s || x(P) || m per item, then 16-way tree levels, then
+    // SHA-256(root || le32 n).  Synchronous on `s`.
+    int input_digest(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_t* d_sigs, uint32_t n, cudaStream_t s,
+                     uint8_t out[32]);
+    // The same over host buffers (copied in on the backend's stream).
+    int input_digest_host(const uint8_t* msgs, const uint8_t* xs, const uint8_t* sigs, uint32_t n, uint8_t out[32]);
 
     // Multi-scalar multiplication sum k_i P_i over host arrays (32-byte
     // big-endian scalars, 33-byte compressed points) with the same Pippenger
@@ -108,6 +118,7 @@ private:
     // host-buffer calls
     DevBuf in_m_, in_x_, in_s_, in_out_, in_rows_, gate_;
     DevBuf segpt_;       // each segment's final sum (Jacobian, 112 B)
+    DevBuf dig_a_, dig_b_;   // input digest tree levels
     std::vector<uint8_t> ok_host_;
 };
 

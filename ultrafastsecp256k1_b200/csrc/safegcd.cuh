@@ -5,10 +5,37 @@
 // Role in the reference: the CPU inverses Scalar::inverse (src/cpu/src/scalar.cpp:841,
 // 30-bit variant :850-1120) and fe_inverse_safegcd_impl (src/cpu/src/field.cpp:2848).
 // The reference GPU path uses Fermat chains instead (secp256k1.cuh:823, :2614-2706);
-// this file gives the GPU the divstep algorithm.  Written from the published
-// algorithm (Bernstein & Yang, "Fast constant-time gcd computation and modular
-// inversion", 2019), variable-time variant (inputs here are public):
+// this file gives the GPU the divstep algorithm (Bernstein & Yang, "Fast
+// constant-time gcd computation and modular inversion", 2019), variable-time
+// variant (inputs here are public).
 //
+// Code form followed: libsecp256k1's variable-time modular inversion,
+// src/modinv32_impl.h (secp256k1_modinv32_divsteps_30_var,
+// secp256k1_modinv32_update_de_30) and, for the 6-bit inverse step of
+// f^-1 mod 2^6 (w = f g (f f - 2)), src/modinv64_impl.h.  divsteps30_var and
+// update_de30 below take their statement structure from those functions
+// (the trailing-zero batched loop, the swap / negate, the md / me correction
+// that makes the division by 2^30 exact); the limb conversion helpers are
+// this file's own.  That code is distributed under the MIT licence:
+//
+//   Copyright (c) 2020 Peter Dettman (libsecp256k1 modinv32 / modinv64)
+//   Permission is hereby granted, free of charge, to any person obtaining a
+//   copy of this software and associated documentation files (the
+//   "Software"), to deal in the Software without restriction, including
+//   without limitation the rights to use, copy, modify, merge, publish,
+//   distribute, sublicense, and/or sell copies of the Software, and to permit
+//   persons to whom the Software is furnished to do so, subject to the
+//   following conditions: The above copyright notice and this permission
+//   notice shall be included in all copies or substantial portions of the
+//   Software.  THE SOFTWARE IS PROVIDED "AS IS", WITHOUT WARRANTY OF ANY
+//   KIND, EXPRESS OR IMPLIED, INCLUDING BUT NOT LIMITED TO THE WARRANTIES OF
+//   MERCHANTABILITY, FITNESS FOR A PARTICULAR PURPOSE AND NONINFRINGEMENT.
+//   IN NO EVENT SHALL THE AUTHORS OR COPYRIGHT HOLDERS BE LIABLE FOR ANY
+//   CLAIM, DAMAGES OR OTHER LIABILITY, WHETHER IN AN ACTION OF CONTRACT, TORT
+//   OR OTHERWISE, ARISING FROM, OUT OF OR IN CONNECTION WITH THE SOFTWARE OR
+//   THE USE OR OTHER DEALINGS IN THE SOFTWARE.
+//
+// Algorithm:
 //   state f = M, g = x, d = 0, e = 1, with invariants d*x = f, e*x = g (mod M)
 //   and delta = 1 (kept as eta = -delta).  Batches of 30 divsteps are run on
 //   the low 32 bits of f, g, accumulating a 2x2 transition matrix T with

@@ -55,6 +55,24 @@ typedef struct {
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
                                                      size_t n_jobs);
 
+/* Resident key table of ufsecp_gpu_ext_verify_jobs (no reference
+ * counterpart).  Per distinct public key (x, parity) a device slot keeps the
+ * decompressed key's 1P..8P table, so a key seen before skips its square root,
+ * table additions and the table's inversion; an x off the curve is remembered
+ * as such.  Before the verify kernels, a resolve pass gives each item its key's
+ * slot and a build pass fills the new slots, so the verify warps never mix
+ * lanes that build a table with lanes that copy one.  Verdicts never depend on
+ * the table.  log2_slots: 0 = off; 8..24 = a new, empty table of 2^log2_slots
+ * slots of 576 bytes (made on the next verify_jobs call).  Default: 18
+ * (151 MB), from the tuning file's key_table_log2 or the environment
+ * variable UFSECP_B200_KEY_TABLE when set.  Slots are never evicted: when a
+ * key's probe window is full it is verified without the table.
+ * key_table_stats: out[0] lookups (items whose key parsed) and out[1] hits
+ * (items whose key already had a slot, claimed by an earlier item) since the
+ * table was made, out[2] its slot count (0 = off or not made yet). */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_key_table(ufsecp_gpu_ctx* ctx, uint32_t log2_slots);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_key_table_stats(ufsecp_gpu_ctx* ctx, uint64_t out[3]);
+
 /* Allocation-free variant of ufsecp_gpu_ext_verify_jobs, for callers that
  * cannot call cudaMalloc (GPU memory owned by another allocator or framework,
  * a fixed device-memory budget, or a policy that the verifier must not
@@ -153,22 +171,22 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_identify_invalid(ufsecp_g
  * runs, its context belongs to the server's thread: make no other call on that
  * context.  Destroy the server (it finishes the pending requests) before the
  * context.  With key_cache_log2 set, decompressed keys with their 1P..8P
- * tables stay resident in a device cache shared by the slots, so a key seen
- * before skips its square root, table additions and inversion (verdicts are
- * unchanged); off by default (on B200 it measured no faster, see the bench).  The memory
- * budget covers the slots' fixed staging (pinned + device) and the key cache,
+ * tables stay resident in a device key table shared by the slots (the design
+ * of ufsecp_gpu_ext_set_key_table), so a key seen before skips its square
+ * root, table additions and inversion (verdicts are unchanged).  The memory
+ * budget covers the slots' fixed staging (pinned + device) and the key table,
  * reserved at creation (fewer slots are made if they do not fit), plus the
  * staged bytes of the items in flight; pending requests wait for room.
  * Config NULL = defaults: 8 slots, 65,536 items per launch, an 8 GiB budget,
- * no batch window, no key cache. */
+ * no batch window, a key table of 2^18 slots. */
 typedef struct ufsecp_gpu_ext_server ufsecp_gpu_ext_server;
 typedef struct {
     uint32_t slots;                 /* streams / launches in flight, 1..64 */
     uint32_t max_launch_items;      /* 1..65536 */
     uint64_t memory_budget_bytes;
     uint32_t batch_window_us;       /* 0: launch as soon as a slot is free */
-    uint32_t key_cache_log2;        /* resident key / P-table cache of 2^k slots, 576 B each:
-                                       0 or 1 = no cache (the default), else 8..24 */
+    uint32_t key_cache_log2;        /* resident key table of 2^k slots, 576 B each:
+                                       0 or 1 = none, else 8..24 (NULL config: 18) */
 } ufsecp_gpu_ext_server_config_t;
 typedef struct {
     uint64_t requests_done, items_done, launches;

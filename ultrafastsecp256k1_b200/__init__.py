@@ -130,6 +130,8 @@ _SIGS = {
     "ufsecp_gpu_ext_server_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats), ctypes.c_int]),
     "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "ufsecp_gpu_ext_set_key_table": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_key_table_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_rlc_input_digest": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_schnorr_batch_verify": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
     "ufsecp_gpu_ext_schnorr_batch_identify_invalid": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t,
@@ -340,6 +342,16 @@ class GpuContext:
                     "verify_jobs")
         return [out_all[o:o + n] for o, n in offs]
 
+    def set_key_table(self, log2_slots: int):
+        """ufsecp_gpu_ext_set_key_table: 0 = no resident key table for verify_jobs,
+        8..24 = a new, empty table of 2^log2_slots slots."""
+        self._check(self.L.ufsecp_gpu_ext_set_key_table(self._ctx, log2_slots), "set_key_table")
+
+    def key_table_stats(self) -> dict:
+        v = (ctypes.c_uint64 * 3)()
+        self._check(self.L.ufsecp_gpu_ext_key_table_stats(self._ctx, v), "key_table_stats")
+        return {"lookups": v[0], "hits": v[1], "slots": v[2]}
+
     def schnorr_verify_rlc(self, msg_hashes32, pubkeys_x32, sigs64, batch_size: int = 0, seed32=None,
                            window_bits: int = 0):
         """ufsecp_gpu_ext_schnorr_verify_rlc: RLC batch verify with bisection.
@@ -503,8 +515,8 @@ class Server:
     of ECDSA / BIP-340 jobs from any thread, wait for their verdicts."""
 
     def __init__(self, ctx: GpuContext, slots: int = 8, max_launch_items: int = 1 << 16,
-                 memory_budget_bytes: int = 8 << 30, batch_window_us: int = 0, key_cache_log2: int = 0):
-        """key_cache_log2: 0 or 1 = no resident key cache (default), 8..24 = a cache of 2^k slots."""
+                 memory_budget_bytes: int = 8 << 30, batch_window_us: int = 0, key_cache_log2: int = 18):
+        """key_cache_log2: 0 or 1 = no resident key table, 8..24 = a table of 2^k slots (default 18)."""
         self.L = ctx.L
         self._ctx = ctx
         cfg = ServerConfig(slots, max_launch_items, memory_budget_bytes, batch_window_us, key_cache_log2)

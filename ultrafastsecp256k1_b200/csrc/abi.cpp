@@ -106,6 +106,17 @@ ufsecp_error_t guarded_out(uint8_t* out, size_t count, size_t stride, F&& run) {
     }
 }
 
+template <class F>
+ufsecp_error_t guarded_call(F&& run) {
+    try {
+        return run();
+    } catch (const std::bad_alloc&) {
+        return UFSECP_ERR_GPU_MEMORY;
+    } catch (...) {
+        return UFSECP_ERR_INTERNAL;
+    }
+}
+
 ufsecp_error_t unsupported(ufsecp_gpu_ctx* ctx, size_t count) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     if (count == 0) return UFSECP_OK;
@@ -503,6 +514,24 @@ ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_
     }
 }
 
+ufsecp_error_t ufsecp_gpu_ext_set_key_table(ufsecp_gpu_ctx* ctx, uint32_t log2_slots) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    return guarded_call([&]() -> ufsecp_error_t {
+        cudaError_t e = cudaSetDevice(ctx->backend->device());
+        if (e != cudaSuccess) return ctx->backend->cuda_error(e, "cudaSetDevice");
+        return ctx->backend->set_key_table(log2_slots);
+    });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_key_table_stats(ufsecp_gpu_ctx* ctx, uint64_t out[3]) {
+    if (!ctx || !out) return UFSECP_ERR_NULL_ARG;
+    return guarded_call([&]() -> ufsecp_error_t {
+        cudaError_t e = cudaSetDevice(ctx->backend->device());
+        if (e != cudaSuccess) return ctx->backend->cuda_error(e, "cudaSetDevice");
+        return ctx->backend->key_table_stats(&out[0], &out[1], &out[2]);
+    });
+}
+
 ufsecp_error_t ufsecp_gpu_ext_verify_jobs_noalloc(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
                                                   size_t n_jobs, void* stream) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
@@ -822,7 +851,7 @@ ufsecp_error_t ufsecp_gpu_ext_server_create(ufsecp_gpu_ctx* ctx, const ufsecp_gp
             cfg.max_launch_items = config->max_launch_items;
             cfg.memory_budget_bytes = config->memory_budget_bytes;
             cfg.batch_window_us = config->batch_window_us;
-            cfg.key_cache_log2 = config->key_cache_log2 <= 1 ? 0 : config->key_cache_log2;
+            cfg.key_cache_log2 = config->key_cache_log2 <= 1 ? 0 : config->key_cache_log2;   // NULL: the default
         }
         cudaError_t e = cudaSetDevice(ctx->backend->device());
         if (e != cudaSuccess) return ctx->backend->cuda_error(e, "cudaSetDevice");

@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include "batch.h"
+#include "keytable.h"
 #include "kernels.h"
 #include "pack_pool.h"
 #include "rlc.h"
@@ -129,6 +130,8 @@ void Backend::load_tuning() {
                     rlc_window_[size] = val;
                 if (sscanf(key, "rlc_chunk_%u", &size) == 1 && size > 0 && val >= 2 && val <= 256)
                     rlc_chunk_[size] = (uint32_t)val;
+                if (!strcmp(key, "key_table_log2") && (val == 0 || (val >= 8 && val <= 24)))
+                    key_log2_ = (uint32_t)val;
             }
             fclose(f);
         }
@@ -137,6 +140,8 @@ void Backend::load_tuning() {
     // near what the device consumes at full speed), 2 on 4+ cores
     const unsigned hw = std::thread::hardware_concurrency();
     pack_threads_ = hw >= 8 ? 4 : (hw >= 4 ? 2 : 1);
+    const int kt = env_int("UFSECP_B200_KEY_TABLE", -1);
+    if (kt == 0 || (kt >= 8 && kt <= 24)) key_log2_ = (uint32_t)kt;
     const int pt = env_int("UFSECP_B200_PACK_THREADS", 0);
     if (pt >= 1 && pt <= 16) pack_threads_ = pt;
     const int rc_env = env_int("UFSECP_B200_RLC_CHUNK", 0);
@@ -223,6 +228,7 @@ RlcVerifier& Backend::rlc() {
 Backend::~Backend() {
     batch_[0].reset();
     batch_[1].reset();
+    keys_.reset();
     if (dev_ >= 0) cudaSetDevice(dev_);
     rlc_.reset();
     if (dev_ >= 0) {
@@ -449,13 +455,41 @@ int Backend::sign_device(int kind, const uint8_t* d_msgs, const uint8_t* d_sks, 
     return kOk;
 }
 
+int Backend::set_key_table(uint32_t log2) {
+    if (log2 != 0 && (log2 < KeyTable::kMinLog2 || log2 > KeyTable::kMaxLog2))
+        return set_error(kErrBadInput, "key table: log2 slots must be 0 or 8..24");
+    // the batch slots' captured graphs hold the old table's pointers
+    batch_[0].reset();
+    batch_[1].reset();
+    keys_.reset();
+    key_log2_ = log2;
+    clear_error();
+    return kOk;
+}
+
+int Backend::key_table_stats(uint64_t* lookups, uint64_t* hits, uint64_t* slots) {
+    *lookups = *hits = *slots = 0;
+    if (!keys_ || !keys_->on()) return kOk;
+    *slots = keys_->slot_count();
+    const cudaError_t e = keys_->read_counters(lookups, hits);
+    if (e != cudaSuccess) return cuda_error(e, "key table counters");
+    return kOk;
+}
+
 int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
     if (!ready_) return set_error(kErrGpuDevice, "context not ready");
+    if (key_log2_ && !keys_) {
+        auto kt = std::make_unique<KeyTable>();
+        const int rc = kt->create(this, key_log2_);
+        if (rc != kOk) return rc;
+        keys_ = std::move(kt);
+    }
     for (int q = 0; q < 2; ++q) {
         if (!batch_[q]) {
             auto slot = std::make_unique<BatchSlot>();
             const int rc = slot->init(this);
             if (rc != kOk) return rc;
+            if (keys_) slot->set_cache(keys_->slots(), keys_->mask(), keys_->counters());
             batch_[q] = std::move(slot);
         }
         if (q == 0) {

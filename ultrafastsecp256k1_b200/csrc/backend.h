@@ -44,6 +44,7 @@ struct VerifyJob;
 class BatchSlot;
 class RlcVerifier;
 class PackPool;
+class KeyTable;
 
 class Backend {
 public:
@@ -76,8 +77,16 @@ public:
     int sign_device(int kind, const uint8_t* d_msgs, const uint8_t* d_sks, const uint8_t* d_auxs, size_t count,
                     uint8_t* d_pubs, uint8_t* d_sigs, uint8_t* d_ok, cudaStream_t stream);
     // Mixed ECDSA / BIP-340 jobs (host buffers) in one persistent-queue launch;
-    // synchronous.
+    // synchronous.  Keys go through the context's resident key table when it
+    // is on (set_key_table).
     int verify_jobs(const VerifyJob* jobs, size_t n_jobs);
+    // Resident key table of verify_jobs: 0 = off, 8..24 = a new, empty table
+    // of 2^log2 slots (made on the next verify_jobs call).  The default is the
+    // tuning file's key_table_log2, else UFSECP_B200_KEY_TABLE, else 18.
+    int set_key_table(uint32_t log2);
+    uint32_t key_table_log2() const { return key_log2_; }
+    // lookups, hits since the table was made; slots (0 = off / not made yet)
+    int key_table_stats(uint64_t* lookups, uint64_t* hits, uint64_t* slots);
     // RLC batch verifier of BIP-340 signatures (created on first use).
     RlcVerifier& rlc();
     // Pippenger window bits for an RLC segment of `len` items: the tuned value
@@ -167,6 +176,8 @@ private:
     int queue_grid_ = 0;
     int queue_pair_grid_ = 0;
     std::unique_ptr<BatchSlot> batch_[2];   // slots of the synchronous mixed-batch call (two for large calls)
+    std::unique_ptr<KeyTable> keys_;        // resident key table of verify_jobs (made on first use)
+    uint32_t key_log2_ = 18;
     std::unique_ptr<RlcVerifier> rlc_;
     std::map<uint32_t, int> rlc_window_;   // tuned window bits per RLC batch size
     std::map<uint32_t, uint32_t> rlc_chunk_;  // tuned bucket points per chunk thread per RLC batch size

@@ -73,18 +73,18 @@ int BatchSlot::init(Backend* be, bool use_graphs) {
     if (e == cudaSuccess && use_graphs) {
         // the graph buckets all bind this one staging pair, sized for the largest bucket
         const QueueLayout maxl(kGraphMaxItems, kGraphMaxItems);
-        e = pinned_.ensure(maxl.total);
+        e = pinned_.ensure(maxl.host_bytes);
         if (e == cudaSuccess) e = dev_.ensure(maxl.total);
     }
     if (e != cudaSuccess) return be->cuda_error(e, "batch slot init");
     return kOk;
 }
 
-// Small layouts without the key cache run two lanes per signature (the
-// backend's tuned limit); the choice is part of the graph key, so a changed
-// limit never replays a graph captured with the other kernels.
+// Small layouts run two lanes per signature (the backend's tuned limit); the
+// choice is part of the graph key, so a changed limit never replays a graph
+// captured with the other kernels.
 bool BatchSlot::two_lanes(const QueueArgs& a) const {
-    return !a.cache && (uint64_t)a.cap_e + a.cap_s <= be_->queue_pair_items();
+    return (uint64_t)a.cap_e + a.cap_s <= be_->queue_pair_items();
 }
 
 uint64_t BatchSlot::graph_key(const QueueArgs& a) const {
@@ -107,6 +107,12 @@ QueueArgs BatchSlot::args_for(uint8_t* d) const {
     a.cache = cache_;
     a.cache_mask = cache_mask_;
     a.cache_stats = cache_stats_;
+    if (cache_) {
+        a.e_slot = reinterpret_cast<uint32_t*>(d + layout_.e_slot);
+        a.s_slot = reinterpret_cast<uint32_t*>(d + layout_.s_slot);
+        a.todo = reinterpret_cast<uint32_t*>(d + layout_.todo);
+        a.todo_count = reinterpret_cast<uint32_t*>(d) + 2;
+    }
     return a;
 }
 
@@ -160,13 +166,14 @@ int BatchSlot::enqueue(const VerifyJob* jobs, size_t n_jobs) {
     } else {
         layout_ = QueueLayout((uint32_t)n_e, (uint32_t)n_s);
         staged_big_ = true;
-        if ((e = big_pinned_.ensure(layout_.total)) != cudaSuccess) return be_->cuda_error(e, "cudaHostAlloc");
+        if ((e = big_pinned_.ensure(layout_.host_bytes)) != cudaSuccess) return be_->cuda_error(e, "cudaHostAlloc");
         if ((e = big_dev_.ensure(layout_.total)) != cudaSuccess) return be_->cuda_error(e, "cudaMalloc");
     }
     uint8_t* h = staged_big_ ? (uint8_t*)big_pinned_.p : (uint8_t*)pinned_.p;
     uint32_t* hdr = reinterpret_cast<uint32_t*>(h);
     hdr[0] = (uint32_t)n_e;
     hdr[1] = (uint32_t)n_s;
+    hdr[2] = 0;   // the key table's to-do count
     size_t oe = 0, os = 0;
     for (size_t j = 0; j < n_jobs; ++j) {
         const VerifyJob& J = jobs[j];
@@ -206,6 +213,7 @@ int BatchSlot::prewarm(uint32_t max_items) {
             uint32_t* hdr = reinterpret_cast<uint32_t*>(pinned_.p);
             hdr[0] = 0;
             hdr[1] = 0;
+            hdr[2] = 0;
             const QueueArgs a = args_for((uint8_t*)dev_.p);
             const int rc = run_graph(a, graph_key(a));
             if (rc != kOk) return rc;

@@ -57,8 +57,9 @@ public:
     // Waits for the enqueued work and writes every job's verdicts.
     int finish(const VerifyJob* jobs, size_t n_jobs);
 
-    // Resident key / table cache for the queue kernel (kernels.h QueueArgs);
-    // set before the first enqueue: captured graphs keep the pointers.
+    // Resident key table for the queue kernels (kernels.h QueueArgs,
+    // pubcache.cuh); set before the first enqueue: captured graphs keep the
+    // pointers.
     void set_cache(PubCacheSlot* slots, uint32_t mask, unsigned long long* stats) {
         cache_ = slots;
         cache_mask_ = mask;

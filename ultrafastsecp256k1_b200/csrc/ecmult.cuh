@@ -130,12 +130,12 @@ UF_HD void add_gtab(Jac& R, const GT& gt, int d, bool sneg, int lam) {
 }
 
 // R = a*G + b*P for P = (px, py) on the curve (not infinity).  With
-// have_tab the caller already filled `tab` (a cached key) and px, py are not
+// have_tab the caller already filled `tab` (a resident key) and px, py are not
 // read; otherwise the table is built here, after the digit recoding (the order
-// that keeps the kernel at 3 blocks per SM), and offered to `cache`.
-template <class Tab, class GT, class Cache>
+// that keeps the kernel at 3 blocks per SM).
+template <class Tab, class GT>
 UF_HDI void dual_mul_c(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt,
-                       bool have_tab, const Cache& cache, bool odd) {
+                       bool have_tab) {
     GlvSplit sa, sb;
     glv_split(sa, a);
     glv_split(sb, b);
@@ -145,10 +145,7 @@ UF_HDI void dual_mul_c(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc
     booth_recode<kWP, kNWP>(dp2, sb.k2);
     booth_recode<kWG, kNWG>(dg1, sa.k1);
     booth_recode<kWG, kNWG>(dg2, sa.k2);
-    if (!have_tab) {
-        build_ptable(tab, px, py);
-        cache.put(px, odd, tab);
-    }
+    if (!have_tab) build_ptable(tab, px, py);
     Fe beta;
     fe_beta(beta);
     jac_set_inf(R);
@@ -168,10 +165,11 @@ UF_HDI void dual_mul_c(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc
 // sums the a1*G and b1*P streams, half 1 the a2*(lambda G) and b2*(lambda P)
 // streams (the GLV halves), each with the full 128 doublings, so that the two
 // partial sums add up to R.  Both lanes build the same P table in their own
-// shared-memory slots (the same instruction stream, so no divergence).
+// shared-memory slots (the same instruction stream, so no divergence), unless
+// have_tab says the caller already filled `tab`.
 template <class Tab, class GT>
 UF_HDI void dual_mul_half(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt,
-                          int half) {
+                          int half, bool have_tab = false) {
     GlvSplit sa, sb;
     glv_split(sa, a);
     glv_split(sb, b);
@@ -186,7 +184,7 @@ UF_HDI void dual_mul_half(Jac& R, const Sc& a, const Fe& px, const Fe& py, const
     GDigit dg[kNWG];
     booth_recode<kWP, kNWP>(dp, kp);
     booth_recode<kWG, kNWG>(dg, kg);
-    build_ptable(tab, px, py);
+    if (!have_tab) build_ptable(tab, px, py);
     Fe beta;
     fe_beta(beta);
     jac_set_inf(R);
@@ -200,7 +198,7 @@ UF_HDI void dual_mul_half(Jac& R, const Sc& a, const Fe& px, const Fe& py, const
 
 template <class Tab, class GT>
 UF_HDI void dual_mul(Jac& R, const Sc& a, const Fe& px, const Fe& py, const Sc& b, Tab& tab, const GT& gt) {
-    dual_mul_c(R, a, px, py, b, tab, gt, false, NoPubCache(), false);
+    dual_mul_c(R, a, px, py, b, tab, gt, false);
 }
 
 }  // namespace uf

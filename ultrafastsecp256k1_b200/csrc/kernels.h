@@ -71,14 +71,18 @@ cudaError_t launch_tagged_hash(const uint8_t tag_hash[32], const uint8_t* msgs, 
                                cudaStream_t s);
 
 // Mixed-batch staging layout shared by host (pinned) and device buffers:
-//   [header 256 B: counts n_e, n_s][e_msgs cap_e*32][s_msgs cap_s*32]
+//   [header 256 B: n_e, n_s, to-do count][e_msgs cap_e*32][s_msgs cap_s*32]
 //   [e_sigs cap_e*64][s_sigs cap_s*64][s_pubs cap_s*32][e_pubs cap_e*33]
 //   [e_out cap_e][s_out cap_s]
+// then, on the device only, the key table's per-launch scratch:
+//   [e_slot cap_e*4][s_slot cap_s*4][todo (cap_e+cap_s)*4]
 // Every region starts 256-byte aligned.  in_bytes covers header + inputs (one
-// host->device copy), out_bytes the verdicts (one device->host copy).
+// host->device copy), out_bytes the verdicts (one device->host copy),
+// host_bytes the pinned staging, total the device buffer.
 struct QueueLayout {
     uint32_t cap_e = 0, cap_s = 0;
-    size_t e_msgs, s_msgs, e_sigs, s_sigs, s_pubs, e_pubs, e_out, s_out, in_bytes, out_bytes, total;
+    size_t e_msgs, s_msgs, e_sigs, s_sigs, s_pubs, e_pubs, e_out, s_out, e_slot, s_slot, todo, in_bytes, out_bytes,
+        host_bytes, total;
     static size_t up(size_t x) { return (x + 255) & ~size_t{255}; }
     QueueLayout() = default;
     QueueLayout(uint32_t ce, uint32_t cs) : cap_e(ce), cap_s(cs) {
@@ -90,23 +94,30 @@ struct QueueLayout {
         e_pubs = up(s_pubs + (size_t)cs * 32);
         e_out = up(e_pubs + (size_t)ce * 33);
         s_out = up(e_out + (size_t)ce);
-        total = up(s_out + (size_t)cs);
+        e_slot = up(s_out + (size_t)cs);
+        s_slot = up(e_slot + (size_t)ce * 4);
+        todo = up(s_slot + (size_t)cs * 4);
+        total = up(todo + ((size_t)ce + cs) * 4);
         in_bytes = e_out;
-        out_bytes = total - e_out;
+        out_bytes = e_slot - e_out;
+        host_bytes = e_slot;
     }
 };
 
 struct PubCacheSlot;
 struct QueueArgs {
-    const uint32_t* counts;  // device header: n_e, n_s
+    const uint32_t* counts;  // device header: n_e, n_s, to-do count
     uint32_t cap_e, cap_s;   // region capacities: the kernel never reads past them
     const uint8_t *e_msgs, *e_pubs, *e_sigs, *s_msgs, *s_pubs, *s_sigs;
     uint8_t *e_out, *s_out;
-    // optional resident key / table cache (pubcache.cuh): slots, slot count - 1,
-    // and two counters (lookups, hits); null = no cache
+    // optional resident key table (pubcache.cuh): slots, slot count - 1, two
+    // counters (lookups, hits); the launch's per-item slot indices and to-do
+    // list (device-only regions of the layout) and its to-do counter (header
+    // word 2, zeroed by the host copy); null cache = no table
     PubCacheSlot* cache = nullptr;
     uint32_t cache_mask = 0;
     unsigned long long* cache_stats = nullptr;
+    uint32_t *e_slot = nullptr, *s_slot = nullptr, *todo = nullptr, *todo_count = nullptr;
 };
 constexpr size_t kPubCacheSlotBytes = 576;
 
@@ -114,10 +125,15 @@ constexpr size_t kPubCacheSlotBytes = 576;
 // launches the per-kind persistent queue kernels (`grid` resident blocks
 // each) over the items described by `a`: kinds with capacity 0 are skipped;
 // with both kinds, the BIP-340 kernel runs on s2 between a fork event recorded
-// on s and a join event s waits for (kernels_queue.cu).
+// on s and a join event s waits for (kernels_queue.cu).  With a key table
+// (a.cache) the resolve and build passes (pubcache.cuh) run first, on s.
 cudaError_t launch_verify_queue(const QueueArgs& a, const void* d_gtab, unsigned int* d_head, int grid,
                                 cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
 int verify_queue_occupancy();
+// The key table's resolve and build passes alone (launch_verify_queue and
+// launch_verify_queue_pair call it when a.cache is set); `grid` resident blocks
+// for the build pass.
+cudaError_t launch_key_passes(const QueueArgs& a, int grid, cudaStream_t s);
 
 // Two lanes per signature (kernels_pair.cu), kind 0 ECDSA (compact) or 1
 // BIP-340, for small calls; verify_pair_occupancy() also opts the kernels in

@@ -46,10 +46,13 @@ __device__ __forceinline__ Jac shfl_partner(const Jac& a) {
 // must call it: it ends with warp shuffles.  The verdict is meaningful on the
 // even lane (half 0).
 // kKind 0: ECDSA (compact r || s, low-S), 1: BIP-340.
-template <int kKind>
+// `cache` (SlotPubCache / NoPubCache) may supply the key's table (both lanes
+// copy it into their own shared-memory columns) or know the key to be off the
+// curve.
+template <int kKind, class Cache>
 __device__ __forceinline__ bool pair_item(const uint8_t* msg, const uint8_t* pub, const uint8_t* sig, bool valid,
-                                          int half, const SmemTab& tab, const GlobalGT& g) {
-    bool ok = valid;
+                                          int half, const SmemTab& tab, const GlobalGT& g, const Cache& cache) {
+    bool ok = valid, have_tab = false;
     Sc r, s, a, b;        // r kept for the ECDSA check
     uint32_t rb[8];       // BIP-340: r as limbs
     Fe px, py;
@@ -67,7 +70,12 @@ __device__ __forceinline__ bool pair_item(const uint8_t* msg, const uint8_t* pub
             ok = ok && (prefix == 0x02 || prefix == 0x03);
             if (ok) {
                 be32_to_limbs(px.v, pub + 1);
-                ok = limbs_lt_p(px.v) && lift_x_parity(py, px, prefix == 0x03);
+                ok = limbs_lt_p(px.v);
+            }
+            if (ok) {
+                const int c = cache.fetch(tab);
+                have_tab = c == kKeyTable;
+                ok = c != kKeyBad && (have_tab || lift_x_parity(py, px, prefix == 0x03));
             }
             if (ok) {
                 Sc z, w;
@@ -86,7 +94,12 @@ __device__ __forceinline__ bool pair_item(const uint8_t* msg, const uint8_t* pub
             ok = limbs_lt_p(rb) && !sc_is_zero(a) && limbs_lt_n(a.v);
             if (ok) {
                 words_be_to_limbs(px.v, pw);
-                ok = limbs_lt_p(px.v) && lift_x_parity(py, px, false);
+                ok = limbs_lt_p(px.v);
+            }
+            if (ok) {
+                const int c = cache.fetch(tab);
+                have_tab = c == kKeyTable;
+                ok = c != kKeyBad && (have_tab || lift_x_parity(py, px, false));
             }
             if (ok) {
                 uint32_t rbe[8], pbe[8], mbe[8], h[8];
@@ -107,7 +120,7 @@ __device__ __forceinline__ bool pair_item(const uint8_t* msg, const uint8_t* pub
     }
     Jac R;
     jac_set_inf(R);
-    if (ok) dual_mul_half(R, a, px, py, b, tab, g, half);
+    if (ok) dual_mul_half(R, a, px, py, b, tab, g, half, have_tab);
     const Jac other = shfl_partner(R);     // every lane of the warp arrives here
     if (ok && half == 0) {
         jac_add(R, other);
@@ -131,7 +144,7 @@ k_verify_pair(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs
     const bool valid = i < n;
     const uint32_t j = valid ? i : 0;      // an in-bounds index for the (unused) pointers
     const bool ok = pair_item<kKind>(msgs + 32ull * j, pubs + (kKind == 0 ? 33ull : 32ull) * j, sigs + 64ull * j,
-                                     valid, half, tab, g);
+                                     valid, half, tab, g, NoPubCache());
     if (valid && half == 0) {
         if (collect) {
             if (ok) out[i] = 0;
@@ -141,10 +154,11 @@ k_verify_pair(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ pubs
     }
 }
 
-// The work-queue form (the per-kind queues of kernels_queue.cu, without the
-// key cache): each warp claims 16 items and verifies them with its 16 lane
-// pairs, until its queue is empty.  The claim is warp-uniform, so every lane
-// reaches the shuffles of each round.
+// The work-queue form (the per-kind queues of kernels_queue.cu): each warp
+// claims 16 items and verifies them with its 16 lane pairs, until its queue is
+// empty.  The claim is warp-uniform, so every lane reaches the shuffles of each
+// round.  With the key table (a.cache) an item's table comes from its resolved
+// slot.
 template <int kKind>
 __global__ void __launch_bounds__(kPairThreads)
 k_verify_queue_pair(QueueArgs a, const uint4* __restrict__ gt, unsigned int* __restrict__ head) {
@@ -165,8 +179,10 @@ k_verify_queue_pair(QueueArgs a, const uint4* __restrict__ gt, unsigned int* __r
         const uint32_t i = base + (lane >> 1);
         const bool valid = i < total;
         const uint32_t j = valid ? i : 0;
+        const uint32_t si = a.cache && valid ? (kKind == 0 ? a.e_slot : a.s_slot)[i] : kNoSlot;
         const bool ok = pair_item<kKind>(msgs + 32ull * j, pubs + (kKind == 0 ? 33ull : 32ull) * j, sigs + 64ull * j,
-                                         valid, (int)(lane & 1u), tab, g);
+                                         valid, (int)(lane & 1u), tab, g,
+                                         SlotPubCache{si == kNoSlot ? nullptr : a.cache + si});
         if (valid && (lane & 1u) == 0) out[i] = ok ? 1 : 0;
     }
 }
@@ -194,6 +210,7 @@ cudaError_t launch_verify_queue_pair(const QueueArgs& a, const void* d_gtab, uns
     const uint4* gt = reinterpret_cast<const uint4*>(d_gtab);
     cudaError_t e = cudaMemsetAsync(d_head, 0, 2 * sizeof(unsigned int), s);
     if (e != cudaSuccess) return e;
+    if ((e = launch_key_passes(a, grid, s)) != cudaSuccess) return e;
     const bool both = a.cap_e > 0 && a.cap_s > 0;
     if (both) {
         if ((e = cudaEventRecord(fork, s)) != cudaSuccess) return e;

@@ -15,7 +15,7 @@ Server::~Server() {
     cv_work_.notify_all();
     if (thread_.joinable()) thread_.join();
     launches_.clear();
-    if (d_cache_) cudaFree(d_cache_);
+    keys_.release();
 }
 
 int Server::start(const ServerConfig& cfg) {
@@ -27,23 +27,19 @@ int Server::start(const ServerConfig& cfg) {
         return be_->set_error(kErrBadInput, "max_launch_items must be 1..65536");
     // every slot holds pinned + device staging for its largest graph bucket
     const QueueLayout maxl(BatchSlot::kGraphMaxItems, BatchSlot::kGraphMaxItems);
-    const uint64_t slot_bytes = 2ull * maxl.total;
-    if (cfg_.key_cache_log2 != 0 && (cfg_.key_cache_log2 < 8 || cfg_.key_cache_log2 > 24))
+    const uint64_t slot_bytes = (uint64_t)maxl.host_bytes + maxl.total;
+    if (cfg_.key_cache_log2 != 0 &&
+        (cfg_.key_cache_log2 < KeyTable::kMinLog2 || cfg_.key_cache_log2 > KeyTable::kMaxLog2))
         return be_->set_error(kErrBadInput, "key_cache_log2 must be 0 or 8..24");
-    const uint64_t cache_slots = cfg_.key_cache_log2 ? (1ull << cfg_.key_cache_log2) : 0;
-    const uint64_t cache_bytes = cache_slots * kPubCacheSlotBytes + (cache_slots ? 256 : 0);
+    const uint64_t cache_bytes =
+        cfg_.key_cache_log2 ? (kPubCacheSlotBytes << cfg_.key_cache_log2) + 256 : 0;
     if (cfg_.memory_budget_bytes < slot_bytes + cache_bytes)
         return be_->set_error(kErrBadInput, "memory budget below one slot and the key cache");
     cfg_.slots = (uint32_t)std::min<uint64_t>(
         cfg_.slots, std::max<uint64_t>(1, (cfg_.memory_budget_bytes - cache_bytes) / slot_bytes));
-    if (cache_slots) {
-        cudaError_t e = cudaMalloc(&d_cache_, cache_bytes);
-        if (e == cudaSuccess) e = cudaMemset(d_cache_, 0, cache_bytes);
-        if (e != cudaSuccess) {
-            if (d_cache_) cudaFree(d_cache_);
-            d_cache_ = nullptr;
-            return be_->cuda_error(e, "key cache");
-        }
+    if (cfg_.key_cache_log2) {
+        const int rc = keys_.create(be_, cfg_.key_cache_log2);
+        if (rc != kOk) return rc;
     }
     launches_.resize(cfg_.slots);
     for (auto& L : launches_) {
@@ -53,9 +49,7 @@ int Server::start(const ServerConfig& cfg) {
             launches_.clear();
             return rc;
         }
-        if (d_cache_)
-            L.slot->set_cache((PubCacheSlot*)d_cache_, (uint32_t)(cache_slots - 1),
-                              (unsigned long long*)((uint8_t*)d_cache_ + cache_slots * kPubCacheSlotBytes));
+        if (keys_.on()) L.slot->set_cache(keys_.slots(), keys_.mask(), keys_.counters());
         // instantiate every launch shape now, not on a request's critical path
         const int pw = L.slot->prewarm(cfg_.max_launch_items);
         if (pw != kOk) {
@@ -231,15 +225,7 @@ void Server::stats(ServerStats* out, bool reset) {
     s.launches = n_launches_;
     s.peak_budget_bytes = peak_budget_;
     s.reserved_bytes = reserved_;
-    if (d_cache_) {
-        const uint64_t slots = 1ull << cfg_.key_cache_log2;
-        unsigned long long c[2] = {0, 0};
-        if (cudaMemcpy(c, (uint8_t*)d_cache_ + slots * kPubCacheSlotBytes, sizeof(c), cudaMemcpyDeviceToHost) ==
-            cudaSuccess) {
-            s.cache_lookups = c[0];
-            s.cache_hits = c[1];
-        }
-    }
+    if (keys_.on()) (void)keys_.read_counters(&s.cache_lookups, &s.cache_hits);
     s.peak_slots_in_flight = peak_in_flight_;
     s.pending_requests = pending_.size();
     s.busy_s = busy_s_;

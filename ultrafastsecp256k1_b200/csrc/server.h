@@ -13,9 +13,10 @@
 // Admission is bounded by a memory budget: the slots' fixed staging (pinned +
 // device, reserved at start) plus the staged bytes of the items of every launch
 // in flight stay within memory_budget_bytes.  Decompressed keys and their
-// 1P..8P tables stay resident in a device cache shared by all slots
-// (pubcache.cuh), so repeated keys skip decompression and table set-up.  The verdicts
-// of a request are the per-kind verify's, whatever it is batched with.
+// 1P..8P tables stay resident in a device key table shared by all slots
+// (pubcache.cuh, keytable.h), so repeated keys skip decompression and table
+// set-up.  The verdicts of a request are the per-kind verify's, whatever it is
+// batched with.
 #pragma once
 #include <stddef.h>
 #include <stdint.h>
@@ -31,6 +32,7 @@
 
 #include "backend.h"
 #include "batch.h"
+#include "keytable.h"
 
 namespace uf {
 
@@ -39,7 +41,7 @@ struct ServerConfig {
     uint32_t max_launch_items = 1u << 16;
     uint64_t memory_budget_bytes = 8ull << 30;
     uint32_t batch_window_us = 0;     // wait this long for more work before launching a small batch
-    uint32_t key_cache_log2 = 0;      // resident key / table cache of 2^k slots (576 B each); 0 = none
+    uint32_t key_cache_log2 = 18;     // resident key table of 2^k slots (576 B each); 0 = none
 };
 
 struct ServerStats {
@@ -98,7 +100,8 @@ private:
     void loop();
     bool admit(Launch& L);               // under mu_
     void complete(Launch& L, int rc);    // under mu_
-    static size_t bytes_per_item(int kind) { return 2 * (32 + (kind == 0 ? 33 : 32) + 64 + 1); }
+    // pinned + device staging of one item, and its key-table slot index and to-do entry
+    static size_t bytes_per_item(int kind) { return 2 * (32 + (kind == 0 ? 33 : 32) + 64 + 1) + 8; }
 
     Backend* be_;
     ServerConfig cfg_;
@@ -111,7 +114,7 @@ private:
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs_;
     std::vector<Launch> launches_;
     uint64_t budget_used_ = 0, reserved_ = 0;
-    void* d_cache_ = nullptr;        // key cache slots, then 2 counters
+    KeyTable keys_;                  // resident key table shared by the slots
     // statistics
     std::vector<double> lat_us_;
     uint64_t items_done_ = 0, n_launches_ = 0, peak_budget_ = 0;

@@ -63,8 +63,9 @@ UF_HDI bool schnorr_check(const Jac& R, const uint32_t r[8]) {
 }
 
 // ECDSA after the signature's scalars are parsed (r, s in [1, n-1]).  `cache`
-// (PubCache / NoPubCache) may supply the key's table instead of decompressing
-// the key and building it.
+// (SlotPubCache / NoPubCache, pubcache.cuh) may supply the key's table instead
+// of decompressing the key and building it, or know the key to be off the
+// curve.
 template <class Tab, class GT, class Cache = NoPubCache>
 UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const Sc& r, const Sc& s, Tab& tab,
                             const GT& gt, const Cache& cache = Cache()) {
@@ -73,7 +74,9 @@ UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const
     Fe qx, qy;
     be32_to_limbs(qx.v, pub33 + 1);
     if (!limbs_lt_p(qx.v)) return false;
-    const bool cached = cache.fetch(qx, prefix == 0x03, tab);
+    const int c = cache.fetch(tab);
+    if (c == kKeyBad) return false;
+    const bool cached = c == kKeyTable;
     if (!cached && !lift_x_parity(qy, qx, prefix == 0x03)) return false;
     Sc z, w, u1, u2;
     words_be_to_limbs(z.v, msg_w);
@@ -82,7 +85,7 @@ UF_HDI bool ecdsa_verify_rs(const uint32_t msg_w[8], const uint8_t* pub33, const
     sc_mul(u1, z, w);
     sc_mul(u2, r, w);
     Jac R;
-    dual_mul_c(R, u1, qx, qy, u2, tab, gt, cached, cache, prefix == 0x03);
+    dual_mul_c(R, u1, qx, qy, u2, tab, gt, cached);
     return ecdsa_check_x(R, r);
 }
 
@@ -132,7 +135,9 @@ UF_HDI bool schnorr_verify_one(const uint32_t msg_w[8], const uint32_t px_w[8], 
     Fe px, py;
     words_be_to_limbs(px.v, px_w);
     if (!limbs_lt_p(px.v)) return false;
-    const bool cached = cache.fetch(px, false, tab);
+    const int c = cache.fetch(tab);
+    if (c == kKeyBad) return false;
+    const bool cached = c == kKeyTable;
     if (!cached && !lift_x_parity(py, px, false)) return false;
     uint32_t rbe[8], pbe[8], mbe[8], h[8];
     UF_UNROLL
@@ -148,7 +153,7 @@ UF_HDI bool schnorr_verify_one(const uint32_t msg_w[8], const uint32_t px_w[8], 
     sc_reduce_once(e);
     sc_neg(ne, e);
     Jac R;
-    dual_mul_c(R, s, px, py, ne, tab, gt, cached, cache, false);
+    dual_mul_c(R, s, px, py, ne, tab, gt, cached);
     return schnorr_check(R, r);
 }
 

@@ -46,7 +46,7 @@ P_FIELD = 2**256 - 2**32 - 977
 W_SIG = 3.33e5            # IMAD-class ops per verified signature (canonical work model)
 BYTES_PER_SIG = 32 + 32 + 64 + 1
 BATCH = 1 << 20
-CPU_SAMPLE = 200_000
+CPU_SAMPLE = 1 << 20            # the whole headline batch
 
 
 def parse():
@@ -339,28 +339,34 @@ def run_ours(args):
     e2e_agree = int((res == expect).sum())
 
     # ---- secondary: plain ECDSA on 4096 and 2^20 signatures ---------------
-    ecdsa_rate = ecdsa_big = None
+    c1 = ecdsa_big = None
     mixed = None
     rlc = None
     serving = None
     if rank == 0:
-        ecdsa_rate = ecdsa_4096_rate(ctx, torch)
+        try:
+            c1 = bench_c1(ctx, torch)
+        except Exception as e:   # reference library missing on this box
+            c1 = {"unavailable": str(e)}
         if not args.no_secondary:
-            ecdsa_big = ecdsa_4096_rate(ctx, torch, n=1 << 20, reps=3)
+            ecdsa_big = ecdsa_plain_rate(ctx, torch, n=1 << 20, reps=3)
             mixed = bench_mixed(ctx, torch)
             rlc = bench_rlc(ctx, torch)
             serving = bench_serving(ctx, torch)
 
     # ---- CPU baseline (rank 0, one GPU only) --------------------------------
     cpu = None
+    ref_agree = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
+            # every item of the batch: the CPU baseline's sample and the full verdict check at once
             sample = min(CPU_SAMPLE, n)
             rate, threads, verdicts, dt = cpu_reference_rate(msgs, xs, sigs, sample)
+            ref_agree = float((verdicts == d_out.cpu().numpy()[:sample]).mean())
             cpu = {"value": rate, "unit": "sigs/s", "cores": threads, "kind": "reference",
-                   "sample": f"first {sample:,} signatures of the 1,048,576-signature BIP-340 batch "
-                             f"({dt:.1f} s wall), ufsecp_schnorr_verify per signature, one ufsecp_ctx per thread",
-                   "verdicts_equal_gpu": bool((verdicts == d_out.cpu().numpy()[:sample]).all())}
+                   "sample": f"all {sample:,} signatures of the BIP-340 batch ({dt:.1f} s wall), "
+                             "ufsecp_schnorr_verify per signature, one ufsecp_ctx per thread",
+                   "verdicts_equal_gpu": ref_agree == 1.0}
         except Exception as e:  # reference library missing on this box
             cpu = {"value": None, "unit": "sigs/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"}
@@ -397,8 +403,11 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": args.steps * launches_per_call(n),
-            "verdict_agreement": agree / n,
-            "secondary": {"ecdsa_4096_plain_sigs_per_s": ecdsa_rate, "ecdsa_1048576_plain_sigs_per_s": ecdsa_big,
+            "verdict_agreement": ref_agree if ref_agree is not None else agree / n,
+            "verdict_agreement_source": ("reference library, every item of the batch" if ref_agree is not None
+                                         else "construction (reference library unavailable)"),
+            "verdict_agreement_construction": agree / n,
+            "secondary": {"ecdsa_4096": c1, "ecdsa_1048576_plain_sigs_per_s": ecdsa_big,
                           "mixed_batches": mixed, "rlc_batch_verify": rlc,
                           "serving": serving},
         }
@@ -448,22 +457,39 @@ def mixed_workload(ctx, torch, n_batches=2000, seed=3, pool=100_000):
     bounds = np.concatenate([[0], np.cumsum(sizes)])
     pos = {0: np.searchsorted(out[0][0], bounds), 1: np.searchsorted(out[1][0], bounds)}
     batches = []
+    kinds_j, starts_j, counts_j = [], [], []
     for b in range(n_batches):
         parts = []
         for kind in (0, 1):
             lo, hi = pos[kind][b], pos[kind][b + 1]
             sel, m, p, s, ex = out[kind]
             parts.append((kind, m[lo:hi], p[lo:hi], s[lo:hi], ex[lo:hi]))
+            kinds_j.append(kind)
+            starts_j.append(lo)
+            counts_j.append(hi - lo)
         batches.append(parts)
-    return batches, total
+    # the same jobs as index ranges of the two per-kind corpora
+    corpora = {k: tuple(np.ascontiguousarray(a) for a in out[k][1:4]) for k in (0, 1)}
+    expects = {k: out[k][4] for k in (0, 1)}
+    ranges = (np.array(kinds_j), np.array(starts_j), np.array(counts_j))
+    return batches, total, corpora, expects, ranges
 
 
 def bench_mixed(ctx, torch):
-    """Per-batch plain ABI calls against one-launch batched jobs, same batches.
-    Each form runs once untimed first (first-use set-up: staging buffers,
-    batch slot, streams), then once timed."""
+    """The mixed-batch workload (2000 caller batches) five ways, same items:
+    one plain ABI call per batch and kind; ufsecp_gpu_ext_verify_jobs over
+    groups of >= 262,144 signatures and over all 2000 batches in one call (job
+    lists marshalled per job in Python); the one call with the job table built
+    by vector operations from index ranges (what a C / C++ caller pays), with
+    the resident key table cold (emptied just before), warm (every key resident
+    from the previous call) and off; and the plain one-signature-per-thread
+    kernel over the same items already on the device (one launch per kind,
+    CUDA events): the ceiling a batched form has to beat.  Each host form runs
+    once untimed first (staging buffers, batch slots, streams, graphs), then
+    once timed.  Verdicts: every form against the construction, and every item
+    against the reference library on the host cores."""
     import time as _t
-    batches, total = mixed_workload(ctx, torch)
+    batches, total, corpora, expects, (kinds_j, starts_j, counts_j) = mixed_workload(ctx, torch)
 
     def plain_pass():
         # the reference-style synchronous call per batch and kind; verdicts
@@ -511,15 +537,63 @@ def bench_mixed(ctx, torch):
         dt = _t.perf_counter() - t0
         return dt, sum(int((o == ex).sum()) for o, ex in zip(got, exps))
 
+    def ranges_pass():
+        t0 = _t.perf_counter()
+        got = ctx.verify_job_ranges(corpora, kinds_j, starts_j, counts_j)
+        dt = _t.perf_counter() - t0
+        return dt, sum(int((got[k] == expects[k]).sum()) for k in (0, 1)), got
+
     plain_pass()
     t_plain, agree = plain_pass()
     batched_pass()
     t_batched, agree_b = batched_pass()
     one_call_pass()
     t_one, agree_o = one_call_pass()
+    ranges_pass()
+    ctx.set_key_table(18)                       # emptied in place: the timed call builds every key's table
+    t_cold, agree_c, _ = ranges_pass()
+    cold_stats = ctx.key_table_stats()
+    t_warm, agree_w, got_w = ranges_pass()      # every key resident from the call before
+    ctx.set_key_table(0)
+    ranges_pass()
+    t_off, agree_n, _ = ranges_pass()
+    ctx.set_key_table(18)
+
+    # the plain kernel over the same items, device-resident, one launch per kind
+    st = torch.cuda.Stream()
+    dev = {k: [torch.from_numpy(a.reshape(-1)).cuda() for a in corpora[k]] for k in (0, 1)}
+    d_out = {k: torch.zeros(len(corpora[k][0]), dtype=torch.uint8, device="cuda") for k in (0, 1)}
+    torch.cuda.synchronize()
+
+    def plain_kernel():
+        for k, f in ((0, ctx.ecdsa_verify_device), (1, ctx.schnorr_verify_device)):
+            m, p, sg = dev[k]
+            f(m.data_ptr(), p.data_ptr(), sg.data_ptr(), len(d_out[k]), d_out[k].data_ptr(), st.cuda_stream)
+
+    for _ in range(2):
+        plain_kernel()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    a.record(st)
+    for _ in range(reps):
+        plain_kernel()
+    b.record(st)
+    torch.cuda.synchronize()
+    plain_kernel_rate = total * reps / (a.elapsed_time(b) * 1e-3)
+    agree_k = sum(int((d_out[k].cpu().numpy() == expects[k]).sum()) for k in (0, 1))
+
+    # every item against the reference library (host cores), outside the timed regions
+    ref_agree = None
+    try:
+        from oracle import RefDriver
+        drv = RefDriver()
+        thr = os.cpu_count() or 1
+        ref_agree = sum(int((drv.verify(k, *corpora[k], thr) == got_w[k]).sum()) for k in (0, 1)) / total
+    except Exception as e:   # reference library missing on this box
+        ref_agree = f"unavailable: {e}"
     return {"workload": "2000 mixed batches, sizes log-uniform [1, 8192], 70/30 BIP-340/ECDSA, Zipf(1.1) keys "
                         "from a 100k pool, 0.5% invalid",
-            "signatures": total,
+            "signatures": total, "jobs": int(len(kinds_j)),
             "plain_sigs_per_s": total / t_plain, "batched_sigs_per_s": total / t_batched,
             "batched_over_plain": t_plain / t_batched,
             "plain": "one ufsecp_gpu_{ecdsa,schnorr}_verify_batch call per batch and kind (host buffers, wall clock, "
@@ -527,9 +601,24 @@ def bench_mixed(ctx, torch):
             "batched": f"ufsecp_gpu_ext_verify_jobs over groups of >= {group_items} signatures (host buffers, wall "
                        "clock, second pass)",
             "batched_one_call_sigs_per_s": total / t_one,
-            "batched_one_call": "all 2000 batches in one ufsecp_gpu_ext_verify_jobs call (host buffers, wall clock, "
-                                "second pass)",
-            "verdict_agreement": {"plain": agree / total, "batched": agree_b / total, "batched_one_call": agree_o / total}}
+            "batched_one_call": "all 2000 batches in one ufsecp_gpu_ext_verify_jobs call, job list marshalled per "
+                                "job in Python (host buffers, wall clock, second pass)",
+            "one_call_ranges": {
+                "api": "ufsecp_gpu_ext_verify_jobs, job table built by numpy vector operations from per-batch index "
+                       "ranges (host buffers, wall clock)",
+                "key_table_cold_sigs_per_s": total / t_cold,
+                "key_table_warm_sigs_per_s": total / t_warm,
+                "key_table_off_sigs_per_s": total / t_off,
+                "cold_key_table": {"lookups": cold_stats["lookups"], "hits": cold_stats["hits"]},
+                "cold_over_plain_kernel": (total / t_cold) / plain_kernel_rate,
+                "warm_over_plain_kernel": (total / t_warm) / plain_kernel_rate},
+            "plain_kernel_sigs_per_s": plain_kernel_rate,
+            "plain_kernel": "ufsecp_gpu_ext_{ecdsa,schnorr}_verify_device over all items of each kind, one call per "
+                            "kind, inputs on the device, CUDA events",
+            "verdict_agreement": {"plain": agree / total, "batched": agree_b / total, "batched_one_call": agree_o / total,
+                                  "ranges_cold": agree_c / total, "ranges_warm": agree_w / total,
+                                  "ranges_off": agree_n / total, "plain_kernel": agree_k / total,
+                                  "reference_library_all_items": ref_agree}}
 
 
 def bench_rlc(ctx, torch, n: int = 1 << 20, reps: int = 3):
@@ -754,8 +843,8 @@ def bench_serving(ctx, torch):
             "rates": rows, "fixed_4096": fixed}
 
 
-def ecdsa_4096_rate(ctx, torch, n=4096, reps=10):
-    """Plain ECDSA, n signatures in one call (4096: the small-batch case),
+def ecdsa_plain_rate(ctx, torch, n=1 << 20, reps=3):
+    """Plain ECDSA over n signatures in one call (all valid, keys from a seed),
     device-resident inputs, CUDA events around `reps` calls."""
     rng = np.random.default_rng(n)
     sks = rng.integers(1, 255, (n, 32), dtype=np.uint8)
@@ -780,6 +869,83 @@ def ecdsa_4096_rate(ctx, torch, n=4096, reps=10):
     torch.cuda.synchronize()
     assert bool(d_out.all())
     return n * reps / (a.elapsed_time(b) * 1e-3)
+
+
+def c1_corpus(n=4096, seed=4096):
+    """The plain-ECDSA workload: private keys uniform in [1, n-1] from a seed
+    (rejection sampling), 33-byte compressed keys, uniform 32-byte message
+    hashes, RFC 6979 low-S signatures from the reference's own CPU signer
+    (oracle/_ref), 10% tampered: one uniformly random bit flipped in the
+    message, r or s (the field chosen uniformly).  Returns the arrays and the
+    verdict each item must get by construction."""
+    from oracle import RefDriver
+    rng = np.random.default_rng(seed)
+    sks = np.zeros((n, 32), np.uint8)
+    for i in range(n):
+        while True:
+            k = rng.integers(0, 256, 32, dtype=np.uint8)
+            if 0 < int.from_bytes(k.tobytes(), "big") < N_ORDER:
+                sks[i] = k
+                break
+    msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    drv = RefDriver()
+    pubs, sigs, ok = drv.sign(0, msgs, sks, None, os.cpu_count() or 1)
+    assert ok.all()
+    expect = np.ones(n, np.uint8)
+    for i in rng.choice(n, size=n // 10, replace=False):
+        field = int(rng.integers(0, 3))
+        bit = int(rng.integers(0, 256))
+        if field == 0:
+            msgs[i, bit // 8] ^= 1 << (bit % 8)
+        else:
+            sigs[i, 32 * (field - 1) + bit // 8] ^= 1 << (bit % 8)
+        expect[i] = 0
+    return np.ascontiguousarray(msgs), np.ascontiguousarray(pubs), np.ascontiguousarray(sigs), expect
+
+
+def bench_c1(ctx, torch, reps=50):
+    """Plain ECDSA, 4096 signatures in one call (the workload above).  value:
+    inputs on the device, CUDA events around `reps` back-to-back calls; e2e:
+    ufsecp_gpu_ecdsa_verify_batch with host buffers, wall clock around `reps`
+    synchronous calls (copies in and out inside); verdicts of every item against
+    the reference library and the construction."""
+    import time as _t
+    from oracle import RefDriver
+    msgs, pubs, sigs, expect = c1_corpus()
+    n = len(msgs)
+    ref = RefDriver().verify(0, msgs, pubs, sigs, os.cpu_count() or 1)
+    dev = lambda a: torch.from_numpy(a.reshape(-1)).cuda()
+    d_m, d_p, d_s = dev(msgs), dev(pubs), dev(sigs)
+    d_out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for _ in range(3):
+        ctx.ecdsa_verify_device(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), n, d_out.data_ptr(), st.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        ctx.ecdsa_verify_device(d_m.data_ptr(), d_p.data_ptr(), d_s.data_ptr(), n, d_out.data_ptr(), st.cuda_stream)
+    b.record(st)
+    torch.cuda.synchronize()
+    value = n * reps / (a.elapsed_time(b) * 1e-3)
+    dev_verdicts = d_out.cpu().numpy()
+    for _ in range(3):
+        ctx.ecdsa_verify_batch(msgs, pubs, sigs)
+    t0 = _t.perf_counter()
+    for _ in range(reps):
+        host_verdicts = ctx.ecdsa_verify_batch(msgs, pubs, sigs)
+    e2e = n * reps / (_t.perf_counter() - t0)
+    return {"workload": "plain ECDSA, 4096 signatures per call: keys uniform in [1, n-1] from a seed, compressed keys, "
+                        "uniform message hashes, RFC 6979 low-S signatures from the reference's CPU signer, 10% "
+                        "tampered (one bit of the message, r or s)",
+            "value_sigs_per_s": value, "value": "ufsecp_gpu_ext_ecdsa_verify_device, inputs on the device, CUDA events, "
+                                                f"{reps} calls",
+            "e2e_sigs_per_s": e2e, "e2e": f"ufsecp_gpu_ecdsa_verify_batch, host buffers, wall clock, {reps} calls",
+            "e2e_ms_per_call": n / e2e * 1e3,
+            "verdict_agreement": {"reference_library_device": float((dev_verdicts == ref).mean()),
+                                  "reference_library_e2e": float((host_verdicts == ref).mean()),
+                                  "construction": float((host_verdicts == expect).mean())},
+            "valid": int(ref.sum())}
 
 
 def main():

@@ -62,8 +62,9 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const 
  * as such.  Before the verify kernels, a resolve pass gives each item its key's
  * slot and a build pass fills the new slots, so the verify warps never mix
  * lanes that build a table with lanes that copy one.  Verdicts never depend on
- * the table.  log2_slots: 0 = off; 8..24 = a new, empty table of 2^log2_slots
- * slots of 576 bytes (made on the next verify_jobs call).  Default: 18
+ * the table.  log2_slots: 0 = off; 8..24 = an empty table of 2^log2_slots
+ * slots of 576 bytes (a table of that size is emptied in place, another size
+ * is made on the next verify_jobs call).  Default: 18
  * (151 MB), from the tuning file's key_table_log2 or the environment
  * variable UFSECP_B200_KEY_TABLE when set.  Slots are never evicted: when a
  * key's probe window is full it is verified without the table.

@@ -144,3 +144,29 @@ def test_jobs_gating(gpu_ctx):
     buf = np.zeros(64 * 4, np.uint8)
     j = (uf.Job * 1)(uf.Job(2, 0, 4, buf.ctypes.data, buf.ctypes.data, buf.ctypes.data, out.ctypes.data))
     assert L.ufsecp_gpu_ext_verify_jobs(h, j, 1) == uf.UFSECP_ERR_BAD_INPUT
+
+
+def test_job_ranges_equal_job_lists(gpu_ctx, corpora):
+    """verify_job_ranges (job table built by vector operations from index
+    ranges of per-kind corpora) gives the verdicts of the same jobs passed as a
+    job list, and leaves items no job covers at 0."""
+    (e, s, we, ws) = corpora
+    rng = np.random.default_rng(17)
+    kinds, starts, counts = [], [], []
+    for kind, n in ((0, 6000), (1, 6000)):
+        pos = 0
+        while pos < n - 400:
+            c = int(rng.integers(0, 300))
+            kinds.append(kind)
+            starts.append(pos)
+            counts.append(c)
+            pos += c + int(rng.integers(0, 3))          # small gaps: uncovered items
+    got = gpu_ctx.verify_job_ranges({0: e, 1: s}, kinds, starts, counts)
+    covered = {0: np.zeros(6000, bool), 1: np.zeros(6000, bool)}
+    for k, st, c in zip(kinds, starts, counts):
+        covered[k][st:st + c] = True
+    for k, w in ((0, we), (1, ws)):
+        assert (got[k][covered[k]] == w[covered[k]]).all()
+        assert (got[k][~covered[k]] == 0).all()
+    with pytest.raises(ValueError):
+        gpu_ctx.verify_job_ranges({0: e}, [0], [5990], [20])

@@ -342,6 +342,48 @@ class GpuContext:
                     "verify_jobs")
         return [out_all[o:o + n] for o, n in offs]
 
+    def verify_job_ranges(self, corpora: dict, kinds, starts, counts) -> dict:
+        """ufsecp_gpu_ext_verify_jobs over jobs given as index ranges of per-kind
+        corpora: corpora = {kind: (msgs, pubs, sigs)} (contiguous uint8 arrays of
+        32 / 33 or 32 / 64 bytes per item), job j = items starts[j] ..
+        starts[j] + counts[j] - 1 of corpora[kinds[j]].  The job table is built
+        with vector operations (no per-job Python work), so a call of thousands
+        of jobs costs what the C ABI call costs.  Returns {kind: verdicts},
+        aligned with the corpora (items no job covers stay 0)."""
+        kinds = np.asarray(kinds, np.uint32)
+        starts = np.asarray(starts, np.uint64)
+        counts = np.asarray(counts, np.uint64)
+        if not (kinds.shape == starts.shape == counts.shape):
+            raise ValueError("kinds, starts and counts differ in length")
+        tab = np.zeros(max(1, kinds.size), _JOB_DTYPE)[:kinds.size]
+        tab["kind"] = kinds
+        tab["count"] = counts
+        outs, keep = {}, []
+        for k, (m, p, sg) in corpora.items():
+            m, p, sg = _flat_u8(m), _flat_u8(p), _flat_u8(sg)
+            n = m.size // 32
+            ps = 33 if k == 0 else 32
+            if p.size != ps * n or sg.size != 64 * n:
+                raise ValueError(f"corpus of kind {k}: inconsistent sizes")
+            sel = kinds == k
+            if (starts[sel] + counts[sel] > n).any():
+                raise ValueError(f"a job of kind {k} reaches past its corpus")
+            out = np.zeros(max(1, n), np.uint8)
+            outs[k] = out[:n]
+            keep.append((m, p, sg, out))
+            if n and sel.any():
+                st = starts[sel]
+                tab["msg_hashes32"][sel] = _addr(m) + 32 * st
+                tab["pubkeys"][sel] = _addr(p) + ps * st
+                tab["sigs64"][sel] = _addr(sg) + 64 * st
+                tab["out_results"][sel] = _addr(out) + st
+        orphan = ~np.isin(kinds, np.array(list(corpora), np.uint32))
+        if (counts[orphan] > 0).any():
+            raise ValueError("a job names a kind with no corpus")
+        self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, tab.ctypes.data_as(ctypes.POINTER(Job)), kinds.size),
+                    "verify_jobs")
+        return outs
+
     def set_key_table(self, log2_slots: int):
         """ufsecp_gpu_ext_set_key_table: 0 = no resident key table for verify_jobs,
         8..24 = a new, empty table of 2^log2_slots slots."""

@@ -458,6 +458,14 @@ int Backend::sign_device(int kind, const uint8_t* d_msgs, const uint8_t* d_sks, 
 int Backend::set_key_table(uint32_t log2) {
     if (log2 != 0 && (log2 < KeyTable::kMinLog2 || log2 > KeyTable::kMaxLog2))
         return set_error(kErrBadInput, "key table: log2 slots must be 0 or 8..24");
+    if (keys_ && keys_->on() && log2 == key_log2_) {
+        // same size: empty the table in place (the batch slots and their graphs stay)
+        cudaError_t e = keys_->clear(stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) return cuda_error(e, "key table clear");
+        clear_error();
+        return kOk;
+    }
     // the batch slots' captured graphs hold the old table's pointers
     batch_[0].reset();
     batch_[1].reset();

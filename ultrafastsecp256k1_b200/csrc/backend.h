@@ -80,8 +80,9 @@ public:
     // synchronous.  Keys go through the context's resident key table when it
     // is on (set_key_table).
     int verify_jobs(const VerifyJob* jobs, size_t n_jobs);
-    // Resident key table of verify_jobs: 0 = off, 8..24 = a new, empty table
-    // of 2^log2 slots (made on the next verify_jobs call).  The default is the
+    // Resident key table of verify_jobs: 0 = off, 8..24 = an empty table of
+    // 2^log2 slots (the current table emptied in place when it has that size,
+    // else a new one made on the next verify_jobs call).  The default is the
     // tuning file's key_table_log2, else UFSECP_B200_KEY_TABLE, else 18.
     int set_key_table(uint32_t log2);
     uint32_t key_table_log2() const { return key_log2_; }

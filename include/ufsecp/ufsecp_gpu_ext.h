@@ -10,6 +10,7 @@
 #define UFSECP_GPU_EXT_H
 
 #include "ufsecp_gpu.h"
+#include "ufsecp_cancel.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -54,6 +55,18 @@ typedef struct {
 
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
                                                      size_t n_jobs);
+
+/* Host-side fault injection, for testing fail-closed behaviour (no
+ * reference counterpart; nothing faults on the device).  Once armed, the
+ * (after + 1)-th fault point the context crosses fails, and the injector
+ * disarms itself: kind 1 as if a CUDA call returned cudaErrorMemoryAllocation
+ * (UFSECP_ERR_GPU_MEMORY), 2 as if a launch returned cudaErrorLaunchFailure
+ * (UFSECP_ERR_GPU_LAUNCH), 3 as if the host ran out of memory (std::bad_alloc,
+ * UFSECP_ERR_GPU_MEMORY); kind 0 disarms.  Fault points: every chunk launch
+ * of the host-buffer verify calls, every device-buffer verify call, every
+ * mixed-job or served launch and every RLC round.  The failing step is not
+ * made; the call returns the error with its result bytes cleared. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_inject_fault(ufsecp_gpu_ctx* ctx, uint32_t after, int kind);
 
 /* Resident key table of ufsecp_gpu_ext_verify_jobs (no reference
  * counterpart).  Per distinct public key (x, parity) a device slot keeps the
@@ -208,6 +221,29 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_submit(ufsecp_gpu_ext_server* se
                                                        uint64_t* request_id);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_wait(ufsecp_gpu_ext_server* server, uint64_t request_id,
                                                      uint32_t timeout_ms);
+/* Cancellation (the token type is the reference's, include/ufsecp/ufsecp_cancel.h).
+ * submit_cancellable: as submit, with a token (may be NULL; copied) that the
+ * scheduler polls before every launch that would take a piece of the request;
+ * once it answers non-zero no further piece is launched, pieces already on
+ * the device finish, and the request ends with UFSECP_ERR_CANCELLED, its
+ * verdict bytes cleared (wait() returns that code).  The predicate runs on
+ * the server's scheduler thread and must not call into the server.
+ * cancel: abandons a request, typically after wait() timed out.  Pieces not
+ * launched yet are dropped; pieces on the device finish (a kernel is not
+ * stopped) and cancel waits for them, at most timeout_ms.  UFSECP_OK: the
+ * server has forgotten the request and touches its buffers no more, so the
+ * caller may free them; the verdict bytes are cleared unless the request had
+ * completed before the call.  UFSECP_ERR_GPU_QUEUE: pieces were still on the
+ * device at the timeout (nothing more is launched for it; call cancel or wait
+ * again before freeing the buffers).  UFSECP_ERR_BAD_INPUT: unknown id.  A
+ * request that fails on the GPU ends with its error code and its verdict
+ * bytes cleared as well (fail closed). */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_submit_cancellable(ufsecp_gpu_ext_server* server,
+                                                                   const ufsecp_gpu_ext_job_t* jobs, size_t n_jobs,
+                                                                   const ufsecp_cancel_token* cancel,
+                                                                   uint64_t* request_id);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_cancel(ufsecp_gpu_ext_server* server, uint64_t request_id,
+                                                       uint32_t timeout_ms);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_server_stats(ufsecp_gpu_ext_server* server,
                                                       ufsecp_gpu_ext_server_stats_t* out, int reset);
 UFSECP_API void ufsecp_gpu_ext_server_destroy(ufsecp_gpu_ext_server* server);
@@ -226,6 +262,11 @@ UFSECP_API void ufsecp_gpu_ext_server_destroy(ufsecp_gpu_ext_server* server);
 UFSECP_API int ufsecp_gpu_ext_engine_columns_hook(int kind, const uint8_t* digests32, const uint8_t* keys,
                                                   const uint8_t* sigs64, size_t count,
                                                   uint8_t* out_results) UFSECP_NOEXCEPT;
+/* Arms host-side fault injection on the hook's process-wide context (made here
+ * if needed), as ufsecp_gpu_ext_inject_fault does for a caller's context:
+ * the hook then declines the failing call and the engine answers on its CPU
+ * path.  UFSECP_ERR_GPU_UNAVAILABLE without a device. */
+UFSECP_API int ufsecp_gpu_ext_engine_hook_inject_fault(uint32_t after, int kind);
 /* Calls the hook handled on the GPU / declined, since load. */
 UFSECP_API void ufsecp_gpu_ext_engine_hook_counters(uint64_t* handled, uint64_t* declined);
 /* Destroys the hook's process-wide context (the next call creates it again). */

@@ -98,3 +98,54 @@ def test_device_info_without_device(lib):
     assert lib.ufsecp_gpu_device_info(1, 0, None) == uf.UFSECP_ERR_NULL_ARG
     with pytest.raises(uf.UfsecpError):
         uf.GpuContext(0)
+
+
+def _reference_tree():
+    import sys
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import reference_tree
+    return reference_tree()
+
+
+EXAMPLE_BIN = os.path.join(ROOT, "oracle", "_ref", "gpu_example")
+
+
+def test_reference_c_example_compiles_links_and_runs(tmp_path):
+    """The reference's own C example of the GPU API (include/ufsecp/examples/
+    gpu_example.c), compiled UNCHANGED against this include/ and linked to
+    libufsecp_gpu.so by a C compiler: it must build without warnings of
+    missing declarations and run to completion.  Without a device it takes its
+    no-device path."""
+    import subprocess
+    ref = _reference_tree()
+    if ref is None:
+        pytest.skip("reference source tree not present (the prebuilt binary is run by the gpu test)")
+    src = os.path.join(ref, "include", "ufsecp", "examples", "gpu_example.c")
+    exe = tmp_path / "gpu_example"
+    libdir = os.path.dirname(uf.LIB_PATH)
+    cc = subprocess.run(["gcc", "-O2", "-Wall", "-Werror=implicit-function-declaration", "-I",
+                         os.path.join(ROOT, "include"), "-o", str(exe), src, "-L", libdir, "-lufsecp_gpu",
+                         f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "Compiled GPU backends: 1" in run.stdout
+    if uf.device_count() == 0:
+        assert "No available GPU device found." in run.stdout
+
+
+@pytest.mark.gpu
+def test_reference_c_example_on_the_gpu():
+    """The same example, prebuilt from the reference's source by `make -C oracle
+    example`, on a B200: it creates a context, meets UNSUPPORTED for the
+    generator multiplication (outside the verify path) and verifies a batch
+    through ufsecp_gpu_ecdsa_verify_batch."""
+    import subprocess
+    if not os.path.exists(EXAMPLE_BIN):
+        pytest.skip("oracle/_ref/gpu_example not built (make -C oracle example REF=<reference tree>)")
+    run = subprocess.run([EXAMPLE_BIN], capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "Using: NVIDIA" in run.stdout
+    assert "generator_mul_batch not supported on this backend." in run.stdout
+    assert "ecdsa_verify_batch returned: OK" in run.stdout
+    assert "Done." in run.stdout

@@ -78,3 +78,17 @@ def test_hook_handles_engine_calls_on_the_gpu(oracle, reflib):
     before, after = _run(oracle, reflib)
     assert after[0] == before[0] + 2 and after[1] == before[1]      # both calls ran on the GPU
     uf.load_library().ufsecp_gpu_ext_engine_hook_release()
+
+
+@pytest.mark.gpu
+def test_hook_declines_on_a_backend_error(oracle, reflib):
+    """A backend failure inside the hook (injected on the host: the hook's
+    context fails its next launch) makes the hook decline that call; the
+    engine's CPU path answers it with the right verdicts, and the next call is
+    handled on the GPU again."""
+    U = uf.load_library()
+    U.ufsecp_gpu_ext_engine_hook_release()
+    assert U.ufsecp_gpu_ext_engine_hook_inject_fault(0, 2) == uf.UFSECP_OK    # first launch of the hook fails
+    before, after = _run(oracle, reflib)
+    assert after[1] == before[1] + 1 and after[0] == before[0] + 1     # one declined (CPU answered), one handled
+    U.ufsecp_gpu_ext_engine_hook_release()

@@ -28,6 +28,7 @@ UFSECP_ERR_BAD_INPUT = 5
 UFSECP_ERR_VERIFY_FAIL = 6
 UFSECP_ERR_ARITH = 7
 UFSECP_ERR_INTERNAL = 9
+UFSECP_ERR_CANCELLED = 13
 UFSECP_ERR_GPU_UNAVAILABLE = 100
 UFSECP_ERR_GPU_DEVICE = 101
 UFSECP_ERR_GPU_LAUNCH = 102
@@ -53,6 +54,14 @@ class Job(ctypes.Structure):
     """ufsecp_gpu_ext_job_t: one caller batch of a mixed ufsecp_gpu_ext_verify_jobs call."""
     _fields_ = [("kind", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("count", ctypes.c_size_t),
                 ("msg_hashes32", _vp), ("pubkeys", _vp), ("sigs64", _vp), ("out_results", _vp)]
+
+
+CANCEL_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+
+
+class CancelToken(ctypes.Structure):
+    """ufsecp_cancel_token (include/ufsecp/ufsecp_cancel.h)."""
+    _fields_ = [("is_cancelled", CANCEL_FN), ("user", ctypes.c_void_p), ("check_interval", ctypes.c_uint32)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -131,6 +140,11 @@ _SIGS = {
     "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_set_key_table": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_inject_fault": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_int]),
+    "ufsecp_gpu_ext_engine_hook_inject_fault": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int]),
+    "ufsecp_gpu_ext_server_submit_cancellable": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_size_t, _vp,
+                                                                ctypes.POINTER(ctypes.c_uint64)]),
+    "ufsecp_gpu_ext_server_cancel": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint32]),
     "ufsecp_gpu_ext_key_table_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_rlc_input_digest": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_schnorr_batch_verify": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
@@ -582,12 +596,38 @@ class Server:
         return rid.value
 
     def wait(self, rid: int, timeout_ms: int = 60_000):
-        """Verdict arrays of request `rid`, one per job."""
+        """Verdict arrays of request `rid`, one per job.  A failed or cancelled
+        request raises UfsecpError with its code (its verdicts were cleared); a
+        timeout raises with UFSECP_ERR_GPU_QUEUE and keeps the request."""
         rc = self.L.ufsecp_gpu_ext_server_wait(self._h, rid, timeout_ms)
+        if rc == UFSECP_ERR_GPU_QUEUE:
+            raise UfsecpError(rc, "server_wait")
+        keep = self._keep.pop(rid)
         if rc != UFSECP_OK:
             raise UfsecpError(rc, "server_wait")
-        keep, outs, arr = self._keep.pop(rid)
-        return outs
+        return keep[1]
+
+    def submit_cancellable(self, jobs, is_cancelled, check_interval: int = 0) -> int:
+        """submit() with a cancellation token: is_cancelled() -> bool is polled by
+        the server before each launch that would take a piece of the request."""
+        tab, keep, out_all, offs = _job_table(jobs)
+        fn = CANCEL_FN(lambda user: 1 if is_cancelled() else 0)
+        tok = CancelToken(fn, None, check_interval)
+        rid = ctypes.c_uint64()
+        rc = self.L.ufsecp_gpu_ext_server_submit_cancellable(self._h, tab.ctypes.data_as(ctypes.POINTER(Job)),
+                                                             len(jobs), ctypes.byref(tok), ctypes.byref(rid))
+        if rc != UFSECP_OK:
+            raise UfsecpError(rc, "server_submit_cancellable")
+        self._keep[rid.value] = (keep, [out_all[o:o + n] for o, n in offs], tab, fn, tok)
+        return rid.value
+
+    def cancel(self, rid: int, timeout_ms: int = 60_000) -> int:
+        """ufsecp_gpu_ext_server_cancel; returns its code.  On UFSECP_OK the server
+        no longer touches the request's buffers."""
+        rc = self.L.ufsecp_gpu_ext_server_cancel(self._h, rid, timeout_ms)
+        if rc == UFSECP_OK:
+            self._keep.pop(rid, None)
+        return rc
 
     def stats(self, reset: bool = False) -> dict:
         st = ServerStats()

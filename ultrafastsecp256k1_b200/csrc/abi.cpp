@@ -498,20 +498,29 @@ ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_
         if (J.kind > 1) return UFSECP_ERR_BAD_INPUT;
     }
     if (total > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    int rc;
     try {
         std::vector<uf::VerifyJob> v(n_jobs);
         for (size_t j = 0; j < n_jobs; ++j)
             v[j] = uf::VerifyJob{(int)jobs[j].kind, jobs[j].count, jobs[j].msg_hashes32, jobs[j].pubkeys,
                                  jobs[j].sigs64, jobs[j].out_results};
-        const int rc = ctx->backend->verify_jobs(v.data(), n_jobs);
-        if (rc != UFSECP_OK)
-            for (size_t j = 0; j < n_jobs; ++j) clear_out(jobs[j].out_results, jobs[j].count, 1);
-        return rc;
+        rc = ctx->backend->verify_jobs(v.data(), n_jobs);
     } catch (const std::bad_alloc&) {
-        return UFSECP_ERR_GPU_MEMORY;
+        rc = UFSECP_ERR_GPU_MEMORY;
     } catch (...) {
-        return UFSECP_ERR_INTERNAL;
+        rc = UFSECP_ERR_INTERNAL;
     }
+    // fail closed: no verdict of a failed call may read as valid
+    if (rc != UFSECP_OK)
+        for (size_t j = 0; j < n_jobs; ++j) clear_out(jobs[j].out_results, jobs[j].count, 1);
+    return (ufsecp_error_t)rc;
+}
+
+ufsecp_error_t ufsecp_gpu_ext_inject_fault(ufsecp_gpu_ctx* ctx, uint32_t after, int kind) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (kind < 0 || kind > 3) return ctx->backend->set_error(UFSECP_ERR_BAD_INPUT, "fault kind must be 0..3");
+    ctx->backend->arm_fault(after, kind);
+    return UFSECP_OK;
 }
 
 ufsecp_error_t ufsecp_gpu_ext_set_key_table(ufsecp_gpu_ctx* ctx, uint32_t log2_slots) {
@@ -731,23 +740,24 @@ ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc(ufsecp_gpu_ctx* ctx, const uint
     const size_t n_batches = batch_size == 0 || batch_size >= count ? 1 : (count + batch_size - 1) / batch_size;
     clear_out(out_batch_ok, n_batches, 1);
     if (!msg_hashes32 || !pubkeys_x32 || !sigs64 || !seed32 || !out_results) return UFSECP_ERR_NULL_ARG;
-    return guarded([&]() -> ufsecp_error_t {
+    const ufsecp_error_t rc = guarded([&]() -> ufsecp_error_t {
         uf::Backend& be = *ctx->backend;
         if (!be.ready()) return be.set_error(UFSECP_ERR_GPU_DEVICE, "context not ready");
         cudaError_t e = cudaSetDevice(be.device());
         if (e != cudaSuccess) return be.cuda_error(e, "cudaSetDevice");
         ctx->rlc_stats = uf::RlcStats{};
-        const int rc = be.rlc().verify_host(msg_hashes32, pubkeys_x32, sigs64, (uint32_t)count,
-                                            (uint32_t)std::min(batch_size, count), seed32, window_bits, out_results,
-                                            out_batch_ok, &ctx->rlc_stats);
-        if (rc != UFSECP_OK) {
-            clear_out(out_results, count, 1);
-            clear_out(out_batch_ok, n_batches, 1);
-            return rc;
-        }
+        const int r = be.rlc().verify_host(msg_hashes32, pubkeys_x32, sigs64, (uint32_t)count,
+                                           (uint32_t)std::min(batch_size, count), seed32, window_bits, out_results,
+                                           out_batch_ok, &ctx->rlc_stats);
+        if (r != UFSECP_OK) return (ufsecp_error_t)r;
         be.clear_error();
         return UFSECP_OK;
     });
+    if (rc != UFSECP_OK) {   // fail closed, exceptions included
+        clear_out(out_results, count, 1);
+        clear_out(out_batch_ok, n_batches, 1);
+    }
+    return rc;
 }
 
 ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc_device(ufsecp_gpu_ctx* ctx, const uint8_t* d_msg_hashes32,
@@ -866,6 +876,12 @@ ufsecp_error_t ufsecp_gpu_ext_server_create(ufsecp_gpu_ctx* ctx, const ufsecp_gp
 
 ufsecp_error_t ufsecp_gpu_ext_server_submit(ufsecp_gpu_ext_server* server, const ufsecp_gpu_ext_job_t* jobs,
                                             size_t n_jobs, uint64_t* request_id) {
+    return ufsecp_gpu_ext_server_submit_cancellable(server, jobs, n_jobs, nullptr, request_id);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_server_submit_cancellable(ufsecp_gpu_ext_server* server,
+                                                        const ufsecp_gpu_ext_job_t* jobs, size_t n_jobs,
+                                                        const ufsecp_cancel_token* cancel, uint64_t* request_id) {
     if (!server || !request_id || (n_jobs && !jobs)) return UFSECP_ERR_NULL_ARG;
     size_t total = 0;
     for (size_t j = 0; j < n_jobs; ++j) {
@@ -884,8 +900,13 @@ ufsecp_error_t ufsecp_gpu_ext_server_submit(ufsecp_gpu_ext_server* server, const
             v.push_back(uf::VerifyJob{(int)jobs[j].kind, jobs[j].count, jobs[j].msg_hashes32, jobs[j].pubkeys,
                                       jobs[j].sigs64, jobs[j].out_results});
         }
-        return server->server->submit(v.data(), v.size(), request_id);
+        return server->server->submit(v.data(), v.size(), cancel, request_id);
     });
+}
+
+ufsecp_error_t ufsecp_gpu_ext_server_cancel(ufsecp_gpu_ext_server* server, uint64_t request_id, uint32_t timeout_ms) {
+    if (!server) return UFSECP_ERR_NULL_ARG;
+    return guarded([&]() -> ufsecp_error_t { return server->server->cancel(request_id, timeout_ms); });
 }
 
 ufsecp_error_t ufsecp_gpu_ext_server_wait(ufsecp_gpu_ext_server* server, uint64_t request_id, uint32_t timeout_ms) {
@@ -959,8 +980,13 @@ int ufsecp_gpu_ext_engine_columns_hook(int kind, const uint8_t* digests32, const
             ++g_hook_declined;
             return -1;
         }
-        const int rc = g_hook_ctx->backend->verify_host(kind == 0 ? 2 : 1, digests32, keys, sigs64, count,
-                                                        out_results, false);
+        int rc;
+        try {
+            rc = g_hook_ctx->backend->verify_host(kind == 0 ? 2 : 1, digests32, keys, sigs64, count, out_results,
+                                                  false);
+        } catch (...) {
+            rc = UFSECP_ERR_INTERNAL;
+        }
         if (rc != UFSECP_OK) {
             ++g_hook_declined;
             return -1;   // operational error: the engine falls back to its CPU path
@@ -978,6 +1004,24 @@ void ufsecp_gpu_ext_engine_hook_counters(uint64_t* handled, uint64_t* declined) 
     std::lock_guard<std::mutex> lk(g_hook_mu);
     if (handled) *handled = g_hook_handled;
     if (declined) *declined = g_hook_declined;
+}
+
+int ufsecp_gpu_ext_engine_hook_inject_fault(uint32_t after, int kind) {
+    if (kind < 0 || kind > 3) return UFSECP_ERR_BAD_INPUT;
+    std::lock_guard<std::mutex> lk(g_hook_mu);
+    if (!g_hook_probed) {
+        g_hook_probed = true;
+        if (cuda_device_count() > 0) {
+            std::unique_ptr<ufsecp_gpu_ctx> c(new ufsecp_gpu_ctx());
+            c->backend_id = UFSECP_GPU_BACKEND_CUDA;
+            c->device_index = 0;
+            c->backend.reset(new uf::Backend());
+            if (c->backend->init(0) == UFSECP_OK && c->backend->ready()) g_hook_ctx = std::move(c);
+        }
+    }
+    if (!g_hook_ctx) return UFSECP_ERR_GPU_UNAVAILABLE;
+    g_hook_ctx->backend->arm_fault(after, kind);
+    return UFSECP_OK;
 }
 
 void ufsecp_gpu_ext_engine_hook_release(void) {

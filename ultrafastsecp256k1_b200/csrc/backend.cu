@@ -4,6 +4,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <new>
 #include <thread>
 #include <vector>
 #include <math.h>
@@ -16,6 +17,7 @@
 #include "kernels.h"
 #include "pack_pool.h"
 #include "rlc.h"
+#include "nvtx.h"
 
 namespace uf {
 
@@ -258,6 +260,16 @@ Backend::~Backend() {
     }
 }
 
+int Backend::fault_point(const char* where) {
+    if (fault_kind_.load(std::memory_order_relaxed) == 0) return kOk;
+    if (fault_after_.fetch_sub(1) != 0) return kOk;
+    const int kind = fault_kind_.exchange(0);
+    if (kind == 3) throw std::bad_alloc();
+    if (kind == 1) return cuda_error(cudaErrorMemoryAllocation, where);
+    if (kind == 2) return cuda_error(cudaErrorLaunchFailure, where);
+    return kOk;
+}
+
 int Backend::set_error(int code, const char* what) {
     last_err_ = code;
     last_msg_ = what ? what : "";
@@ -336,6 +348,7 @@ int Backend::verify_device(int kind, const uint8_t* d_msgs, const uint8_t* d_pub
     if ((e = cudaEventRecord(dfork_, s)) != cudaSuccess || (e = cudaStreamWaitEvent(dstream_, dfork_, 0)) != cudaSuccess)
         return cuda_error(e, "fork");
     const size_t pub_sz = kind == 1 ? 32 : 33;
+    if (const int rc = fault_point("verify launch")) return rc;
     size_t k = 0;
     for (size_t off = 0; off < count; off += kDeviceChunk, ++k) {
         const size_t m = std::min(kDeviceChunk, count - off);
@@ -359,6 +372,7 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
                                  bool collect) {
     if (!ready_) return set_error(kErrGpuDevice, "context not ready");
     if (count == 0) return kOk;
+    NvtxRange range("ufsecp verify (host buffers)");
     cudaError_t e = cudaSetDevice(dev_);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
     if (!pstream_[0]) {
@@ -394,10 +408,19 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
     // pipeline's fill (packing and copying the first chunk while the device
     // is idle) costs a small chunk, and the device fills up while the CPU
     // packs the next, larger ones.
+    // every early return waits for the slots' streams first, so that no copy
+    // of this call is still in flight when the next call packs a slot
+    auto fail = [&](int rc) {
+        for (int q = 0; q < kPipeSlots; ++q)
+            if (pstream_[q]) (void)cudaStreamSynchronize(pstream_[q]);
+        (void)cudaGetLastError();
+        return rc;
+    };
     size_t k = 0, m = 0;
     for (size_t off = 0; off < count; off += m, ++k) {
         const int j = (int)(k % kPipeSlots);
-        if ((e = drain(j)) != cudaSuccess) return cuda_error(e, "verify");
+        if ((e = drain(j)) != cudaSuccess) return fail(cuda_error(e, "verify"));
+        if (const int rc = fault_point("verify launch")) return fail(rc);
         m = std::min(std::min(sub, kPipeFirst << std::min<size_t>(k, 20)), count - off);
         const size_t o_p = m * 32, o_s = a16(o_p + m * pub_sz), o_o = o_s + m * 64;
         uint8_t* h = (uint8_t*)pstage_[j].p;
@@ -415,6 +438,7 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
             one(h + o_p, pubs, pub_sz, p_stride);
             one(h + o_s, sigs, 64, s_stride);
         };
+        NvtxRange pack_range("pack chunk");
         if (pack_threads_ > 1 && m >= kPackSplitItems) {
             if (!pack_pool_) pack_pool_.reset(new PackPool(pack_threads_));
             const int parts = pack_pool_->threads();
@@ -425,18 +449,18 @@ int Backend::verify_host_strided(int kind, const uint8_t* msgs, size_t m_stride,
         if (collect) memcpy(h + o_o, out + off, m);
         const size_t in_bytes = o_o + (collect ? m : 0);
         if ((e = cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, pstream_[j])) != cudaSuccess)
-            return cuda_error(e, "host->device copy");
+            return fail(cuda_error(e, "host->device copy"));
         e = launch_verify(kind, d, d + o_p, d + o_s, (uint32_t)m, d + o_o, collect, pstream_[j], count);
-        if (e != cudaSuccess) return cuda_error(e, "verify launch");
+        if (e != cudaSuccess) return fail(cuda_error(e, "verify launch"));
         if ((e = cudaMemcpyAsync(h + o_o, d + o_o, m, cudaMemcpyDeviceToHost, pstream_[j])) != cudaSuccess)
-            return cuda_error(e, "device->host copy");
-        if ((e = cudaEventRecord(pev_[j], pstream_[j])) != cudaSuccess) return cuda_error(e, "event record");
+            return fail(cuda_error(e, "device->host copy"));
+        if ((e = cudaEventRecord(pev_[j], pstream_[j])) != cudaSuccess) return fail(cuda_error(e, "event record"));
         pend_off[j] = off;
         pend_n[j] = m;
         pend_out[j] = o_o;
     }
     for (int j = 0; j < kPipeSlots; ++j)
-        if ((e = drain(j)) != cudaSuccess) return cuda_error(e, "verify");
+        if ((e = drain(j)) != cudaSuccess) return fail(cuda_error(e, "verify"));
     clear_error();
     return kOk;
 }
@@ -486,6 +510,7 @@ int Backend::key_table_stats(uint64_t* lookups, uint64_t* hits, uint64_t* slots)
 
 int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
     if (!ready_) return set_error(kErrGpuDevice, "context not ready");
+    NvtxRange range("ufsecp verify_jobs");
     if (key_log2_ && !keys_) {
         auto kt = std::make_unique<KeyTable>();
         const int rc = kt->create(this, key_log2_);

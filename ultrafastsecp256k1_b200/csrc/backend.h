@@ -12,6 +12,7 @@
 #include <stddef.h>
 #include <stdint.h>
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <string>
@@ -20,7 +21,7 @@ namespace uf {
 
 // ABI error codes (same values as ufsecp_error.h / ufsecp_gpu.h).
 enum : int {
-    kOk = 0, kErrNullArg = 1, kErrBadInput = 5, kErrInternal = 9,
+    kOk = 0, kErrNullArg = 1, kErrBadInput = 5, kErrInternal = 9, kErrCancelled = 13,
     kErrGpuUnavailable = 100, kErrGpuDevice = 101, kErrGpuLaunch = 102, kErrGpuMemory = 103,
     kErrGpuUnsupported = 104, kErrGpuBackend = 105, kErrGpuQueue = 106,
 };
@@ -130,6 +131,20 @@ public:
 
     int set_error(int code, const char* what);
     int cuda_error(cudaError_t e, const char* what);
+
+    // Host-side fault injection, for the fail-closed tests: once armed, the
+    // (after + 1)-th fault point this context crosses fails as kind says --
+    // 1: a CUDA call returned cudaErrorMemoryAllocation, 2: a launch returned
+    // cudaErrorLaunchFailure, 3: std::bad_alloc is thrown -- and the injector
+    // disarms itself; kind 0 disarms.  Fault points: each chunk launch of the
+    // host-buffer verify, each device-buffer verify call, each mixed-job /
+    // served launch (BatchSlot::enqueue) and each RLC round.  Nothing reaches
+    // the device: the failing call is not made.
+    void arm_fault(uint32_t after, int kind) {
+        fault_after_.store((long long)after);
+        fault_kind_.store(kind);
+    }
+    int fault_point(const char* where);
     void clear_error() { last_err_ = kOk; last_msg_ = "OK"; }
 
 private:
@@ -185,6 +200,8 @@ private:
     uint32_t rlc_chunk_fixed_ = 0;            // set_rlc_chunk / UFSECP_B200_RLC_CHUNK override, 0 = tuned
     int last_err_ = kOk;
     std::string last_msg_ = "OK";
+    std::atomic<long long> fault_after_{-1};
+    std::atomic<int> fault_kind_{0};
 };
 
 }  // namespace uf

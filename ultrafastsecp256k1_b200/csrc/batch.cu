@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "backend.h"
+#include "nvtx.h"
 
 namespace uf {
 
@@ -155,10 +156,15 @@ int BatchSlot::run_graph(const QueueArgs& a, uint64_t key) {
 }
 
 int BatchSlot::enqueue(const VerifyJob* jobs, size_t n_jobs) {
+    NvtxRange range("batch slot: pack + launch");
+    if (const int rc = be_->fault_point("batch enqueue")) return rc;
     size_t n_e = 0, n_s = 0;
     for (size_t j = 0; j < n_jobs; ++j) (jobs[j].kind == 0 ? n_e : n_s) += jobs[j].count;
     cudaError_t e = cudaSetDevice(be_->device());
     if (e != cudaSuccess) return be_->cuda_error(e, "cudaSetDevice");
+    // the staging is reused: the previous launch (finished or abandoned after
+    // an error) must be off it first; normally it is complete already
+    if ((e = cudaEventSynchronize(done_)) != cudaSuccess) return be_->cuda_error(e, "batch slot");
     const bool graph = use_graphs_ && n_e <= kGraphMaxItems && n_s <= kGraphMaxItems;
     if (graph) {
         layout_ = QueueLayout(bucket(n_e), bucket(n_s));
@@ -226,6 +232,7 @@ int BatchSlot::prewarm(uint32_t max_items) {
 bool BatchSlot::ready() { return cudaEventQuery(done_) != cudaErrorNotReady; }
 
 int BatchSlot::finish(const VerifyJob* jobs, size_t n_jobs) {
+    NvtxRange range("batch slot: verdicts out");
     cudaError_t e = cudaEventSynchronize(done_);
     if (e != cudaSuccess) return be_->cuda_error(e, "batch");
     const uint8_t* h = staged_big_ ? (const uint8_t*)big_pinned_.p : (const uint8_t*)pinned_.p;

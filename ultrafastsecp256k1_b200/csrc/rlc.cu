@@ -19,6 +19,7 @@
 #include "kernels.h"
 #include "sign.cuh"
 #include "verify.cuh"
+#include "nvtx.h"
 
 namespace uf {
 
@@ -605,6 +606,8 @@ RlcVerifier::~RlcVerifier() {
 }
 
 int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok) {
+    NvtxRange range("RLC round");
+    if (const int rc = be_->fault_point("RLC round")) return rc;
     const uint32_t n_seg = (uint32_t)(seg.size() / 2);
     const int W = (129 + c - 1) / c, B = 1 << (c - 1), S = sub_ranges(c);
     std::vector<uint32_t> host(3 * (size_t)n_seg + 1);
@@ -688,6 +691,7 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
 
 int RlcVerifier::verify_leaves(const std::vector<uint32_t>& leaves, const uint8_t* d_msgs, const uint8_t* d_xs,
                                const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats) {
+    NvtxRange range("RLC leaves");
     std::vector<uint32_t> idx;
     for (size_t k = 0; k < leaves.size(); k += 2)
         for (uint32_t i = 0; i < leaves[k + 1]; ++i) idx.push_back(leaves[k] + i);

@@ -1,7 +1,10 @@
 // Serving loop implementation (see server.h).
 #include "server.h"
+#include "nvtx.h"
 
 #include <cuda_runtime.h>
+
+#include <string.h>
 
 #include <algorithm>
 
@@ -65,8 +68,12 @@ int Server::start(const ServerConfig& cfg) {
     return kOk;
 }
 
-int Server::submit(const VerifyJob* jobs, size_t n_jobs, uint64_t* id) {
+int Server::submit(const VerifyJob* jobs, size_t n_jobs, const ufsecp_cancel_token* cancel, uint64_t* id) {
     std::unique_ptr<Request> r(new Request());
+    if (cancel && cancel->is_cancelled) {
+        r->has_token = true;
+        r->token = *cancel;
+    }
     r->jobs.reserve(n_jobs);
     for (size_t j = 0; j < n_jobs; ++j) {
         if (jobs[j].count == 0) continue;
@@ -95,6 +102,54 @@ int Server::submit(const VerifyJob* jobs, size_t n_jobs, uint64_t* id) {
     return kOk;
 }
 
+namespace {
+bool token_cancelled(const ufsecp_cancel_token& t) {
+    try {
+        return t.is_cancelled(t.user) != 0;
+    } catch (...) {
+        return true;   // a predicate that throws counts as a cancellation (fail closed)
+    }
+}
+}  // namespace
+
+void Server::drop_pending(Request* r) {
+    if (r->all_launched) return;
+    r->all_launched = true;
+    auto it = std::find(pending_.begin(), pending_.end(), r);
+    if (it != pending_.end()) pending_.erase(it);
+}
+
+void Server::finalize(Request* r) {
+    r->done = true;
+    if (r->status != kOk) {
+        // fail closed: a failed or cancelled request reports no verdict as valid
+        for (const VerifyJob& J : r->jobs) memset(J.out, 0, J.count);
+        return;
+    }
+    lat_us_.push_back(std::chrono::duration<double, std::micro>(Clock::now() - r->t_submit).count());
+    items_done_ += r->items;
+    t_last_done_ = Clock::now();
+}
+
+int Server::cancel(uint64_t id, uint32_t timeout_ms) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) return kErrBadInput;
+    Request* r = it->second.get();
+    if (!r->done) {
+        r->abandoned = true;
+        drop_pending(r);
+        if (!cv_done_.wait_for(lk, std::chrono::milliseconds(timeout_ms), [r] { return r->pieces_in_flight == 0; }))
+            return kErrGpuQueue;
+        if (!r->done) {
+            r->status = kErrCancelled;
+            finalize(r);
+        }
+    }
+    reqs_.erase(it);
+    return kOk;
+}
+
 int Server::wait(uint64_t id, uint32_t timeout_ms) {
     std::unique_lock<std::mutex> lk(mu_);
     auto it = reqs_.find(id);
@@ -107,6 +162,7 @@ int Server::wait(uint64_t id, uint32_t timeout_ms) {
 }
 
 bool Server::admit(Launch& L) {
+    NvtxRange range("server: admit");
     L.jobs.clear();
     L.owners.clear();
     size_t items = 0, bytes = 0;
@@ -114,6 +170,14 @@ bool Server::admit(Launch& L) {
     bool budget_stop = false;
     while (!pending_.empty() && items < cap && !budget_stop) {
         Request* r = pending_.front();
+        if (r->has_token && token_cancelled(r->token)) {
+            // the caller's token asks to stop: no further piece of r is launched
+            r->status = kErrCancelled;
+            drop_pending(r);
+            if (r->pieces_in_flight == 0) finalize(r);
+            cv_done_.notify_all();
+            continue;
+        }
         while (r->next_job < r->jobs.size() && items < cap) {
             const VerifyJob& J = r->jobs[r->next_job];
             const size_t take = std::min(J.count - r->next_item, cap - items);
@@ -158,13 +222,10 @@ void Server::complete(Launch& L, int rc) {
     const Clock::time_point now = Clock::now();
     for (Request* r : L.owners) {
         r->pieces_in_flight--;
-        if (rc != kOk) r->status = rc;
-        if (r->all_launched && r->pieces_in_flight == 0 && !r->done) {
-            r->done = true;
-            lat_us_.push_back(std::chrono::duration<double, std::micro>(now - r->t_submit).count());
-            items_done_ += r->items;
-            t_last_done_ = now;
-        }
+        if (rc != kOk && r->status == kOk) r->status = rc;
+        if (rc != kOk) drop_pending(r);    // the rest of a failed request is not launched
+        if (r->abandoned && r->status == kOk) r->status = kErrCancelled;
+        if (r->all_launched && r->pieces_in_flight == 0 && !r->done) finalize(r);
     }
     budget_used_ -= L.bytes;
     if (--in_flight_ == 0) busy_s_ += std::chrono::duration<double>(now - t_busy_since_).count();

@@ -33,6 +33,7 @@
 #include "backend.h"
 #include "batch.h"
 #include "keytable.h"
+#include "ufsecp/ufsecp_cancel.h"
 
 namespace uf {
 
@@ -68,11 +69,26 @@ public:
     int start(const ServerConfig& cfg);
     // Thread-safe.  The jobs' host buffers must stay valid until wait() for
     // this id has returned kOk; the verdicts are written into jobs[j].out.
-    int submit(const VerifyJob* jobs, size_t n_jobs, uint64_t* id);
+    int submit(const VerifyJob* jobs, size_t n_jobs, uint64_t* id) { return submit(jobs, n_jobs, nullptr, id); }
+    // Thread-safe.  `cancel` (may be null; copied) is polled by the scheduler
+    // before every launch that would take a piece of this request; once it
+    // answers non-zero the pieces not launched yet are dropped and the request
+    // ends with kErrCancelled, its verdict bytes cleared.  The predicate is
+    // called on the scheduler thread and must not call into the server.
+    int submit(const VerifyJob* jobs, size_t n_jobs, const ufsecp_cancel_token* cancel, uint64_t* id);
     // Thread-safe.  kOk once the request is complete (its record is then
     // released), kErrGpuQueue on timeout, kErrBadInput for an unknown id; a
-    // launch failure is returned as its error code.
+    // launch failure is returned as its error code, after the request's
+    // verdict bytes were cleared (fail closed).
     int wait(uint64_t id, uint32_t timeout_ms);
+    // Thread-safe.  Abandons a request: pieces not launched yet are dropped,
+    // pieces on the device finish (a kernel is not stopped) and cancel waits
+    // for them, at most timeout_ms.  kOk: the server has forgotten the request
+    // and touches its buffers no more; the verdict bytes are cleared unless the
+    // request had completed before the call.  kErrGpuQueue: pieces were still
+    // in flight at the timeout (nothing more will be launched for it; call
+    // cancel or wait again).  kErrBadInput: unknown id.
+    int cancel(uint64_t id, uint32_t timeout_ms);
     // Latency percentiles over the requests completed since the last reset.
     void stats(ServerStats* out, bool reset);
 
@@ -86,6 +102,9 @@ private:
         size_t next_job = 0, next_item = 0;      // first piece not yet launched
         uint32_t pieces_in_flight = 0;
         bool all_launched = false, done = false;
+        bool abandoned = false;                  // cancel() was called before completion
+        bool has_token = false;
+        ufsecp_cancel_token token{};
         int status = kOk;
         Clock::time_point t_submit;
     };
@@ -100,6 +119,8 @@ private:
     void loop();
     bool admit(Launch& L);               // under mu_
     void complete(Launch& L, int rc);    // under mu_
+    void finalize(Request* r);           // under mu_: r is done; clears its verdicts unless it succeeded
+    void drop_pending(Request* r);       // under mu_: r's pieces not launched yet are dropped
     // pinned + device staging of one item, and its key-table slot index and to-do entry
     static size_t bytes_per_item(int kind) { return 2 * (32 + (kind == 0 ? 33 : 32) + 64 + 1) + 8; }
 

@@ -321,6 +321,18 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_lanes(ufsecp_gpu_ctx* ctx, int kind
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_lanes(ufsecp_gpu_ctx* ctx, int kind, int* lanes_out,
                                                    uint32_t* items_out);
 
+/* Inversion group per kind (0 ECDSA, 1 BIP-340): 1 = every signature runs its
+ * own inversions (the variant kernels above); 64 or 128 = kernels whose
+ * blocks of that many threads share each modular inversion by Montgomery's
+ * trick (the P table's Z product, BIP-340's final Z, ECDSA's s^-1: one
+ * inversion per block and site instead of one per warp).  Applies to the main
+ * verify launches, not to the two-lane or small-launch paths.  The tuning file
+ * sets it per kind (ecdsa_inv_group / schnorr_inv_group, chosen by the
+ * autotuner); UFSECP_B200_INV_GROUP overrides both kinds; set_variant resets
+ * the kind to 1.  Verdicts do not depend on it. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_inversion_group(ufsecp_gpu_ctx* ctx, int kind, int group);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_inversion_group(ufsecp_gpu_ctx* ctx, int kind, int* group_out);
+
 /* RLC bucket chunk: the number of bucket points one thread sums before the
  * per-bucket merge.  The tuning file sets it per batch size (rlc_chunk_<n>;
  * the nearest tuned size in log scale applies, else 16).  set: 2..256 fixes it

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import ultrafastsecp256k1_b200 as uf
-from conftest import N, P, ecdsa_corpus, load_golden, rand_keys, schnorr_corpus
+from conftest import N, P, ecdsa_corpus, load_golden, opaque_rows_corpus, rand_keys, schnorr_corpus
 
 pytestmark = pytest.mark.gpu
 
@@ -431,6 +431,57 @@ def test_every_kernel_variant_matches_oracle(gpu_ctx, oracle, variant):
         gpu_ctx.set_variant(1, old[1])
         for k in (0, 1):
             gpu_ctx.set_small_variant(k, *old_small[k])
+
+
+@pytest.mark.parametrize("group", [64, 128])
+def test_inversion_groups_match_oracle(gpu_ctx, oracle, group):
+    """Block-wide batch inversion (ufsecp_gpu_ext_set_inversion_group): one
+    inversion per block of 64 / 128 signatures for the table, the BIP-340 final
+    Z and the ECDSA s.  Groups that hold invalid items (failed parses,
+    off-curve keys, tampered signatures, results at infinity from the edge
+    corpus) and partial last groups give the per-signature verdicts, through
+    the compact, opaque-row and collect forms, small and chunked calls."""
+    import ctypes
+    _, wy, e = load_golden()
+    saved = [(gpu_ctx.get_variant(k)[0], gpu_ctx.get_small_variant(k), gpu_ctx.get_lanes(k),
+              gpu_ctx.get_inversion_group(k)) for k in (0, 1)]
+    try:
+        for k in (0, 1):
+            gpu_ctx.set_variant(k, 4)              # no small-launch or two-lane path: every call is grouped
+            gpu_ctx.set_inversion_group(k, group)
+            assert gpu_ctx.get_inversion_group(k) == group
+        assert (gpu_ctx.ecdsa_verify_batch(wy["msgs"], wy["pubs"], wy["sigs"]) == wy["ref_valid"]).all()
+        assert (gpu_ctx.ecdsa_verify_batch(e["ecdsa_msgs"], e["ecdsa_pubs"], e["ecdsa_sigs"])
+                == e["ecdsa_ref_valid"]).all()
+        assert (gpu_ctx.schnorr_verify_batch(e["schnorr_msgs"], e["schnorr_pubs"], e["schnorr_sigs"])
+                == e["schnorr_ref_valid"]).all()
+        for n in (1, 63, 129, 700):
+            m, p, s = ecdsa_corpus(oracle, n, seed=900 + n, tamper=0.25)
+            assert (gpu_ctx.ecdsa_verify_batch(m, p, s) == oracle.ecdsa_verify_batch(m, p, s)).all()
+            mx, x, sx = schnorr_corpus(oracle, n, seed=950 + n, tamper=0.25)
+            assert (gpu_ctx.schnorr_verify_batch(mx, x, sx) == oracle.schnorr_verify_batch(mx, x, sx)).all()
+            kb = np.full(n, 5, np.uint8)
+            got = gpu_ctx.schnorr_verify_collect(mx, x, sx, kb)
+            assert (got == np.where(oracle.schnorr_verify_batch(mx, x, sx) == 1, 0, 5)).all()
+        rows = opaque_rows_corpus(oracle, 600, seed=990)
+        L = uf.load_library()
+        L.ufsecp_gpu_ecdsa_verify_opaque_rows.argtypes = [uf._vp, uf._vp, ctypes.c_size_t, ctypes.c_size_t, uf._vp]
+        got = np.full(len(rows), 9, np.uint8)
+        assert L.ufsecp_gpu_ecdsa_verify_opaque_rows(gpu_ctx.handle, rows.ctypes.data, 129, len(rows),
+                                                     got.ctypes.data) == uf.UFSECP_OK
+        assert (got == oracle.ecdsa_verify_opaque_rows(rows, 129)).all()
+        # a call of several pipeline chunks (16k, 32k, 64k, 128k items ...)
+        mx, x, sx = schnorr_corpus(oracle, 3000, seed=991, tamper=0.05)
+        want = oracle.schnorr_verify_batch(mx, x, sx)
+        big = [np.ascontiguousarray(np.concatenate([a] * 70)) for a in (mx, x, sx)]
+        assert (gpu_ctx.schnorr_verify_batch(*big) == np.concatenate([want] * 70)).all()
+    finally:
+        for k in (0, 1):
+            v, small, lanes, grp = saved[k]
+            gpu_ctx.set_variant(k, v)
+            gpu_ctx.set_small_variant(k, *small)
+            gpu_ctx.set_lanes(k, *lanes)
+            gpu_ctx.set_inversion_group(k, grp)
 
 
 def test_two_lanes_per_signature_match_oracle(gpu_ctx, oracle):

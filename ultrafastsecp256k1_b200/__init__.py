@@ -140,6 +140,8 @@ _SIGS = {
     "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_set_key_table": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_set_inversion_group": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "ufsecp_gpu_ext_get_inversion_group": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "ufsecp_gpu_ext_inject_fault": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_int]),
     "ufsecp_gpu_ext_engine_hook_inject_fault": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int]),
     "ufsecp_gpu_ext_server_submit_cancellable": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_size_t, _vp,
@@ -397,6 +399,16 @@ class GpuContext:
         self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, tab.ctypes.data_as(ctypes.POINTER(Job)), kinds.size),
                     "verify_jobs")
         return outs
+
+    def set_inversion_group(self, kind: int, group: int):
+        """ufsecp_gpu_ext_set_inversion_group: 1, 64 or 128 threads share each inversion."""
+        self._check(self.L.ufsecp_gpu_ext_set_inversion_group(self._ctx, kind, group), "set_inversion_group")
+
+    def get_inversion_group(self, kind: int) -> int:
+        g = ctypes.c_int()
+        self._check(self.L.ufsecp_gpu_ext_get_inversion_group(self._ctx, kind, ctypes.byref(g)),
+                    "get_inversion_group")
+        return g.value
 
     def set_key_table(self, log2_slots: int):
         """ufsecp_gpu_ext_set_key_table: 0 = no resident key table for verify_jobs,

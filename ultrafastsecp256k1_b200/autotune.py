@@ -6,9 +6,10 @@ For each signature kind (ECDSA, BIP-340) it times every verify-kernel variant
 (ufsecp_gpu_ext_set_variant; the variants differ in how much field / point
 arithmetic is inlined, i.e. instruction-cache footprint against call
 overhead) on a GPU-signed batch, checks that all variants return identical
-verdicts, and picks them, plus a small-launch variant and its item limit for
-latency-bound launches (a few warps per SM) and the call size up to which two
-lanes per signature beat one; then, for RLC batch verification, it times the
+verdicts, and picks them, plus the inversion group (threads of a block that
+share each modular inversion: 1, 64 or 128), a small-launch variant and its
+item limit for latency-bound launches (a few warps per SM) and the call size
+up to which two lanes per signature beat one; then, for RLC batch verification, it times the
 Pippenger window width (the MSM bucket width, 2^(c-1) buckets per window)
 for each batch size of 64 / 512 / 4096 / 16384 over the model's choice and
 its neighbours and picks the fastest.  The winners go to a tuning file of
@@ -123,6 +124,26 @@ def tune_lanes(ctx, torch, kind, bufs, reps: int = 10) -> dict:
     return {"items": items, "sigs_per_s": {str(l): {str(n): r for n, r in rs.items()} for l, rs in rates.items()}}
 
 
+INV_GROUPS = (1, 64, 128)
+
+
+def tune_inversion_group(ctx, torch, kind, bufs, n, ref, reps: int = 3) -> dict:
+    """Threads per block that share each modular inversion (Montgomery's trick
+    across a block, ufsecp_gpu_ext_set_inversion_group): 1 (every signature
+    alone, the tuned variant), 64 or 128, timed at the main batch size with the
+    main variant in place; every group must reproduce the verdicts."""
+    rates = {}
+    for g in INV_GROUPS:
+        ctx.set_inversion_group(kind, g)
+        rate, verdicts = time_variant(ctx, torch, kind, bufs, n, reps)
+        if not (verdicts == ref).all():
+            raise RuntimeError(f"inversion group {g} disagrees with the variants")
+        rates[g] = rate
+    best = max(rates, key=rates.get)
+    ctx.set_inversion_group(kind, best)
+    return {"best": best, "sigs_per_s": {str(g): r for g, r in rates.items()}}
+
+
 def model_window(n: int) -> int:
     """The backend's cost model (rlc_window_bits in csrc/rlc.cu)."""
     best, cost = 4, float("inf")
@@ -216,10 +237,11 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
             best = max(rates, key=rates.get)
             small = tune_small(ctx, torch, kind, bufs, best)
             ctx.set_variant(kind, best)
+            group = tune_inversion_group(ctx, torch, kind, bufs, batch, ref)
             if small["variant"] is not None:
                 ctx.set_small_variant(kind, small["variant"], small["items"])
             res["kinds"][label] = {"sigs_per_s": {str(k): r for k, r in rates.items()}, "best": best,
-                                   "valid": int(ref.sum()), "small": small,
+                                   "valid": int(ref.sum()), "small": small, "inversion_group": group,
                                    "lanes": tune_lanes(ctx, torch, kind, bufs)}
         res["rlc_window"] = tune_rlc(ctx, torch)
         res["rlc_chunk"] = tune_rlc_chunk(ctx, torch, res["rlc_window"])
@@ -230,6 +252,7 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
             for label in ("ecdsa", "schnorr"):
                 k = res["kinds"][label]
                 f.write(f"{label}_variant {k['best']}\n")
+                f.write(f"{label}_inv_group {k['inversion_group']['best']}\n")
                 if k["small"]["variant"] is not None:
                     f.write(f"{label}_small_variant {k['small']['variant']}\n")
                     f.write(f"{label}_small_items {k['small']['items']}\n")

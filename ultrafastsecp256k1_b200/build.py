@@ -56,6 +56,7 @@ _VARIANT_FLAGS = [
 _BEST_FLAGS = ["-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]
 VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS, "kernels_probe.cu": _VARIANT_FLAGS,
             "kernels_queue.cu": [("", _BEST_FLAGS)], "kernels_noalloc.cu": [("", _BEST_FLAGS)],
+            "kernels_verify_grp.cu": [("", _BEST_FLAGS)],
             # small calls are latency-bound: the two-lane kernel takes variant 6's
             # code generation (field ops inlined into out-of-line point ops)
             "kernels_pair.cu": [("", ["-DUF_NOINLINE_POINT", "-DUF_PTX_MUL"])],

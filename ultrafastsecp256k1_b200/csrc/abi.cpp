@@ -642,6 +642,18 @@ ufsecp_error_t ufsecp_gpu_ext_get_lanes(ufsecp_gpu_ctx* ctx, int kind, int* lane
     return UFSECP_OK;
 }
 
+ufsecp_error_t ufsecp_gpu_ext_set_inversion_group(ufsecp_gpu_ctx* ctx, int kind, int group) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    return ctx->backend->set_inversion_group(kind, group);
+}
+
+ufsecp_error_t ufsecp_gpu_ext_get_inversion_group(ufsecp_gpu_ctx* ctx, int kind, int* group_out) {
+    if (!ctx || !group_out) return UFSECP_ERR_NULL_ARG;
+    if (kind < 0 || kind > 1) return UFSECP_ERR_BAD_INPUT;
+    *group_out = ctx->backend->inversion_group(kind);
+    return UFSECP_OK;
+}
+
 ufsecp_error_t ufsecp_gpu_ext_set_rlc_chunk(ufsecp_gpu_ctx* ctx, uint32_t chunk) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     return ctx->backend->set_rlc_chunk(chunk);

@@ -49,8 +49,21 @@ cudaError_t Backend::launch_verify(int kind, const uint8_t* m, const uint8_t* p,
     const int k = kind & 1;
     if (kind != 2 && call_items <= pair_items_[k])
         return launch_verify_pair(kind, m, p, s, n, d_gtab_, out, collect, st);
-    const int v = small_variant_[k] >= 0 && call_items <= small_items_[k] ? small_variant_[k] : variant_[k];
+    const bool small = small_variant_[k] >= 0 && call_items <= small_items_[k];
+    if (!small && inv_group_[k] > 1) {
+        const int gi = inv_group_[k] == 64 ? 0 : 1;
+        return launch_verify_grp(inv_group_[k], kind, m, p, s, n, d_gtab_, out, collect, grp_grid_[gi][k], st);
+    }
+    const int v = small ? small_variant_[k] : variant_[k];
     return kLaunchers[v](kind, m, p, s, n, d_gtab_, out, collect, grid_[v][k], st);
+}
+
+int Backend::set_inversion_group(int kind, int group) {
+    if (kind < 0 || kind > 1 || (group != 1 && group != 64 && group != 128))
+        return set_error(kErrBadInput, "inversion group must be 1, 64 or 128");
+    inv_group_[kind] = group;
+    clear_error();
+    return kOk;
 }
 
 int Backend::set_variant(int kind, int v) {
@@ -58,6 +71,7 @@ int Backend::set_variant(int kind, int v) {
     variant_[kind] = v;
     small_variant_[kind] = -1;   // an explicit choice applies to every launch size
     pair_items_[kind] = 0;
+    inv_group_[kind] = 1;
     clear_error();
     return kOk;
 }
@@ -134,6 +148,8 @@ void Backend::load_tuning() {
                     rlc_chunk_[size] = (uint32_t)val;
                 if (!strcmp(key, "key_table_log2") && (val == 0 || (val >= 8 && val <= 24)))
                     key_log2_ = (uint32_t)val;
+                if (!strcmp(key, "ecdsa_inv_group") && (val == 1 || val == 64 || val == 128)) inv_group_[0] = val;
+                if (!strcmp(key, "schnorr_inv_group") && (val == 1 || val == 64 || val == 128)) inv_group_[1] = val;
             }
             fclose(f);
         }
@@ -153,12 +169,16 @@ void Backend::load_tuning() {
         variant_[0] = ve;
         small_variant_[0] = -1;
         pair_items_[0] = 0;
+        inv_group_[0] = 1;
     }
     if (vs >= 0 && vs < kVerifyVariants) {
         variant_[1] = vs;
         small_variant_[1] = -1;
         pair_items_[1] = 0;
+        inv_group_[1] = 1;
     }
+    const int ig = env_int("UFSECP_B200_INV_GROUP", 0);
+    if (ig == 1 || ig == 64 || ig == 128) inv_group_[0] = inv_group_[1] = ig;
 }
 
 cudaError_t DevBuf::ensure(size_t bytes) {
@@ -311,6 +331,8 @@ int Backend::init(int device_index) {
     for (int v = 0; v < kVerifyVariants; ++v)
         for (int k = 0; k < 2; ++k) grid_[v][k] = std::max(1, kOccupancy[v](k)) * sms_;
     queue_grid_ = std::max(1, verify_queue_occupancy()) * sms_;
+    for (int gi = 0; gi < 2; ++gi)
+        for (int k = 0; k < 2; ++k) grp_grid_[gi][k] = std::max(1, verify_grp_occupancy(gi ? 128 : 64, k)) * sms_;
     queue_pair_grid_ = std::max(1, verify_pair_occupancy()) * sms_;   // also the two-lane kernels' shared-memory opt-in
     load_tuning();
     (void)cudaGetLastError();

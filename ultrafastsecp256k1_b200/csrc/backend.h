@@ -125,6 +125,13 @@ public:
     int set_variant(int kind, int v);
     int set_small_variant(int kind, int v, uint32_t items);   // v = -1: none
     int set_lanes(int kind, int lanes, uint32_t items);       // lanes 2 for calls of <= items, 1: never
+    // Inversion group per kind: 1 = every signature inverts alone (the
+    // variant kernels), 64 / 128 = the block-wide batch-inversion kernels with
+    // that many threads per block share each inversion.  Applies to the main
+    // launches (not the two-lane or small-launch paths).  set_variant resets
+    // it to 1.
+    int set_inversion_group(int kind, int group);
+    int inversion_group(int kind) const { return inv_group_[kind & 1]; }
     uint32_t pair_items(int kind) const { return pair_items_[kind & 1]; }
     int verify_grid(int kind) const { return grid_[variant_[kind & 1]][kind & 1]; }
     int blocks_per_sm(int kind, int v) const { return sms_ ? grid_[v][kind & 1] / sms_ : 0; }
@@ -163,6 +170,8 @@ private:
     // per signature (kernels_pair.cu); 0 = never.  Also cleared by an explicit
     // variant choice.
     uint32_t pair_items_[2] = {0, 0};
+    int inv_group_[2] = {1, 1};
+    int grp_grid_[2][2] = {};    // [64, 128][kind] resident-grid size of the batch-inversion kernels
     // call_items: the size of the whole call this launch belongs to; the
     // small-launch variant is used only when the whole call is small (the
     // chunks of a large call run beside one another at full occupancy).

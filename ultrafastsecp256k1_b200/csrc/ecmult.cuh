@@ -57,11 +57,15 @@ UF_HD void booth_recode(T* out, const uint32_t k[4]) {
     }
 }
 
-// Table of (k+1)*P for k = 0..7, affine.  Tab must provide
-// store(k, Fe x, Fe y) / load(k, Fe& x, Fe& y).
+// Table of (k+1)*P for k = 0..7, affine, in two halves around its one field
+// inversion, so that a block of signatures can share that inversion
+// (Montgomery's trick across threads, grpinv.cuh).  _pre stores 1P..8P with
+// their Jacobian X, Y in `tab` (1P affine), the Z of 2P..8P in zs and their
+// running products in cs; cs[kPTab - 2] is the product of all of them.  _post
+// turns the entries affine from `inv`, the inverse of that product.  Tab must
+// provide store(k, Fe x, Fe y) / load(k, Fe& x, Fe& y).
 template <class Tab>
-UF_HDI void build_ptable(Tab& tab, const Fe& px, const Fe& py) {
-    Fe zs[kPTab - 1], cs[kPTab - 1];
+UF_HDI void build_ptable_pre(Tab& tab, const Fe& px, const Fe& py, Fe zs[kPTab - 1], Fe cs[kPTab - 1]) {
     tab.store(0, px, py);
     UF_NOUNROLL
     for (int k = 2; k <= kPTab; ++k) {
@@ -85,9 +89,10 @@ UF_HDI void build_ptable(Tab& tab, const Fe& px, const Fe& py) {
         if (k == 2) cs[0] = t.Z;
         else fe_mul(cs[k - 2], cs[k - 3], t.Z);
     }
-    // one inversion for all seven Z (Montgomery's trick)
-    Fe inv;
-    fe_inv(inv, cs[kPTab - 2]);
+}
+
+template <class Tab>
+UF_HDI void build_ptable_post(Tab& tab, const Fe zs[kPTab - 1], const Fe cs[kPTab - 1], Fe inv) {
     UF_NOUNROLL
     for (int k = kPTab; k >= 2; --k) {
         Fe zi, zi2, X, Y;
@@ -104,6 +109,16 @@ UF_HDI void build_ptable(Tab& tab, const Fe& px, const Fe& py) {
         fe_mul(Y, Y, zi2);
         tab.store(k - 1, X, Y);
     }
+}
+
+// The whole table with its own inversion.
+template <class Tab>
+UF_HDI void build_ptable(Tab& tab, const Fe& px, const Fe& py) {
+    Fe zs[kPTab - 1], cs[kPTab - 1];
+    build_ptable_pre(tab, px, py, zs, cs);
+    Fe inv;
+    fe_inv(inv, cs[kPTab - 2]);
+    build_ptable_post(tab, zs, cs, inv);
 }
 
 template <class Tab>
@@ -127,6 +142,46 @@ UF_HD void add_gtab(Jac& R, const GT& gt, int d, bool sneg, int lam) {
     gt.load(idx, x, y);
     if (neg) fe_neg(y, y);
     jac_add_aff(R, x, y);
+}
+
+// Booth digits of the four GLV streams of R = a*G + b*P, for kernels that
+// split the computation into phases (kernels_verify_grp.cu).
+struct DualDigits {
+    int8_t dp1[kNWP], dp2[kNWP];
+    GDigit dg1[kNWG], dg2[kNWG];
+    bool np1, np2, ng1, ng2;
+};
+
+UF_HDI void dual_recode(DualDigits& d, const Sc& a, const Sc& b) {
+    GlvSplit sa, sb;
+    glv_split(sa, a);
+    glv_split(sb, b);
+    booth_recode<kWP, kNWP>(d.dp1, sb.k1);
+    booth_recode<kWP, kNWP>(d.dp2, sb.k2);
+    booth_recode<kWG, kNWG>(d.dg1, sa.k1);
+    booth_recode<kWG, kNWG>(d.dg2, sa.k2);
+    d.np1 = sb.neg1;
+    d.np2 = sb.neg2;
+    d.ng1 = sa.neg1;
+    d.ng2 = sa.neg2;
+}
+
+// The main loop over recoded digits: 128 doublings, the P-table and G-table additions.
+template <class Tab, class GT>
+UF_HDI void dual_loop(Jac& R, const DualDigits& d, const Tab& tab, const GT& gt) {
+    Fe beta;
+    fe_beta(beta);
+    jac_set_inf(R);
+    UF_NOUNROLL
+    for (int i = kNWP - 1; i >= 0; --i) {
+        if (i != kNWP - 1) jac_dbl_n(R, kWP);
+        add_ptab(R, tab, d.dp1[i], d.np1, false, beta);
+        add_ptab(R, tab, d.dp2[i], d.np2, true, beta);
+        if (i % kGEvery == 0) {
+            add_gtab(R, gt, d.dg1[i / kGEvery], d.ng1, 0);
+            add_gtab(R, gt, d.dg2[i / kGEvery], d.ng2, 1);
+        }
+    }
 }
 
 // R = a*G + b*P for P = (px, py) on the curve (not infinity).  With

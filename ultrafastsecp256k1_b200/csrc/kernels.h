@@ -60,6 +60,14 @@ int verify_occupancy_v6(int kind);
 int verify_occupancy_v7(int kind);
 int verify_occupancy_v8(int kind);
 
+// The same verify with block-wide batch inversion (kernels_verify_grp.cu):
+// the table, final-Z and ECDSA s inversions are shared by the `group` (64 or
+// 128) threads of a block.  `grid` resident blocks from verify_grp_occupancy,
+// which also opts the kernels in to their shared memory.
+cudaError_t launch_verify_grp(int group, int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs,
+                              uint32_t n, const void* d_gtab, uint8_t* out, int collect, int grid, cudaStream_t s);
+int verify_grp_occupancy(int group, int kind);
+
 // Per-item batch operations (kernels_ops.cu); device pointers, asynchronous.
 cudaError_t launch_xonly_validate(const uint8_t* keys32, uint32_t n, uint8_t* out, int sms, cudaStream_t s);
 cudaError_t launch_pubkey_validate(const uint8_t* pubs33, uint32_t n, uint8_t* out, int sms, cudaStream_t s);

@@ -137,10 +137,26 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc_device(ufsecp_gpu_ct
                                                                    size_t batch_size, const uint8_t* seed32,
                                                                    int window_bits, uint8_t* d_out_results,
                                                                    uint8_t* out_batch_ok, void* stream);
-/* Counters of the context's last RLC call: out[0] MSM rounds (the first check
- * plus one per bisection level), out[1] segments checked, out[2] items
- * verified one by one, out[3] window bits of the first round. */
+/* Counters of the context's last RLC call: out[0] MSM rounds (the first check,
+ * one per bisection level and one per locate step), out[1] segments checked
+ * (locate rounds included), out[2] items verified one by one (bisection
+ * leaves and locate candidates), out[3] window bits of the first round.
+ * rlc_located: failing segments the locate step resolved. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_stats(ufsecp_gpu_ctx* ctx, uint64_t out[4]);
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_located(ufsecp_gpu_ctx* ctx, uint64_t* located);
+
+/* Locate step of RLC verification (on = 1, the default; 0 = bisection only).
+ * A failing batch S with sum T = sum a_i D_i != infinity (D_i = R_i + e_i P_i
+ * - s_i G, infinity exactly for a valid item) first gets one more
+ * multi-scalar multiplication with every weight a_i multiplied by its position
+ * j_i = i - start + 1, T' = sum j_i a_i D_i.  With one invalid item j,
+ * T' = j T, and a baby-step giant-step search over the multiples 1 .. |S| of T
+ * (one block per segment) finds j; the candidate is verified by the plain
+ * kernel and, when invalid, resolves S in two rounds instead of one per
+ * bisection level.  With two or more invalid items no multiple matches (but
+ * for a 2^-128 event over the weights) and S is bisected as before; verdicts
+ * never depend on the search.  Segments of at most 65,535 items. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_rlc_locate(ufsecp_gpu_ctx* ctx, int on);
 
 /* Input binding of the reference-shaped batch API's seed: the SHA-256 tree
  * digest of n BIP-340 items (host buffers, layouts as above).  Per item

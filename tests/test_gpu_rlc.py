@@ -62,11 +62,60 @@ def test_rlc_one_batch(gpu_ctx, oracle, n, bad):
     assert bok.tolist() == [0 if bad else 1]
     st = gpu_ctx.rlc_stats()
     if bad:
-        # eight-way splits down to the leaf (<= 32 items) that holds the invalid item
-        rounds, leaf = _bisection(n, int(np.flatnonzero(want == 0)[0]))
-        assert st["rounds"] == rounds and st["leaf_items"] == leaf
+        # the locate round finds the single invalid item: check + locate, one candidate verified
+        assert st["rounds"] == 2 and st["leaf_items"] == 1 and st["located"] == 1
     else:
         assert st["rounds"] == 1 and st["leaf_items"] == 0 and st["segments"] == 1
+    if bad:
+        # bisection alone: eight-way splits down to the leaf (<= 32 items) that holds it
+        try:
+            gpu_ctx.set_rlc_locate(False)
+            out2, _ = gpu_ctx.schnorr_verify_rlc(m, x, s, batch_size=n, seed32=SEED)
+            assert (out2 == want).all()
+            st = gpu_ctx.rlc_stats()
+            rounds, leaf = _bisection(n, int(np.flatnonzero(want == 0)[0]))
+            assert st["rounds"] == rounds and st["leaf_items"] == leaf and st["located"] == 0
+        finally:
+            gpu_ctx.set_rlc_locate(True)
+
+
+@pytest.mark.parametrize("where", ["first", "last", "two", "three_spread"])
+def test_rlc_locate_positions_and_multiples(gpu_ctx, oracle, where):
+    """The locate step at the segment's first and last position (j = 1 and
+    j = len), and with two or three invalid items in one segment (no multiple
+    matches: the segment is bisected and its children located)."""
+    n = 4096
+    m, x, s = schnorr_corpus(oracle, n, seed=1300, tamper=0.0)
+    m = m.copy()
+    bad = {"first": [0], "last": [n - 1], "two": [100, 101], "three_spread": [7, 2000, 4095]}[where]
+    for i in bad:
+        _flip(m, i)
+    out, bok = gpu_ctx.schnorr_verify_rlc(m, x, s, batch_size=n, seed32=SEED)
+    want = oracle.schnorr_verify_batch(m, x, s)
+    assert (out == want).all()
+    assert sorted(np.flatnonzero(out == 0).tolist()) == bad
+    st = gpu_ctx.rlc_stats()
+    if len(bad) == 1:
+        assert st["located"] == 1 and st["leaf_items"] == 1
+    else:
+        assert st["located"] >= 1
+
+
+def test_rlc_locate_segment_limits(gpu_ctx, oracle):
+    """A 65,535-item batch (the longest a locate round searches) and a
+    69,632-item one (longer: bisected first, then its failing child located),
+    one invalid item each; tiled corpora (repeated items share buckets)."""
+    m0, x0, s0 = schnorr_corpus(oracle, 4096, seed=1301, tamper=0.0)
+    for n, bad_i in ((65535, 40000), (69632, 69000)):
+        reps = -(-n // 4096)
+        m, x, s = (np.ascontiguousarray(np.concatenate([a] * reps)[:n]) for a in (m0, x0, s0))
+        _flip(m, bad_i)
+        out, bok = gpu_ctx.schnorr_verify_rlc(m, x, s, batch_size=n, seed32=SEED)
+        assert np.flatnonzero(out == 0).tolist() == [bad_i]
+        assert bok.tolist() == [0]
+        st = gpu_ctx.rlc_stats()
+        assert st["located"] == 1 and st["leaf_items"] == 1
+        assert st["rounds"] == (2 if n <= 65535 else 3)
 
 
 def test_rlc_many_ragged_batches_dense_invalid(gpu_ctx, oracle):

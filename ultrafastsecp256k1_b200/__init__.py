@@ -140,6 +140,8 @@ _SIGS = {
     "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_set_key_table": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "ufsecp_gpu_ext_set_rlc_locate": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "ufsecp_gpu_ext_rlc_located": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_set_inversion_group": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "ufsecp_gpu_ext_get_inversion_group": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "ufsecp_gpu_ext_inject_fault": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_int]),
@@ -453,7 +455,13 @@ class GpuContext:
     def rlc_stats(self) -> dict:
         v = (ctypes.c_uint64 * 4)()
         self._check(self.L.ufsecp_gpu_ext_rlc_stats(self._ctx, v), "rlc_stats")
-        return {"rounds": v[0], "segments": v[1], "leaf_items": v[2], "window_bits": v[3]}
+        loc = ctypes.c_uint64()
+        self._check(self.L.ufsecp_gpu_ext_rlc_located(self._ctx, ctypes.byref(loc)), "rlc_located")
+        return {"rounds": v[0], "segments": v[1], "leaf_items": v[2], "window_bits": v[3], "located": loc.value}
+
+    def set_rlc_locate(self, on: bool):
+        """ufsecp_gpu_ext_set_rlc_locate: the locate step of RLC verification on / off."""
+        self._check(self.L.ufsecp_gpu_ext_set_rlc_locate(self._ctx, 1 if on else 0), "set_rlc_locate")
 
     def rlc_input_digest(self, msg_hashes32, pubkeys_x32, sigs64) -> bytes:
         """ufsecp_gpu_ext_rlc_input_digest: the SHA-256 tree digest that binds the

@@ -654,6 +654,13 @@ ufsecp_error_t ufsecp_gpu_ext_get_inversion_group(ufsecp_gpu_ctx* ctx, int kind,
     return UFSECP_OK;
 }
 
+ufsecp_error_t ufsecp_gpu_ext_set_rlc_locate(ufsecp_gpu_ctx* ctx, int on) {
+    if (!ctx) return UFSECP_ERR_NULL_ARG;
+    if (on != 0 && on != 1) return ctx->backend->set_error(UFSECP_ERR_BAD_INPUT, "locate must be 0 or 1");
+    ctx->backend->set_rlc_locate(on != 0);
+    return UFSECP_OK;
+}
+
 ufsecp_error_t ufsecp_gpu_ext_set_rlc_chunk(ufsecp_gpu_ctx* ctx, uint32_t chunk) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     return ctx->backend->set_rlc_chunk(chunk);
@@ -820,6 +827,12 @@ ufsecp_error_t ufsecp_gpu_ext_rlc_stats(ufsecp_gpu_ctx* ctx, uint64_t out[4]) {
     out[1] = ctx->rlc_stats.segments;
     out[2] = ctx->rlc_stats.leaf_items;
     out[3] = (uint64_t)ctx->rlc_stats.window_bits;
+    return UFSECP_OK;
+}
+
+ufsecp_error_t ufsecp_gpu_ext_rlc_located(ufsecp_gpu_ctx* ctx, uint64_t* located) {
+    if (!ctx || !located) return UFSECP_ERR_NULL_ARG;
+    *located = ctx->rlc_stats.located;
     return UFSECP_OK;
 }
 

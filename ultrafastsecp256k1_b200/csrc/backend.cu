@@ -148,6 +148,7 @@ void Backend::load_tuning() {
                     rlc_chunk_[size] = (uint32_t)val;
                 if (!strcmp(key, "key_table_log2") && (val == 0 || (val >= 8 && val <= 24)))
                     key_log2_ = (uint32_t)val;
+                if (!strcmp(key, "rlc_locate") && (val == 0 || val == 1)) rlc_locate_ = val != 0;
                 if (!strcmp(key, "ecdsa_inv_group") && (val == 1 || val == 64 || val == 128)) inv_group_[0] = val;
                 if (!strcmp(key, "schnorr_inv_group") && (val == 1 || val == 64 || val == 128)) inv_group_[1] = val;
             }
@@ -162,6 +163,8 @@ void Backend::load_tuning() {
     if (kt == 0 || (kt >= 8 && kt <= 24)) key_log2_ = (uint32_t)kt;
     const int pt = env_int("UFSECP_B200_PACK_THREADS", 0);
     if (pt >= 1 && pt <= 16) pack_threads_ = pt;
+    const int lo_env = env_int("UFSECP_B200_RLC_LOCATE", -1);
+    if (lo_env == 0 || lo_env == 1) rlc_locate_ = lo_env != 0;
     const int rc_env = env_int("UFSECP_B200_RLC_CHUNK", 0);
     if (rc_env >= 2 && rc_env <= 256) rlc_chunk_fixed_ = (uint32_t)rc_env;
     const int ve = env_int("UFSECP_B200_VARIANT_ECDSA", -1), vs = env_int("UFSECP_B200_VARIANT_SCHNORR", -1);

@@ -101,6 +101,11 @@ public:
     uint32_t rlc_chunk(uint32_t len) const;
     // 2..256 fixes the chunk for every segment length; 0 restores the tuned values.
     int set_rlc_chunk(uint32_t chunk);
+    // Whether a failing RLC segment first gets a locate round (one more MSM
+    // that finds a single invalid item) before it is bisected.  On by default;
+    // the tuning file's rlc_locate or UFSECP_B200_RLC_LOCATE may turn it off.
+    bool rlc_locate() const { return rlc_locate_; }
+    void set_rlc_locate(bool on) { rlc_locate_ = on; }
     int queue_grid() const { return queue_grid_; }
     int queue_pair_grid() const { return queue_pair_grid_; }
     // Mixed-job launches of at most this many items (both kinds together) run
@@ -207,6 +212,7 @@ private:
     std::map<uint32_t, int> rlc_window_;   // tuned window bits per RLC batch size
     std::map<uint32_t, uint32_t> rlc_chunk_;  // tuned bucket points per chunk thread per RLC batch size
     uint32_t rlc_chunk_fixed_ = 0;            // set_rlc_chunk / UFSECP_B200_RLC_CHUNK override, 0 = tuned
+    bool rlc_locate_ = true;
     int last_err_ = kOk;
     std::string last_msg_ = "OK";
     std::atomic<long long> fault_after_{-1};

@@ -71,10 +71,10 @@ __device__ __forceinline__ void load_jac(const uint4* q, Jac& P) {
     P.inf = q[6].x != 0;
 }
 
-// Signed digit of window w (c bits) of a magnitude m < 2^128 (the recoding of
-// booth_recode in ecmult.cuh with a run-time window width).
-__device__ __forceinline__ int booth_digit(const uint4 m, int w, int c) {
-    const uint32_t k[6] = {m.x, m.y, m.z, m.w, 0u, 0u};
+// Signed digit of window w (c bits) of a magnitude m + hi 2^128 < 2^160 (the
+// recoding of booth_recode in ecmult.cuh with a run-time window width).
+__device__ __forceinline__ int booth_digit(const uint4 m, uint32_t hi, int w, int c) {
+    const uint32_t k[6] = {m.x, m.y, m.z, m.w, hi, 0u};
     const int pos = c * w - 1;
     const uint32_t mask = (1u << (c + 1)) - 1u;
     uint32_t raw;
@@ -200,9 +200,11 @@ __device__ __forceinline__ uint32_t upper_index(const uint32_t* __restrict__ a, 
 
 // Per segment: sum of t_i and count of unparsed items; then the magnitudes of
 // the two generator points from the GLV split of -sum t_i.
+// With `scaled` (the locate round) item i of a segment starting at i0 enters
+// with the weight j = i - i0 + 1: the sum is of j t_i.
 __global__ void __launch_bounds__(256)
 k_rlc_tsum(RoundGeo g, const uint32_t* __restrict__ tsc, const uint8_t* __restrict__ okb,
-           uint4* __restrict__ segmag, uint8_t* __restrict__ segneg, uint32_t* __restrict__ segbad) {
+           uint4* __restrict__ segmag, uint8_t* __restrict__ segneg, uint32_t* __restrict__ segbad, int scaled) {
     __shared__ uint32_t red[8][256];
     __shared__ uint32_t bad;
     const uint32_t s = blockIdx.x, tid = threadIdx.x;
@@ -218,6 +220,12 @@ k_rlc_tsum(RoundGeo g, const uint32_t* __restrict__ tsc, const uint8_t* __restri
         const uint4 lo = q[0], hi = q[1];
         t.v[0] = lo.x; t.v[1] = lo.y; t.v[2] = lo.z; t.v[3] = lo.w;
         t.v[4] = hi.x; t.v[5] = hi.y; t.v[6] = hi.z; t.v[7] = hi.w;
+        if (scaled) {
+            Sc jj;
+            jj.v[0] = i - i0 + 1;
+            for (int k = 1; k < 8; ++k) jj.v[k] = 0;
+            sc_mul(t, t, jj);
+        }
         sc_add(acc, acc, t);
         nbad += okb[i] ? 0u : 1u;
     }
@@ -256,21 +264,22 @@ k_rlc_tsum(RoundGeo g, const uint32_t* __restrict__ tsc, const uint8_t* __restri
 // them at the scanned offsets (order within a bucket is arbitrary: bucket sums
 // do not depend on it).
 __global__ void __launch_bounds__(256)
-k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint4* __restrict__ segmag,
-             const uint8_t* __restrict__ segneg, uint32_t total, uint32_t* __restrict__ counts,
-             uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries, int pass) {
+k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint32_t* __restrict__ mags_hi,
+             const uint4* __restrict__ segmag, const uint8_t* __restrict__ segneg, uint32_t total,
+             uint32_t* __restrict__ counts, uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries, int pass) {
     const uint32_t W = (uint32_t)g.W;
     const uint32_t tp = blockIdx.x * blockDim.x + threadIdx.x;     // point of the round
     if (tp >= total / W) return;
     const uint32_t s = upper_index(g.pwf, g.n_seg, tp * W);
     const uint32_t p = tp - g.pwf[s] / W;
     const uint32_t len = g.seg[2 * s + 1];
-    uint32_t pidx;
+    uint32_t pidx, mhi = 0;
     uint4 m;
     bool neg = false;
     if (p < 3u * len) {
         pidx = 3u * g.seg[2 * s] + p;
         m = mags[pidx];
+        if (mags_hi) mhi = mags_hi[pidx];
     } else {
         const uint32_t j = 2u * s + (p - 3u * len);
         pidx = g.n3 + j;
@@ -279,7 +288,7 @@ k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint4* __restrict
     }
     const uint32_t key0 = s * W * (uint32_t)g.B;
     for (uint32_t w = 0; w < W; ++w) {
-        const int d = booth_digit(m, (int)w, g.c);
+        const int d = booth_digit(m, mhi, (int)w, g.c);
         if (d == 0) continue;
         const uint32_t key = key0 + w * (uint32_t)g.B + (uint32_t)((d < 0 ? -d : d) - 1);
         if (pass == 0) {
@@ -403,6 +412,114 @@ k_rlc_finish(RoundGeo g, const uint4* __restrict__ wins, const uint32_t* __restr
     }
     segok[s] = (uint8_t)((acc.inf ? 1 : 0) | (segbad[s] ? 2 : 0));
     store_jac(segpt + kJacQ * (uint64_t)s, acc);
+}
+
+// ---------------------------------------------------------------- locate --
+// A failing segment S (its sum T = sum a_i D_i != infinity, D_i the defect of
+// item i: R_i + e_i P_i - s_i G, infinity for a valid item) with exactly one
+// invalid item j has T = a_j D_j.  The locate round computes, with the same
+// MSM, T' = sum (i - i0 + 1) a_i D_i, which is then (j - i0 + 1) T, and a
+// baby-step giant-step search over the multiples 1 .. len of T recovers j.
+// With two or more invalid items T' is no such multiple (but for a 2^-128
+// event over the weights), nothing is found and the segment is bisected.  The
+// candidate is verified by the plain kernel, so a verdict never rests on the
+// search.
+
+// Per item of the listed segments: its three magnitudes times j = i - i0 + 1
+// (up to 129 + 17 bits: four words in lmags, the fifth in lmags_hi).
+__global__ void __launch_bounds__(256)
+k_rlc_scale(const uint32_t* __restrict__ seg, const uint4* __restrict__ mags, uint4* __restrict__ lmags,
+            uint32_t* __restrict__ lmags_hi) {
+    const uint32_t s = blockIdx.x;
+    const uint32_t i0 = seg[2 * s], len = seg[2 * s + 1];
+    for (uint32_t k = threadIdx.x; k < 3u * len; k += blockDim.x) {
+        const uint64_t pidx = 3ull * i0 + k;
+        const uint32_t j = k / 3u + 1u;
+        const uint4 m = mags[pidx];
+        uint64_t c = (uint64_t)m.x * j;
+        uint4 r;
+        r.x = (uint32_t)c;
+        c = (uint64_t)m.y * j + (c >> 32);
+        r.y = (uint32_t)c;
+        c = (uint64_t)m.z * j + (c >> 32);
+        r.z = (uint32_t)c;
+        c = (uint64_t)m.w * j + (c >> 32);
+        r.w = (uint32_t)c;
+        lmags[pidx] = r;
+        lmags_hi[pidx] = (uint32_t)(c >> 32);
+    }
+}
+
+// P = k T for a small k >= 0 (double and add from the top bit).
+__device__ __forceinline__ void jac_small_mul(Jac& P, const Jac& T, uint32_t k) {
+    jac_set_inf(P);
+    for (int b = 31; b >= 0; --b) {
+        if (!P.inf) jac_dbl(P);
+        if ((k >> b) & 1u) jac_add(P, T);
+    }
+}
+
+// One block per segment to locate: T = tsave[s] (the segment's sum of the
+// check round), T' = tpr[s] (the locate round's).  With m = ceil(sqrt(len + 1))
+// (blockDim.x >= m), thread t computes the baby step t T and the giant step
+// T' - t m T, both affine; a giant step equal to baby step i gives
+// T' = (t m + i) T.  found[s] = that j in [1, len], or 0.
+__global__ void __launch_bounds__(256)
+k_rlc_locate(const uint4* __restrict__ tsave, const uint4* __restrict__ tpr, const uint32_t* __restrict__ seg,
+             uint32_t* __restrict__ found) {
+    __shared__ uint32_t bx[8][256], by[8][256];
+    __shared__ uint8_t binf[256];
+    const uint32_t s = blockIdx.x, t = threadIdx.x;
+    const uint32_t len = seg[2 * s + 1];
+    uint32_t m = 1;
+    while (m * m < len + 1) ++m;
+    if (t == 0) found[s] = 0;
+    Jac T, Tp;
+    load_jac(tsave + kJacQ * (uint64_t)s, T);
+    load_jac(tpr + kJacQ * (uint64_t)s, Tp);
+    if (t < m) {
+        Jac B;
+        jac_small_mul(B, T, t);
+        Aff a;
+        const bool fin = jac_to_aff(a, B);
+        binf[t] = fin ? 0 : 1;
+        for (int k = 0; k < 8; ++k) {
+            bx[k][t] = fin ? a.x.v[k] : 0u;
+            by[k][t] = fin ? a.y.v[k] : 0u;
+        }
+    }
+    __syncthreads();
+    if (t < m) {
+        Jac Q;
+        jac_small_mul(Q, T, t * m);
+        if (!Q.inf) {
+            fe_neg(Q.Y, Q.Y);
+            fe_normalize(Q.Y);
+        }
+        jac_add(Q, Tp);
+        Aff a;
+        const bool fin = jac_to_aff(a, Q);
+        for (uint32_t i = 0; i < m; ++i) {
+            bool eq;
+            if (!fin) {
+                eq = binf[i] != 0;
+            } else {
+                uint32_t d = binf[i];
+                for (int k = 0; k < 8; ++k) d |= (bx[k][i] ^ a.x.v[k]) | (by[k][i] ^ a.y.v[k]);
+                eq = d == 0;
+            }
+            const uint32_t j = t * m + i;
+            if (eq && j >= 1 && j <= len) atomicMax(&found[s], j);
+        }
+    }
+}
+
+// dst[k] = src[idx[k]] for Jacobian points (7 x uint4)
+__global__ void k_rlc_gather_pts(const uint32_t* __restrict__ idx, uint32_t m, const uint4* __restrict__ src,
+                                 uint4* __restrict__ dst) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    for (int q = 0; q < kJacQ; ++q) dst[kJacQ * (uint64_t)k + q] = src[kJacQ * (uint64_t)idx[k] + q];
 }
 
 __global__ void k_rlc_gather(const uint32_t* __restrict__ idx, uint32_t m, const uint8_t* __restrict__ msgs,
@@ -601,15 +718,23 @@ RlcVerifier::~RlcVerifier() {
     for (DevBuf* b : {&items_, &mags_, &tsc_, &okb_, &segs_, &segmag_, &segneg_, &segbad_, &counts_, &offsets_,
                       &cursor_, &nch_, &coff_, &entries_, &partials_, &buckets_, &wu_, &wt_, &wins_, &segok_,
                       &scan_tmp_, &leaf_idx_, &leaf_m_, &leaf_x_, &leaf_s_, &leaf_out_, &in_m_, &in_x_, &in_s_,
-                      &in_out_, &in_rows_, &gate_, &segpt_, &dig_a_, &dig_b_})
+                      &in_out_, &in_rows_, &gate_, &segpt_, &dig_a_, &dig_b_, &lmags_, &lmags_hi_, &tsave_,
+                      &loc_idx_, &found_})
         b->release();
 }
 
-int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok) {
-    NvtxRange range("RLC round");
+int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok,
+                           bool locate) {
+    NvtxRange range(locate ? "RLC locate round" : "RLC round");
     if (const int rc = be_->fault_point("RLC round")) return rc;
     const uint32_t n_seg = (uint32_t)(seg.size() / 2);
-    const int W = (129 + c - 1) / c, B = 1 << (c - 1), S = sub_ranges(c);
+    uint32_t maxlen = 0;
+    for (uint32_t k = 0; k < n_seg; ++k) maxlen = std::max(maxlen, seg[2 * k + 1]);
+    // a locate round's magnitudes carry the factor j <= maxlen: 129 + bits(maxlen) bits
+    int mag_bits = 129;
+    if (locate)
+        for (uint32_t v = maxlen; v; v >>= 1) ++mag_bits;
+    const int W = (mag_bits + c - 1) / c, B = 1 << (c - 1), S = sub_ranges(c);
     std::vector<uint32_t> host(3 * (size_t)n_seg + 1);
     uint64_t total = 0;
     for (uint32_t k = 0; k < n_seg; ++k) {
@@ -622,8 +747,6 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     host[3 * (size_t)n_seg] = (uint32_t)total;
     const uint64_t K = (uint64_t)n_seg * W * B;
     if (K >= 0x7FFFFFFFull) return be_->set_error(kErrBadInput, "RLC round too large");
-    uint32_t maxlen = 0;
-    for (uint32_t k = 0; k < n_seg; ++k) maxlen = std::max(maxlen, seg[2 * k + 1]);
     const uint32_t chunk = be_->rlc_chunk(maxlen);
     const uint64_t chunk_cap = total / chunk + K + 1;
     size_t scan_bytes = 0;
@@ -643,6 +766,8 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
         (e = segpt_.ensure((uint64_t)n_seg * 112)) != cudaSuccess ||
         (e = scan_tmp_.ensure(std::max<size_t>(scan_bytes, 16))) != cudaSuccess)
         return be_->cuda_error(e, "RLC round buffers");
+    if (locate && ((e = lmags_.ensure(48ull * n_)) != cudaSuccess || (e = lmags_hi_.ensure(12ull * n_)) != cudaSuccess))
+        return be_->cuda_error(e, "RLC locate buffers");
     uint32_t* d_seg = (uint32_t*)segs_.p;
     const RoundGeo g{d_seg, d_seg + 2 * n_seg, n_seg, 3u * n_, c, W, B, S};
     uint32_t* counts = (uint32_t*)counts_.p;
@@ -650,21 +775,26 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     uint32_t* cursor = (uint32_t*)cursor_.p;
     uint32_t* nch = (uint32_t*)nch_.p;
     uint32_t* coff = (uint32_t*)coff_.p;
-    const uint4* mags = (const uint4*)mags_.p;
+    const uint4* mags = locate ? (const uint4*)lmags_.p : (const uint4*)mags_.p;
+    const uint32_t* mags_hi = locate ? (const uint32_t*)lmags_hi_.p : nullptr;
     // `host` is pageable: the copy is staged before cudaMemcpyAsync returns
     e = cudaMemcpyAsync(d_seg, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, (K + 1) * 4, s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC round set-up");
+    if (locate)
+        k_rlc_scale<<<n_seg, 256, 0, s>>>(d_seg, (const uint4*)mags_.p, (uint4*)lmags_.p, (uint32_t*)lmags_hi_.p);
     k_rlc_tsum<<<n_seg, 256, 0, s>>>(g, (const uint32_t*)tsc_.p, (const uint8_t*)okb_.p, (uint4*)segmag_.p,
-                                     (uint8_t*)segneg_.p, (uint32_t*)segbad_.p);
-    k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
-                                                     (uint32_t)total, counts, nullptr, nullptr, 0);
+                                     (uint8_t*)segneg_.p, (uint32_t*)segbad_.p, locate ? 1 : 0);
+    k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, mags_hi, (const uint4*)segmag_.p,
+                                                                 (const uint8_t*)segneg_.p, (uint32_t)total, counts,
+                                                                 nullptr, nullptr, 0);
     size_t tb = scan_tmp_.cap;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, counts, offsets, (int)(K + 1), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(cursor, offsets, K * 4, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC scan");
-    k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, (const uint4*)segmag_.p, (const uint8_t*)segneg_.p,
-                                                     (uint32_t)total, nullptr, cursor, (uint32_t*)entries_.p, 1);
+    k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, mags_hi, (const uint4*)segmag_.p,
+                                                                 (const uint8_t*)segneg_.p, (uint32_t)total, nullptr,
+                                                                 cursor, (uint32_t*)entries_.p, 1);
     k_rlc_nchunks<<<grid_for(K + 1, 256), 256, 0, s>>>(counts, (uint32_t)K, chunk, nch);
     tb = scan_tmp_.cap;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, nch, coff, (int)(K + 1), s);
@@ -695,6 +825,12 @@ int RlcVerifier::verify_leaves(const std::vector<uint32_t>& leaves, const uint8_
     std::vector<uint32_t> idx;
     for (size_t k = 0; k < leaves.size(); k += 2)
         for (uint32_t i = 0; i < leaves[k + 1]; ++i) idx.push_back(leaves[k] + i);
+    return verify_indices(idx, d_msgs, d_xs, d_sigs, d_out, s, stats, nullptr);
+}
+
+int RlcVerifier::verify_indices(const std::vector<uint32_t>& idx, const uint8_t* d_msgs, const uint8_t* d_xs,
+                                const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats,
+                                std::vector<uint8_t>* host_out) {
     const uint32_t m = (uint32_t)idx.size();
     if (m == 0) return kOk;
     cudaError_t e;
@@ -713,8 +849,62 @@ int RlcVerifier::verify_leaves(const std::vector<uint32_t>& leaves, const uint8_
     k_rlc_scatter<<<grid_for(m, 256), 256, 0, s>>>((const uint32_t*)leaf_idx_.p, m, (const uint8_t*)leaf_out_.p,
                                                   d_out);
     if ((e = cudaGetLastError()) != cudaSuccess) return be_->cuda_error(e, "RLC scatter");
+    if (host_out) {
+        host_out->resize(m);
+        if ((e = cudaMemcpyAsync(host_out->data(), leaf_out_.p, m, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+            return be_->cuda_error(e, "RLC leaf verdicts");
+    }
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return be_->cuda_error(e, "RLC leaves");
     if (stats) stats->leaf_items += m;
+    return kOk;
+}
+
+int RlcVerifier::locate(const std::vector<uint32_t>& round_idx, const std::vector<uint32_t>& loc,
+                        const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_t* d_sigs, uint8_t* d_out,
+                        cudaStream_t s, RlcStats* stats, std::vector<uint8_t>& resolved) {
+    NvtxRange range("RLC locate");
+    const uint32_t n_loc = (uint32_t)(loc.size() / 2);
+    resolved.assign(n_loc, 0);
+    if (n_loc == 0) return kOk;
+    cudaError_t e;
+    if ((e = tsave_.ensure(112ull * n_loc)) != cudaSuccess || (e = loc_idx_.ensure(4ull * n_loc)) != cudaSuccess ||
+        (e = found_.ensure(4ull * n_loc)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC locate buffers");
+    // the check round's sums T of these segments, before the locate round overwrites them
+    e = cudaMemcpyAsync(loc_idx_.p, round_idx.data(), 4ull * n_loc, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC locate indices");
+    k_rlc_gather_pts<<<grid_for(n_loc, 128), 128, 0, s>>>((const uint32_t*)loc_idx_.p, n_loc,
+                                                          (const uint4*)segpt_.p, (uint4*)tsave_.p);
+    if ((e = cudaGetLastError()) != cudaSuccess) return be_->cuda_error(e, "RLC locate gather");
+    uint32_t maxlen = 0;
+    for (uint32_t k = 0; k < n_loc; ++k) maxlen = std::max(maxlen, loc[2 * k + 1]);
+    std::vector<uint8_t> ok;
+    int rc = run_round(loc, be_->rlc_window(maxlen), s, ok, true);
+    if (rc != kOk) return rc;
+    if (stats) {
+        stats->rounds++;
+        stats->segments += n_loc;
+    }
+    k_rlc_locate<<<n_loc, 256, 0, s>>>((const uint4*)tsave_.p, (const uint4*)segpt_.p, (const uint32_t*)segs_.p,
+                                       (uint32_t*)found_.p);
+    std::vector<uint32_t> found(n_loc);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(found.data(), found_.p, 4ull * n_loc, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC locate");
+    // the candidates are verified one by one; only an invalid candidate resolves its segment
+    std::vector<uint32_t> cand, owner;
+    for (uint32_t q = 0; q < n_loc; ++q)
+        if (found[q] >= 1 && found[q] <= loc[2 * q + 1]) {
+            cand.push_back(loc[2 * q] + found[q] - 1);
+            owner.push_back(q);
+        }
+    std::vector<uint8_t> verdicts;
+    rc = verify_indices(cand, d_msgs, d_xs, d_sigs, d_out, s, stats, &verdicts);
+    if (rc != kOk) return rc;
+    for (size_t k = 0; k < cand.size(); ++k)
+        if (verdicts[k] == 0) resolved[owner[k]] = 1;
+    if (stats) stats->located += (uint64_t)std::count(resolved.begin(), resolved.end(), (uint8_t)1);
     return kOk;
 }
 
@@ -739,7 +929,7 @@ int RlcVerifier::verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_
     k_rlc_prep<<<grid_for(n, 128), 128, 0, s>>>(d_msgs, d_xs, d_sigs, n, sd, (RlcItem*)items_.p, (uint4*)mags_.p,
                                                 (uint32_t*)tsc_.p, (uint8_t*)okb_.p, d_out);
     if ((e = cudaGetLastError()) != cudaSuccess) return be_->cuda_error(e, "RLC prep");
-    std::vector<uint32_t> seg, next, leaves;
+    std::vector<uint32_t> seg, next, leaves, loc, loc_round;
     for (uint32_t b = 0; b < n; b += batch_size) {
         seg.push_back(b);
         seg.push_back(std::min(batch_size, n - b));
@@ -763,14 +953,9 @@ int RlcVerifier::verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_
         // dense failures (most segments of a bisection level fail): stop splitting
         const bool dense = round > 0 && n_fail >= 8 && 4 * n_fail > 3 * ok_host_.size();
         next.clear();
-        for (size_t k = 0; k < ok_host_.size(); ++k) {
-            if (ok_host_[k] & 1) continue;
-            const uint32_t st = seg[2 * k], len = seg[2 * k + 1];
-            if (dense || len <= kLeaf) {
-                leaves.push_back(st);
-                leaves.push_back(len);
-                continue;
-            }
+        loc.clear();
+        loc_round.clear();
+        auto split = [&](uint32_t st, uint32_t len) {
             // kFanout near-equal children
             const uint32_t parts = std::min<uint32_t>(kFanout, len);
             for (uint32_t q = 0; q < parts; ++q) {
@@ -778,6 +963,29 @@ int RlcVerifier::verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_
                 next.push_back(st + a);
                 next.push_back(b - a);
             }
+        };
+        for (size_t k = 0; k < ok_host_.size(); ++k) {
+            if (ok_host_[k] & 1) continue;
+            const uint32_t st = seg[2 * k], len = seg[2 * k + 1];
+            if (dense || len <= kLeaf) {
+                leaves.push_back(st);
+                leaves.push_back(len);
+            } else if (be_->rlc_locate() && len <= kLocateMax) {
+                loc.push_back(st);
+                loc.push_back(len);
+                loc_round.push_back((uint32_t)k);
+            } else {
+                split(st, len);
+            }
+        }
+        if (!loc.empty()) {
+            // one more MSM over these segments finds a single invalid item; the
+            // others (two or more invalid items) are bisected
+            std::vector<uint8_t> resolved;
+            const int lrc = locate(loc_round, loc, d_msgs, d_xs, d_sigs, d_out, s, stats, resolved);
+            if (lrc != kOk) return lrc;
+            for (size_t q = 0; q < resolved.size(); ++q)
+                if (!resolved[q]) split(loc[2 * q], loc[2 * q + 1]);
         }
         seg.swap(next);
         ++round;

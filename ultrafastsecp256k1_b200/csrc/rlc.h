@@ -41,8 +41,9 @@ namespace uf {
 struct RlcStats {
     uint64_t rounds = 0;          // MSM rounds (the first check and each bisection level)
     uint64_t segments = 0;        // segments checked by MSM, all rounds
-    uint64_t leaf_items = 0;      // items verified one by one after bisection
+    uint64_t leaf_items = 0;      // items verified one by one (bisection leaves and locate candidates)
     int window_bits = 0;          // window of the first round
+    uint64_t located = 0;         // failing segments resolved by a locate round
 };
 
 class RlcVerifier {
@@ -50,6 +51,7 @@ public:
     static constexpr uint32_t kLeaf = 32;      // segments this small are verified per signature
     static constexpr uint32_t kChunk = 16;     // default bucket points summed by one thread
     static constexpr uint32_t kFanout = 8;     // children of a failing segment
+    static constexpr uint32_t kLocateMax = 65535;   // longest segment a locate round searches
     static constexpr uint32_t kMaxItems = 1u << 24;
 
     explicit RlcVerifier(Backend* be) : be_(be) {}
@@ -102,9 +104,23 @@ public:
 private:
     // One MSM check of every segment (start, length pairs); ok[k] bit 0 = the
     // equation holds, bit 1 = the segment holds an item that failed to parse.
-    int run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok);
+    // locate: the round of the locate step (magnitudes and the G scalar
+    // weighted by j = i - start + 1 within each segment).
+    int run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok,
+                  bool locate = false);
     int verify_leaves(const std::vector<uint32_t>& leaves, const uint8_t* d_msgs, const uint8_t* d_xs,
                       const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats);
+    // Plain verify of the listed items; verdicts into d_out (and host_out).
+    int verify_indices(const std::vector<uint32_t>& idx, const uint8_t* d_msgs, const uint8_t* d_xs,
+                       const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats,
+                       std::vector<uint8_t>* host_out);
+    // The locate step for the failing segments `loc` (start, length pairs;
+    // round_idx: their positions in the check round just run, whose sums are
+    // in segpt_): resolved[q] = 1 when segment q's single invalid item was
+    // found and verified invalid (its verdict written, the rest stay valid).
+    int locate(const std::vector<uint32_t>& round_idx, const std::vector<uint32_t>& loc, const uint8_t* d_msgs,
+               const uint8_t* d_xs, const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats,
+               std::vector<uint8_t>& resolved);
 
     Backend* be_;
     uint32_t n_ = 0;
@@ -119,6 +135,7 @@ private:
     DevBuf in_m_, in_x_, in_s_, in_out_, in_rows_, gate_;
     DevBuf segpt_;       // each segment's final sum (Jacobian, 112 B)
     DevBuf dig_a_, dig_b_;   // input digest tree levels
+    DevBuf lmags_, lmags_hi_, tsave_, loc_idx_, found_;   // locate step
     std::vector<uint8_t> ok_host_;
 };
 

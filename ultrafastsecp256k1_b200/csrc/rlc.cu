@@ -334,13 +334,22 @@ k_rlc_chunks(const uint32_t* __restrict__ coff, uint32_t K, uint32_t chunk, cons
 }
 
 // Buckets with 0 or >= 2 chunks: infinity, or the sum of their partials.
+// A bucket of more than kHeavyChunks chunks (skewed digits: the top windows
+// of a locate round's j-scaled magnitudes put most points of a segment into a
+// few buckets) is left to k_rlc_bucket_heavy: its key goes to `heavy`.
+constexpr uint32_t kHeavyChunks = 48;
+
 __global__ void __launch_bounds__(128)
 k_rlc_bucket_fin(const uint32_t* __restrict__ coff, uint32_t K, const uint4* __restrict__ partials,
-                 uint4* __restrict__ buckets) {
+                 uint4* __restrict__ buckets, uint32_t* __restrict__ heavy) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
     const uint32_t c0 = coff[k], c1 = coff[k + 1];
     if (c1 - c0 == 1) return;
+    if (c1 - c0 > kHeavyChunks) {
+        heavy[1 + atomicAdd(&heavy[0], 1u)] = k;
+        return;
+    }
     Jac acc, p;
     jac_set_inf(acc);
     for (uint32_t c = c0; c < c1; ++c) {
@@ -348,6 +357,43 @@ k_rlc_bucket_fin(const uint32_t* __restrict__ coff, uint32_t K, const uint4* __r
         jac_add(acc, p);
     }
     store_jac(buckets + kJacQ * (uint64_t)k, acc);
+}
+
+// Jacobian point from lane `src` of the warp (every lane calls it).
+__device__ __forceinline__ Jac shfl_jac(const Jac& a, int src) {
+    Jac b;
+    for (int k = 0; k < 8; ++k) {
+        b.X.v[k] = __shfl_sync(0xFFFFFFFFu, a.X.v[k], src);
+        b.Y.v[k] = __shfl_sync(0xFFFFFFFFu, a.Y.v[k], src);
+        b.Z.v[k] = __shfl_sync(0xFFFFFFFFu, a.Z.v[k], src);
+    }
+    b.inf = __shfl_sync(0xFFFFFFFFu, a.inf ? 1 : 0, src) != 0;
+    return b;
+}
+
+// One warp per heavy bucket (heavy[0] of them, keys in heavy[1..]): lane l
+// sums partials l, l + 32, ..., then the 32 lane sums meet in a shuffle tree:
+// about chunks / 32 + 5 serial additions instead of chunks.
+__global__ void __launch_bounds__(128)
+k_rlc_bucket_heavy(const uint32_t* __restrict__ coff, const uint4* __restrict__ partials,
+                   uint4* __restrict__ buckets, const uint32_t* __restrict__ heavy) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < heavy[0]; w += warps) {
+        const uint32_t k = heavy[1 + w];
+        const uint32_t c0 = coff[k], c1 = coff[k + 1];
+        Jac acc, p;
+        jac_set_inf(acc);
+        for (uint32_t c = c0 + lane; c < c1; c += 32) {
+            load_jac(partials + kJacQ * (uint64_t)c, p);
+            jac_add(acc, p);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const Jac other = shfl_jac(acc, (int)(lane ^ (uint32_t)o));
+            jac_add(acc, other);
+        }
+        if (lane == 0) store_jac(buckets + kJacQ * (uint64_t)k, acc);
+    }
 }
 
 // One thread per (segment, window, sub-range j of m buckets):
@@ -719,7 +765,7 @@ RlcVerifier::~RlcVerifier() {
                       &cursor_, &nch_, &coff_, &entries_, &partials_, &buckets_, &wu_, &wt_, &wins_, &segok_,
                       &scan_tmp_, &leaf_idx_, &leaf_m_, &leaf_x_, &leaf_s_, &leaf_out_, &in_m_, &in_x_, &in_s_,
                       &in_out_, &in_rows_, &gate_, &segpt_, &dig_a_, &dig_b_, &lmags_, &lmags_hi_, &tsave_,
-                      &loc_idx_, &found_})
+                      &loc_idx_, &found_, &heavy_})
         b->release();
 }
 
@@ -764,6 +810,8 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
         (e = wt_.ensure((uint64_t)n_seg * W * S * 112)) != cudaSuccess ||
         (e = wins_.ensure((uint64_t)n_seg * W * 112)) != cudaSuccess || (e = segok_.ensure(n_seg)) != cudaSuccess ||
         (e = segpt_.ensure((uint64_t)n_seg * 112)) != cudaSuccess ||
+        // a heavy bucket holds more than kHeavyChunks of the at most chunk_cap chunks
+        (e = heavy_.ensure((chunk_cap / (kHeavyChunks + 1) + 2) * 4)) != cudaSuccess ||
         (e = scan_tmp_.ensure(std::max<size_t>(scan_bytes, 16))) != cudaSuccess)
         return be_->cuda_error(e, "RLC round buffers");
     if (locate && ((e = lmags_.ensure(48ull * n_)) != cudaSuccess || (e = lmags_hi_.ensure(12ull * n_)) != cudaSuccess))
@@ -780,6 +828,7 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     // `host` is pageable: the copy is staged before cudaMemcpyAsync returns
     e = cudaMemcpyAsync(d_seg, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, (K + 1) * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(heavy_.p, 0, 4, s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC round set-up");
     if (locate)
         k_rlc_scale<<<n_seg, 256, 0, s>>>(d_seg, (const uint4*)mags_.p, (uint4*)lmags_.p, (uint32_t*)lmags_hi_.p);
@@ -804,7 +853,9 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
                                                           (const uint4*)be_->gtab(), (uint4*)partials_.p,
                                                           (uint4*)buckets_.p);
     k_rlc_bucket_fin<<<grid_for(K, 128), 128, 0, s>>>(coff, (uint32_t)K, (const uint4*)partials_.p,
-                                                      (uint4*)buckets_.p);
+                                                      (uint4*)buckets_.p, (uint32_t*)heavy_.p);
+    k_rlc_bucket_heavy<<<be_->sms() * 4, 128, 0, s>>>(coff, (const uint4*)partials_.p, (uint4*)buckets_.p,
+                                                      (const uint32_t*)heavy_.p);
     k_rlc_wpart<<<grid_for((uint64_t)n_seg * W * S, 128), 128, 0, s>>>(g, (const uint4*)buckets_.p, (uint4*)wu_.p,
                                                                        (uint4*)wt_.p);
     k_rlc_wcomb<<<grid_for((uint64_t)n_seg * W, 128), 128, 0, s>>>(g, (const uint4*)wu_.p, (const uint4*)wt_.p,

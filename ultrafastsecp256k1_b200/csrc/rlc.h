@@ -136,6 +136,7 @@ private:
     DevBuf segpt_;       // each segment's final sum (Jacobian, 112 B)
     DevBuf dig_a_, dig_b_;   // input digest tree levels
     DevBuf lmags_, lmags_hi_, tsave_, loc_idx_, found_;   // locate step
+    DevBuf heavy_;       // count and keys of the buckets with many chunks (k_rlc_bucket_heavy)
     std::vector<uint8_t> ok_host_;
 };
 

@@ -308,15 +308,19 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_device_props(ufsecp_gpu_ctx* ctx, int* 
                                                       int* schnorr_blocks_per_sm);
 
 /* Verify-kernel variant per signature kind (0 ECDSA, 1 BIP-340).  The
- * variants compute the same verdicts; they differ in how much of the field /
- * point arithmetic is inlined (instruction-cache footprint vs. call overhead).
+ * variants compute the same verdicts; 0..8 differ in how much of the field /
+ * point arithmetic is inlined (instruction-cache footprint vs. call overhead),
+ * 9..11 in window widths with variant 4's code: 9 = 3-bit P windows (a 4-entry
+ * table) with 18-bit G windows, 10 = 5-bit P windows (16 entries), 11 = 16-bit
+ * G windows (the default is 4-bit P and 20-bit G windows); the generator
+ * tables of another G width (16 / 4 MB) are made when such a variant is chosen.
  * ultrafastsecp256k1_b200.autotune measures them and writes the tuning file
  * read at context creation (UFSECP_B200_TUNING).  The tuning may also name a
  * small-launch variant per kind, used by verify calls of at most `items`
  * items (latency-bound launches with a few warps per SM, where inlining the
  * field arithmetic wins; the chunks of a larger call keep the main variant); set_variant applies its variant to every launch size and
  * clears the small-launch one.  get_small_variant reports -1 when none. */
-#define UFSECP_EXT_VERIFY_VARIANTS 9
+#define UFSECP_EXT_VERIFY_VARIANTS 12
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_set_variant(ufsecp_gpu_ctx* ctx, int kind, int variant);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_get_variant(ufsecp_gpu_ctx* ctx, int kind, int* variant_out,
                                                      int* blocks_per_sm_out);

@@ -408,9 +408,11 @@ def test_abi_gating_with_context(gpu_ctx):
     assert info.compute_units > 0 and info.global_mem_bytes > 0
 
 
-@pytest.mark.parametrize("variant", range(9))
+@pytest.mark.parametrize("variant", range(12))
 def test_every_kernel_variant_matches_oracle(gpu_ctx, oracle, variant):
-    """The code-size variants (ufsecp_gpu_ext_set_variant) compute identical verdicts."""
+    """The code-size variants (0..8) and the window-width variants (9: 3-bit P /
+    18-bit G windows, 10: 5-bit P, 11: 16-bit G) of ufsecp_gpu_ext_set_variant
+    compute identical verdicts."""
     _, wy, e = load_golden()
     m, p, s = ecdsa_corpus(oracle, 700, seed=60 + variant, tamper=0.2)
     mx, x, sx = schnorr_corpus(oracle, 700, seed=70 + variant, tamper=0.2)

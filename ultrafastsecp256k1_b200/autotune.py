@@ -3,9 +3,10 @@
     python -m ultrafastsecp256k1_b200.autotune [--batch N] [--out PATH]
 
 For each signature kind (ECDSA, BIP-340) it times every verify-kernel variant
-(ufsecp_gpu_ext_set_variant; the variants differ in how much field / point
+(ufsecp_gpu_ext_set_variant; variants 0..8 differ in how much field / point
 arithmetic is inlined, i.e. instruction-cache footprint against call
-overhead) on a GPU-signed batch, checks that all variants return identical
+overhead, 9..11 in the P / G window widths: 3 / 18, 5 / 20, 4 / 16 bits
+against the default 4 / 20) on a GPU-signed batch, checks that all variants return identical
 verdicts, and picks them, plus the inversion group (threads of a block that
 share each modular inversion: 1, 64 or 128), a small-launch variant and its
 item limit for latency-bound launches (a few warps per SM) and the call size
@@ -32,7 +33,10 @@ import numpy as np
 import ultrafastsecp256k1_b200 as uf
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
-VARIANTS = 9
+VARIANTS = 12
+# window widths of each variant (kVariantPWin / kVariantGWin in csrc/kernels.h)
+P_WINDOW = [4] * 9 + [3, 5, 4]
+G_WINDOW = [20] * 9 + [18, 20, 16]
 RLC_SIZES = (64, 512, 4096, 16384)
 
 
@@ -252,6 +256,9 @@ def autotune(batch: int = 1 << 18, out_path: str | None = None, write: bool = Tr
             for label in ("ecdsa", "schnorr"):
                 k = res["kinds"][label]
                 f.write(f"{label}_variant {k['best']}\n")
+                # the window widths of the chosen variant (informational: the variant number selects them)
+                f.write(f"{label}_p_window {P_WINDOW[k['best']]}\n")
+                f.write(f"{label}_g_window {G_WINDOW[k['best']]}\n")
                 f.write(f"{label}_inv_group {k['inversion_group']['best']}\n")
                 if k["small"]["variant"] is not None:
                     f.write(f"{label}_small_variant {k['small']['variant']}\n")

@@ -54,7 +54,14 @@ _VARIANT_FLAGS = [
 # the batched / served kernels are built once, with the code generation that
 # measured fastest for the per-signature kernel on B200 (variant 4)
 _BEST_FLAGS = ["-DUF_NOINLINE_POINT", "-DUF_NOINLINE_FIELD", "-DUF_PTX_MUL"]
-VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS, "kernels_probe.cu": _VARIANT_FLAGS,
+# window-width variants of the per-signature kernel (variant 4's code
+# generation): 3-bit P / 18-bit G windows, 5-bit P windows, 16-bit G windows
+_WINDOW_FLAGS = [
+    ("v9", ["-DUF_VARIANT=9", "-DUF_PWIN=3", "-DUF_GWIN=18"] + _BEST_FLAGS),
+    ("v10", ["-DUF_VARIANT=10", "-DUF_PWIN=5"] + _BEST_FLAGS),
+    ("v11", ["-DUF_VARIANT=11", "-DUF_GWIN=16"] + _BEST_FLAGS),
+]
+VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS + _WINDOW_FLAGS, "kernels_probe.cu": _VARIANT_FLAGS,
             "kernels_queue.cu": [("", _BEST_FLAGS)], "kernels_noalloc.cu": [("", _BEST_FLAGS)],
             "kernels_verify_grp.cu": [("", _BEST_FLAGS)],
             # small calls are latency-bound: the two-lane kernel takes variant 6's

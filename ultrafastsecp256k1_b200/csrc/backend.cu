@@ -31,12 +31,14 @@ constexpr size_t kDeviceChunk = size_t{1} << 17; // items per launch of a large 
 
 const verify_launcher kLaunchers[kVerifyVariants] = {launch_verify_v0, launch_verify_v1, launch_verify_v2,
                                                      launch_verify_v3, launch_verify_v4, launch_verify_v5,
-                                                     launch_verify_v6, launch_verify_v7, launch_verify_v8};
+                                                     launch_verify_v6, launch_verify_v7, launch_verify_v8,
+                                                     launch_verify_v9, launch_verify_v10, launch_verify_v11};
 const verify_occupancy_fn kOccupancy[kVerifyVariants] = {verify_occupancy_v0, verify_occupancy_v1,
                                                          verify_occupancy_v2, verify_occupancy_v3,
                                                          verify_occupancy_v4, verify_occupancy_v5,
                                                          verify_occupancy_v6, verify_occupancy_v7,
-                                                         verify_occupancy_v8};
+                                                         verify_occupancy_v8, verify_occupancy_v9,
+                                                         verify_occupancy_v10, verify_occupancy_v11};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -55,7 +57,27 @@ cudaError_t Backend::launch_verify(int kind, const uint8_t* m, const uint8_t* p,
         return launch_verify_grp(inv_group_[k], kind, m, p, s, n, d_gtab_, out, collect, grp_grid_[gi][k], st);
     }
     const int v = small ? small_variant_[k] : variant_[k];
-    return kLaunchers[v](kind, m, p, s, n, d_gtab_, out, collect, grid_[v][k], st);
+    return kLaunchers[v](kind, m, p, s, n, gtab_for(v), out, collect, grid_[v][k], st);
+}
+
+const void* Backend::gtab_for(int v) const {
+    const int w = kVariantGWin[v];
+    return w == UF_GWIN ? d_gtab_ : gtab_w_[w];
+}
+
+int Backend::ensure_variant_tables(int v) {
+    const int w = kVariantGWin[v];
+    if (w == UF_GWIN || gtab_w_[w]) return kOk;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, (size_t)64 << w);
+    if (e == cudaSuccess) e = launch_gtable_init_w(p, w, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) {
+        if (p) cudaFree(p);
+        return cuda_error(e, "generator tables of a window variant");
+    }
+    gtab_w_[w] = p;
+    return kOk;
 }
 
 int Backend::set_inversion_group(int kind, int group) {
@@ -68,6 +90,7 @@ int Backend::set_inversion_group(int kind, int group) {
 
 int Backend::set_variant(int kind, int v) {
     if (kind < 0 || kind > 1 || v < 0 || v >= kVerifyVariants) return set_error(kErrBadInput, "bad variant");
+    if (const int rc = ensure_variant_tables(v)) return rc;
     variant_[kind] = v;
     small_variant_[kind] = -1;   // an explicit choice applies to every launch size
     pair_items_[kind] = 0;
@@ -85,6 +108,8 @@ int Backend::set_lanes(int kind, int lanes, uint32_t items) {
 
 int Backend::set_small_variant(int kind, int v, uint32_t items) {
     if (kind < 0 || kind > 1 || v < -1 || v >= kVerifyVariants) return set_error(kErrBadInput, "bad variant");
+    if (v >= 0)
+        if (const int rc = ensure_variant_tables(v)) return rc;
     small_variant_[kind] = v;
     small_items_[kind] = v >= 0 ? items : 0;
     clear_error();
@@ -279,6 +304,8 @@ Backend::~Backend() {
             if (pstream_[j]) cudaStreamDestroy(pstream_[j]);
         }
         if (d_gtab_) cudaFree(d_gtab_);
+        for (void*& t : gtab_w_)
+            if (t) cudaFree(t);
         if (stream_) cudaStreamDestroy(stream_);
     }
 }
@@ -338,6 +365,12 @@ int Backend::init(int device_index) {
         for (int k = 0; k < 2; ++k) grp_grid_[gi][k] = std::max(1, verify_grp_occupancy(gi ? 128 : 64, k)) * sms_;
     queue_pair_grid_ = std::max(1, verify_pair_occupancy()) * sms_;   // also the two-lane kernels' shared-memory opt-in
     load_tuning();
+    // generator tables of the window widths the chosen variants use; a variant
+    // whose tables cannot be made falls back to variant 4
+    for (int k = 0; k < 2; ++k) {
+        if (ensure_variant_tables(variant_[k]) != kOk) variant_[k] = 4;
+        if (small_variant_[k] >= 0 && ensure_variant_tables(small_variant_[k]) != kOk) small_variant_[k] = -1;
+    }
     (void)cudaGetLastError();
     ready_ = true;
     clear_error();

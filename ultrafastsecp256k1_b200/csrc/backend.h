@@ -164,7 +164,10 @@ private:
     int dev_ = -1;
     int sms_ = 0;
     std::string dev_name_;
-    int grid_[9][2] = {};        // [variant][kind] resident-grid size
+    int grid_[12][2] = {};       // [variant][kind] resident-grid size
+    void* gtab_w_[32] = {};      // generator tables of other window widths (window variants), by bits
+    const void* gtab_for(int v) const;
+    int ensure_variant_tables(int v);
     int variant_[2] = {4, 4};    // chosen variant per kind (4: out-of-line field / point ops, PTX chains)
     // Verify calls of at most small_items_[kind] items (latency-bound: a few
     // warps per SM) use small_variant_[kind] instead, when the tuning names

@@ -24,15 +24,20 @@
 
 namespace uf {
 
-constexpr int kWP = 4;     // P window bits
-constexpr int kNWP = 33;   // P windows
+// P window bits: 4 by default; the window-width variants of the verify kernel
+// are compiled with 3 or 5 (UF_PWIN), and with other G windows (UF_GWIN).
+#ifndef UF_PWIN
+#define UF_PWIN 4
+#endif
+constexpr int kWP = UF_PWIN;                  // P window bits
+constexpr int kNWP = (129 + kWP - 1) / kWP;   // P windows: 33 for 4 bits (132 >= 129)
 constexpr int kWG = UF_GWIN;                  // G window bits (a multiple of kWP)
 constexpr int kNWG = (129 + kWG - 1) / kWG;   // G windows: 7 for 20 bits (one per five P windows)
 constexpr int kGEvery = kWG / kWP;            // P windows per G window
 static_assert(kWG % kWP == 0 && kNWG * kGEvery >= kNWP, "G windows must align with P windows");
 static_assert(kWG <= 30, "G Booth digits (up to 2^(kWG-1)) are stored as int32_t");
 typedef int32_t GDigit;   // a G-stream Booth digit, |d| <= 2^(kWG-1)
-constexpr int kPTab = 8;   // 1P..8P
+constexpr int kPTab = 1 << (kWP - 1);   // 1P..8P for 4-bit windows
 constexpr int kGTab = 1 << (kWG - 1); // 1G..2^19 G for 20-bit windows (and the same for lambda G)
 
 // Signed fixed-window (Booth) digits of a magnitude k < 2^129:

@@ -8,11 +8,12 @@
 namespace uf {
 
 // ---------------------------------------------------------------- G tables --
-// entry t < kGTab: (t+1)*G ; t >= kGTab: (t-kGTab+1)*lambda*G = (beta x, y)
-__global__ void k_gtable_init(uint4* out) {
+// entry t < half: (t+1)*G ; t >= half: (t-half+1)*lambda*G = (beta x, y),
+// half = 2^(w-1) for w-bit windows
+__global__ void k_gtable_init(uint4* out, int half) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * kGTab) return;
-    const int m = (t & (kGTab - 1)) + 1;
+    if (t >= 2 * half) return;
+    const int m = (t & (half - 1)) + 1;
     Aff G;
     gen_point(G);
     Jac acc;
@@ -23,7 +24,7 @@ __global__ void k_gtable_init(uint4* out) {
     }
     Aff A;
     jac_to_aff(A, acc);
-    if (t >= kGTab) {
+    if (t >= half) {
         Fe beta;
         fe_beta(beta);
         fe_mul(A.x, A.x, beta);
@@ -36,10 +37,13 @@ __global__ void k_gtable_init(uint4* out) {
     q[3] = make_uint4(A.y.v[4], A.y.v[5], A.y.v[6], A.y.v[7]);
 }
 
-cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s) {
-    k_gtable_init<<<(2 * kGTab + 255) / 256, 256, 0, s>>>(reinterpret_cast<uint4*>(d_gtab));
+cudaError_t launch_gtable_init_w(void* d_gtab, int wbits, cudaStream_t s) {
+    const int half = 1 << (wbits - 1);
+    k_gtable_init<<<(2 * half + 255) / 256, 256, 0, s>>>(reinterpret_cast<uint4*>(d_gtab), half);
     return cudaGetLastError();
 }
+
+cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s) { return launch_gtable_init_w(d_gtab, UF_GWIN, s); }
 
 // ---------------------------------------------------------- diagnostics --
 // op: 1 fe_mul(64->32) 2 fe_sqr(32->32) 3 fe_inv(32->32) 4 fe_sqrt(32->33)

@@ -20,6 +20,8 @@ constexpr int kVerifyThreads = 128;
 constexpr size_t kVerifySmemPerThread = 8 * 64;
 
 cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s);
+// The same tables for wbits-bit windows (2^(wbits-1) multiples each, 2^wbits * 64 bytes).
+cudaError_t launch_gtable_init_w(void* d_gtab, int wbits, cudaStream_t s);
 
 // One signature per thread, grid-stride.  kind 0 = ECDSA (pubs: 33-byte SEC1
 // compressed), 1 = BIP-340 (pubs: 32-byte x-only).  msgs 32 B, sigs 64 B, all
@@ -27,7 +29,12 @@ cudaError_t launch_gtable_init(void* d_gtab, cudaStream_t s);
 // for a valid signature, 0 otherwise.  With collect != 0 a valid signature
 // writes 0 and an invalid one leaves out[i] untouched.  Variants 0..5 are the
 // same kernel built with different code-size choices (kernels_verify.cu).
-constexpr int kVerifyVariants = 9;
+constexpr int kVerifyVariants = 12;
+// G-window bits of each variant's generator tables (9: 3-bit P / 18-bit G
+// windows, 10: 5-bit P, 11: 16-bit G; the others 4 / UF_GWIN).
+constexpr int kVariantGWin[kVerifyVariants] = {UF_GWIN, UF_GWIN, UF_GWIN, UF_GWIN, UF_GWIN, UF_GWIN,
+                                               UF_GWIN, UF_GWIN, UF_GWIN, 18, UF_GWIN, 16};
+constexpr int kVariantPWin[kVerifyVariants] = {4, 4, 4, 4, 4, 4, 4, 4, 4, 3, 5, 4};
 typedef cudaError_t (*verify_launcher)(int kind, const uint8_t* msgs, const uint8_t* pubs, const uint8_t* sigs,
                                        uint32_t n, const void* d_gtab, uint8_t* out, int collect, int grid,
                                        cudaStream_t s);
@@ -59,6 +66,15 @@ int verify_occupancy_v5(int kind);
 int verify_occupancy_v6(int kind);
 int verify_occupancy_v7(int kind);
 int verify_occupancy_v8(int kind);
+cudaError_t launch_verify_v9(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                             int, int, cudaStream_t);
+cudaError_t launch_verify_v10(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                              int, int, cudaStream_t);
+cudaError_t launch_verify_v11(int, const uint8_t*, const uint8_t*, const uint8_t*, uint32_t, const void*, uint8_t*,
+                              int, int, cudaStream_t);
+int verify_occupancy_v9(int kind);
+int verify_occupancy_v10(int kind);
+int verify_occupancy_v11(int kind);
 
 // The same verify with block-wide batch inversion (kernels_verify_grp.cu):
 // the table, final-Z and ECDSA s inversions are shared by the `group` (64 or

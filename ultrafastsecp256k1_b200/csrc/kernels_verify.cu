@@ -11,9 +11,11 @@
 //   * Booth digits live in a small per-thread local array indexed uniformly
 //     across the warp (coalesced, L1 resident).
 //
-// This file is compiled several times (UF_VARIANT 0..3) with different
-// code-size choices (UF_NOINLINE_POINT / UF_NOINLINE_FIELD, see common.cuh);
-// the backend picks a variant per signature kind (tuned per device).
+// This file is compiled several times (UF_VARIANT 0..11) with different
+// code-size choices (UF_NOINLINE_POINT / UF_NOINLINE_FIELD, see common.cuh)
+// and, for variants 9..11, other window widths (UF_PWIN P-window bits, 3 / 5;
+// UF_GWIN G-window bits, 18 / 16, over generator tables of that width); the
+// backend picks a variant per signature kind (tuned per device).
 #include "kernels.h"
 #include "verify.cuh"
 #include "dev_tables.cuh"
@@ -36,10 +38,10 @@
 // UF_TAB7: 1P kept in registers, 448 bytes of shared memory per thread.
 #ifdef UF_TAB7
 #define UF_TAB_T SmemTab7
-#define UF_SMEM_PER_THREAD 448
+#define UF_SMEM_PER_THREAD ((size_t)(kPTab - 1) * 64)
 #else
 #define UF_TAB_T const SmemTab
-#define UF_SMEM_PER_THREAD kVerifySmemPerThread
+#define UF_SMEM_PER_THREAD ((size_t)kPTab * 64)   // 2^(UF_PWIN-1) table points of 64 bytes
 #endif
 #define UF_CAT2(a, b) a##b
 #define UF_CAT(a, b) UF_CAT2(a, b)

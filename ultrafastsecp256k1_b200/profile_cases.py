@@ -1,7 +1,7 @@
 """Small, self-checking GPU cases to run under a profiler.
 
     python -m ultrafastsecp256k1_b200.profile_cases verify [--n N] [--reps R]
-    python -m ultrafastsecp256k1_b200.profile_cases rlc    [--n N] [--batch B] [--reps R]
+    python -m ultrafastsecp256k1_b200.profile_cases rlc    [--n N] [--batch B] [--reps R] [--one-per-batch]
     python -m ultrafastsecp256k1_b200.profile_cases queue  [--n N] [--reps R]
 
 Each case signs its own seeded BIP-340 / ECDSA corpus on the GPU, runs the
@@ -30,7 +30,7 @@ def _keys(rng, n):
     return sks
 
 
-def _signed(ctx, torch, kind, n, seed, n_bad):
+def _signed(ctx, torch, kind, n, seed, n_bad, bad_idx=None):
     rng = np.random.default_rng(seed)
     msgs = rng.integers(0, 256, (n, 32), dtype=np.uint8)
     aux = rng.integers(0, 256, (n, 32), dtype=np.uint8)
@@ -47,7 +47,7 @@ def _signed(ctx, torch, kind, n, seed, n_bad):
     assert bool(d_ok.all())
     sigs = d_s.cpu().numpy().reshape(n, 64)
     expect = np.ones(n, np.uint8)
-    bad = rng.choice(n, size=n_bad, replace=False)
+    bad = np.asarray(bad_idx) if bad_idx is not None else rng.choice(n, size=n_bad, replace=False)
     for i in bad:
         sigs[i, 40] ^= 0x04
     expect[bad] = 0
@@ -70,8 +70,15 @@ def case_verify(ctx, torch, a):
 
 
 def case_rlc(ctx, torch, a):
-    n_bad = (a.n // a.batch) // a.bad_every if a.bad_every else 0
-    d_m, d_x, d_s, expect, _ = _signed(ctx, torch, 1, a.n, 2, n_bad)
+    if a.one_per_batch:
+        # exactly one invalid signature in every batch, at a seeded position
+        rng = np.random.default_rng(65)
+        bad_idx = [b + int(rng.integers(0, min(a.batch, a.n - b))) for b in range(0, a.n, a.batch)]
+        n_bad = len(bad_idx)
+    else:
+        bad_idx = None
+        n_bad = (a.n // a.batch) // a.bad_every if a.bad_every else 0
+    d_m, d_x, d_s, expect, _ = _signed(ctx, torch, 1, a.n, 2, n_bad, bad_idx)
     d_o = torch.zeros(a.n, dtype=torch.uint8, device="cuda")
     st = torch.cuda.Stream()
     torch.cuda.synchronize()
@@ -121,6 +128,7 @@ def main():
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--bad-every", type=int, default=8, help="rlc: one invalid signature per this many batches (0: none)")
+    ap.add_argument("--one-per-batch", action="store_true", help="rlc: exactly one invalid signature in every batch")
     a = ap.parse_args()
     import torch
     with uf.GpuContext(0) as ctx:

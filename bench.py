@@ -739,13 +739,14 @@ def _pct(v, q):
     return v[min(len(v) - 1, int(q * (len(v) - 1) + 0.5))] if v else None
 
 
-def run_served(uf, reqs, budget=8 << 30, slots=8):
-    """Submit at the arrival times from one thread, wait from another; the
-    verdicts are compared after the run, so the waiter holds the GIL only
-    around its wait calls."""
+def run_served(uf, reqs, budget=8 << 30, slots=8, key_cache_log2=18, closed=False):
+    """Submit at the arrival times from one thread (closed: all at once), wait
+    from another; the verdicts are compared after the run, so the waiter holds
+    the GIL only around its wait calls."""
     import threading
     sctx = uf.GpuContext(0)
-    srv = uf.Server(sctx, slots=slots, max_launch_items=1 << 16, memory_budget_bytes=budget)
+    srv = uf.Server(sctx, slots=slots, max_launch_items=1 << 16, memory_budget_bytes=budget,
+                    key_cache_log2=key_cache_log2)
     # warm the graph buckets
     for t, jobs, exp in reqs[:8]:
         srv.wait(srv.submit(jobs))
@@ -769,7 +770,7 @@ def run_served(uf, reqs, budget=8 << 30, slots=8):
         t0 = time.perf_counter()
         lag = 0.0
         for k, (t, jobs, exp) in enumerate(reqs):
-            while time.perf_counter() - t0 < t:
+            while not closed and time.perf_counter() - t0 < t:
                 pass
             lag = max(lag, time.perf_counter() - t0 - t)
             ids[k] = srv.submit(jobs)
@@ -788,6 +789,7 @@ def run_served(uf, reqs, budget=8 << 30, slots=8):
             "requests": int(st["requests_done"]), "launches": int(st["launches"]),
             "peak_slots_in_flight": int(st["peak_slots_in_flight"]),
             "peak_budget_mb": st["peak_budget_bytes"] / 2**20, "max_submit_lag_ms": lag * 1e3,
+            "key_table_hits": (st["cache_hits"] / st["cache_lookups"]) if st["cache_lookups"] else None,
             "verdict_agreement": agree[0] / items}
 
 
@@ -834,13 +836,20 @@ def bench_serving(ctx, torch):
     reqs = serving_requests(pools, 1_000_000, 2.0, seed=4096, fixed_size=4096)
     fixed = {"offered_sigs_per_s": 1_000_000, "request_size": 4096, "requests": len(reqs),
              "served": run_served(uf, reqs)}
+    # closed loop: the 10 M sigs/s request set submitted all at once, with and
+    # without the resident key table (each run on a fresh server: the table
+    # starts empty)
+    reqs = serving_requests(pools, 10_000_000, 1.0, seed=10_000_000)
+    closed = {"requests": len(reqs),
+              "key_table_on": run_served(uf, reqs, closed=True, key_cache_log2=18),
+              "key_table_off": run_served(uf, reqs, closed=True, key_cache_log2=0)}
     return {"workload": "Poisson arrivals, request sizes log-uniform [1, 4096], 70/30 BIP-340/ECDSA items, "
                         "Zipf(1.1) keys from a 100k pool, 0.5% invalid, 8 GiB admission budget",
             "served": "ufsecp_gpu_ext_server_* (8 slots, continuous batching); latency submit -> verdicts, "
                       "measured by the server; Python's collector off while requests arrive (both forms)",
             "plain": "one synchronous ufsecp_gpu_{ecdsa,schnorr}_verify_batch call per request and kind, FIFO; "
                      "latency arrival -> verdicts (wall clock)",
-            "rates": rows, "fixed_4096": fixed}
+            "rates": rows, "fixed_4096": fixed, "closed_loop": closed}
 
 
 def ecdsa_plain_rate(ctx, torch, n=1 << 20, reps=3):

@@ -131,3 +131,32 @@ def test_msm_error_codes(gpu_ctx, oracle):
     two_p = np.ascontiguousarray(np.concatenate([pts[:1], pts[:1]]))
     rc = L.ufsecp_gpu_msm(gpu_ctx.handle, two_k.ctypes.data, two_p.ctypes.data, 2, out.ctypes.data)
     assert rc == uf.UFSECP_ERR_ARITH == 7 and (out == 0).all()
+
+
+@pytest.mark.parametrize("affine", [1, 0])
+def test_msm_repeated_and_opposite_points(oracle, monkeypatch, affine):
+    """Equal points with equal scalars land in the same bucket of every window,
+    so the bucket sums meet P + P (doubling) and P + (-P) (infinity) inside one
+    chunk and across chunks; with and without the batch-affine chunk sums."""
+    from conftest import msm_corpus
+    monkeypatch.setenv("UFSECP_B200_RLC_AFFINE", str(affine))
+    L = uf.load_library()
+    L.ufsecp_gpu_msm.argtypes = [_vp, _vp, _vp, _sz, _vp]
+    ks, pts = msm_corpus(oracle, 8, seed=81)
+    neg = pts.copy()
+    neg[:, 0] ^= 1                                  # 02 <-> 03: the opposite point
+    cases = [
+        (np.repeat(ks[:1], 40, 0), np.repeat(pts[:1], 40, 0)),
+        (np.concatenate([np.repeat(ks[:1], 40, 0), ks[3:4]]),
+         np.concatenate([np.repeat(pts[:1], 20, 0), np.repeat(neg[:1], 20, 0), pts[3:4]])),
+        (np.concatenate([np.repeat(ks[:2], 33, 0), np.repeat(ks[:1], 17, 0), ks[4:8]]),
+         np.concatenate([np.repeat(pts[:2], 33, 0), np.repeat(neg[:1], 17, 0), pts[4:8]])),
+        (np.repeat(ks[:1], 300, 0), np.concatenate([np.repeat(pts[:1], 150, 0), np.repeat(neg[:1], 150, 0)])),
+    ]
+    with uf.GpuContext(0) as ctx:
+        for k, p in cases:
+            k, p = np.ascontiguousarray(k), np.ascontiguousarray(p)
+            out = np.full(33, 7, np.uint8)
+            rc = L.ufsecp_gpu_msm(ctx.handle, k.ctypes.data, p.ctypes.data, len(k), out.ctypes.data)
+            st, want = oracle.msm(k, p)
+            assert (rc, out.tobytes()) == (st, want)

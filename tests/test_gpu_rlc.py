@@ -189,7 +189,7 @@ def test_rlc_repeated_items(gpu_ctx, oracle):
     assert (out == want).all()
 
 
-@pytest.mark.parametrize("chunk", [2, 3, 7, 16, 256])
+@pytest.mark.parametrize("chunk", [2, 3, 7, 12, 16, 256])
 def test_rlc_chunk_sizes(gpu_ctx, oracle, chunk):
     """Any bucket chunk (one point per thread up to whole buckets) gives the same verdicts."""
     m, x, s = schnorr_corpus(oracle, 60, seed=82, tamper=0.0)
@@ -208,6 +208,25 @@ def test_rlc_chunk_sizes(gpu_ctx, oracle, chunk):
     finally:
         gpu_ctx.set_rlc_chunk(0)
     assert gpu_ctx.get_rlc_chunk(4096) == tuned
+
+
+@pytest.mark.parametrize("affine", [1, 0])
+def test_rlc_affine_and_jacobian_chunk_sums(oracle, monkeypatch, affine):
+    """Chunks summed in affine coordinates with block-shared inversions (up to
+    16 points) or by mixed Jacobian additions give the same verdicts, repeated
+    items (equal points in one bucket) included."""
+    monkeypatch.setenv("UFSECP_B200_RLC_AFFINE", str(affine))
+    m, x, s = schnorr_corpus(oracle, 80, seed=83, tamper=0.0)
+    _flip(m, 7)
+    idx = np.array([i % 80 for i in range(3000)] + [5] * 300 + [9] * 97)
+    m, x, s = m[idx].copy(), x[idx].copy(), s[idx].copy()
+    want = oracle.schnorr_verify_batch(m, x, s)
+    with uf.GpuContext(0) as ctx:
+        for chunk in (4, 8, 13, 16):
+            ctx.set_rlc_chunk(chunk)
+            for bs in (0, 512):
+                out, _ = ctx.schnorr_verify_rlc(m, x, s, batch_size=bs, seed32=SEED)
+                assert (out == want).all(), (chunk, bs)
 
 
 def test_rlc_chunk_bounds(gpu_ctx):

@@ -174,6 +174,7 @@ void Backend::load_tuning() {
                 if (!strcmp(key, "key_table_log2") && (val == 0 || (val >= 8 && val <= 24)))
                     key_log2_ = (uint32_t)val;
                 if (!strcmp(key, "rlc_locate") && (val == 0 || val == 1)) rlc_locate_ = val != 0;
+                if (!strcmp(key, "rlc_affine") && (val == 0 || val == 1)) rlc_affine_ = val != 0;
                 if (!strcmp(key, "ecdsa_inv_group") && (val == 1 || val == 64 || val == 128)) inv_group_[0] = val;
                 if (!strcmp(key, "schnorr_inv_group") && (val == 1 || val == 64 || val == 128)) inv_group_[1] = val;
             }
@@ -190,6 +191,8 @@ void Backend::load_tuning() {
     if (pt >= 1 && pt <= 16) pack_threads_ = pt;
     const int lo_env = env_int("UFSECP_B200_RLC_LOCATE", -1);
     if (lo_env == 0 || lo_env == 1) rlc_locate_ = lo_env != 0;
+    const int af_env = env_int("UFSECP_B200_RLC_AFFINE", -1);
+    if (af_env == 0 || af_env == 1) rlc_affine_ = af_env != 0;
     const int rc_env = env_int("UFSECP_B200_RLC_CHUNK", 0);
     if (rc_env >= 2 && rc_env <= 256) rlc_chunk_fixed_ = (uint32_t)rc_env;
     const int ve = env_int("UFSECP_B200_VARIANT_ECDSA", -1), vs = env_int("UFSECP_B200_VARIANT_SCHNORR", -1);
@@ -211,9 +214,11 @@ void Backend::load_tuning() {
 
 cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap) return cudaSuccess;
-    release();
-    size_t want = std::max(bytes, cap * 2);
+    // grow by at least half the current size, so that slowly rising requests
+    // do not reallocate on every call
+    size_t want = std::max(bytes, cap + cap / 2);
     want = (want + 255) & ~size_t{255};
+    release();
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;

@@ -106,6 +106,12 @@ public:
     // the tuning file's rlc_locate or UFSECP_B200_RLC_LOCATE may turn it off.
     bool rlc_locate() const { return rlc_locate_; }
     void set_rlc_locate(bool on) { rlc_locate_ = on; }
+    // Whether RLC bucket chunks (of at most 16 points) are summed in affine
+    // coordinates with block-shared inversions (k_rlc_chunks_aff) instead of
+    // mixed Jacobian additions.  On by default; the tuning file's rlc_affine
+    // or UFSECP_B200_RLC_AFFINE may turn it off.
+    bool rlc_affine() const { return rlc_affine_; }
+    void set_rlc_affine(bool on) { rlc_affine_ = on; }
     int queue_grid() const { return queue_grid_; }
     int queue_pair_grid() const { return queue_pair_grid_; }
     // Mixed-job launches of at most this many items (both kinds together) run
@@ -216,6 +222,7 @@ private:
     std::map<uint32_t, uint32_t> rlc_chunk_;  // tuned bucket points per chunk thread per RLC batch size
     uint32_t rlc_chunk_fixed_ = 0;            // set_rlc_chunk / UFSECP_B200_RLC_CHUNK override, 0 = tuned
     bool rlc_locate_ = true;
+    bool rlc_affine_ = true;
     int last_err_ = kOk;
     std::string last_msg_ = "OK";
     std::atomic<long long> fault_after_{-1};

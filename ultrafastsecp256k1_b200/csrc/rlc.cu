@@ -18,6 +18,7 @@
 #include "dev_tables.cuh"
 #include "kernels.h"
 #include "sign.cuh"
+#include "grpinv.cuh"
 #include "verify.cuh"
 #include "nvtx.h"
 
@@ -333,12 +334,476 @@ k_rlc_chunks(const uint32_t* __restrict__ coff, uint32_t K, uint32_t chunk, cons
     else store_jac(partials + kJacQ * (uint64_t)t, acc);
 }
 
+// ------------------------------------------------- batch-affine chunk sums --
+// The same chunks summed in affine coordinates.  Each chunk is reduced by a
+// pairwise tree (level 1 adds entries 2p and 2p + 1, each later level the
+// results of the level before); an affine addition needs one inversion, and
+// every inversion of a level is shared by the whole grid (Montgomery's trick,
+// one safegcd per level and piece of chunks):
+//
+//   forward (k_aff_fwd): per thread, the denominators of its pairs multiplied
+//     up (suffix products kept in `suf`), the thread's product into `tp`;
+//   the threads' products are inverted together (k_binv_*: serial products of
+//     16 values per thread, a block-level product tree over 512 threads,
+//     repeated down to one inversion);
+//   backward (k_aff_bwd): from the thread's inverse, its pairs from the first
+//     up: 1 / den of pair q = inverse x suf[q + 1], the affine sum, written to
+//     the chunk's slot p.
+//
+// An affine addition with the shared inversion costs about 5 multiplies and
+// 1 squaring against 7 and 4 for a mixed Jacobian addition, the product tree
+// adds about 4 multiplies per thread and level, and the chunks' results
+// are affine, so the bucket merge uses mixed additions too.  Level l gives each
+// thread 2^(l-1) consecutive chunks, so a thread has up to C / 2 pairs at every
+// level.
+//
+// Addition cases of A + B (affine, each possibly infinity) and the
+// denominator each needs inverted (never zero: y = 0 has no point on this
+// curve).
+enum : int { kPairGen = 0, kPairDbl = 1, kPairInf = 2, kPairA = 3, kPairB = 4 };
+
+__device__ __forceinline__ int pair_den(const Fe& xa, const Fe& ya, bool ia, const Fe& xb, const Fe& yb, bool ib,
+                                        Fe& den) {
+    if (ia || ib) {
+        fe_set_u32(den, 1);
+        return ia ? kPairB : kPairA;
+    }
+    fe_sub(den, xb, xa);
+    if (!fe_is_zero(den)) return kPairGen;
+    Fe t;
+    fe_sub(t, yb, ya);
+    if (fe_is_zero(t)) {            // A == B: tangent slope 3 x^2 / 2 y
+        fe_add(den, ya, ya);
+        return kPairDbl;
+    }
+    fe_set_u32(den, 1);             // A == -B
+    return kPairInf;
+}
+
+// A <- A + B given inv = 1 / den of pair_den.
+__device__ __forceinline__ void pair_sum(int kase, Fe& xa, Fe& ya, bool& ia, const Fe& xb, const Fe& yb, bool ib,
+                                         const Fe& inv) {
+    if (kase == kPairA) return;
+    if (kase == kPairB) {
+        xa = xb;
+        ya = yb;
+        ia = ib;
+        return;
+    }
+    if (kase == kPairInf) {
+        ia = true;
+        return;
+    }
+    Fe lam, t, x3;
+    if (kase == kPairGen) {
+        fe_sub(t, yb, ya);
+    } else {
+        fe_sqr(t, xa);
+        fe_mul_small(t, t, 3u);
+    }
+    fe_mul(lam, t, inv);
+    fe_sqr(x3, lam);
+    fe_sub(x3, x3, xa);
+    fe_sub(x3, x3, xb);             // xb == xa when doubling
+    fe_sub(t, xa, x3);
+    fe_mul(t, lam, t);
+    fe_sub(ya, t, ya);
+    xa = x3;
+}
+
+__device__ __forceinline__ void ld_fe(const uint4* q, Fe& a) {
+    const uint4 u = q[0], v = q[1];
+    a.v[0] = u.x; a.v[1] = u.y; a.v[2] = u.z; a.v[3] = u.w;
+    a.v[4] = v.x; a.v[5] = v.y; a.v[6] = v.z; a.v[7] = v.w;
+}
+
+__device__ __forceinline__ void st_fe(uint4* q, const Fe& a) {
+    q[0] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
+    q[1] = make_uint4(a.v[4], a.v[5], a.v[6], a.v[7]);
+}
+
+// Warp-level exclusive prefix and suffix products of the lanes' values:
+// returns the product of the other 31 lanes' values; *all = the warp's product.
+__device__ __forceinline__ Fe warp_others(const Fe& x, Fe* all) {
+    const int lane = (int)(threadIdx.x & 31u);
+    Fe incl = x, suf = x;
+    UF_UNROLL
+    for (int d = 1; d < 32; d <<= 1) {
+        const Fe a = grp_shfl_up(incl, d);
+        if (lane >= d) fe_mul(incl, incl, a);
+        const Fe b = grp_shfl_down(suf, d);
+        if (lane + d < 32) fe_mul(suf, suf, b);
+    }
+    Fe ex = grp_shfl_up(incl, 1), sx = grp_shfl_down(suf, 1);
+    if (lane == 0) fe_set_u32(ex, 1);
+    if (lane == 31) fe_set_u32(sx, 1);
+    *all = grp_shfl(incl, 31);
+    Fe o;
+    fe_mul(o, ex, sx);
+    return o;
+}
+
+// ---- grid-wide batch inversion of n values (2 uint4 each) in place ----
+constexpr int kBinvQ = 16;                         // values per thread, serial
+constexpr int kBinvBlock = 512;                    // threads per block
+constexpr uint32_t kBinvTop = (uint32_t)kBinvQ * kBinvBlock;   // sizes up to this: one block
+
+// Serial prefix products of thread j's values [Q j, Q j + Q) into w; returns
+// their product (one past n: 1).
+__device__ __forceinline__ Fe binv_serial(const uint4* __restrict__ v, uint4* __restrict__ w, uint32_t n,
+                                          uint32_t j) {
+    const uint32_t i0 = j * kBinvQ;
+    Fe acc, x;
+    fe_set_u32(acc, 1);
+    for (int k = 0; k < kBinvQ; ++k) {
+        if (i0 + k >= n) break;
+        ld_fe(v + 2ull * (i0 + k), x);
+        if (k == 0) acc = x;
+        else fe_mul(acc, acc, x);
+        st_fe(w + 2ull * (i0 + k), acc);
+    }
+    return acc;
+}
+
+// Block-level product tree (every thread of the block calls it): returns the
+// product of the block's other threads' values; *all = the block's product.
+__device__ __forceinline__ Fe binv_block(const Fe& x, Fe* all, uint32_t (*wsh)[8]) {
+    const uint32_t lane = threadIdx.x & 31u, wi = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    Fe wall;
+    Fe oth = warp_others(x, &wall);
+    if (lane == 0)
+        for (int k = 0; k < 8; ++k) wsh[wi][k] = wall.v[k];
+    __syncthreads();
+    if (wi == 0) {
+        Fe wv, ball;
+        if (lane < nw) {
+            for (int k = 0; k < 8; ++k) wv.v[k] = wsh[lane][k];
+        } else {
+            fe_set_u32(wv, 1);
+        }
+        const Fe wo = warp_others(wv, &ball);       // product of the other warps' products
+        __syncwarp();
+        if (lane < nw)
+            for (int k = 0; k < 8; ++k) wsh[lane][k] = wo.v[k];
+        if (lane == 0)
+            for (int k = 0; k < 8; ++k) wsh[31][k] = ball.v[k];   // lane 31's slot is read back below
+        // (nw <= 16: slot 31 holds no warp's value)
+    }
+    __syncthreads();
+    Fe wo;
+    for (int k = 0; k < 8; ++k) {
+        wo.v[k] = wsh[wi][k];
+        all->v[k] = wsh[31][k];
+    }
+    __syncthreads();
+    fe_mul(oth, oth, wo);
+    return oth;
+}
+
+// Inverses of thread j's values, in place, from t = 1 / (their product).
+__device__ __forceinline__ void binv_unwind(uint4* __restrict__ v, const uint4* __restrict__ w, uint32_t n,
+                                            uint32_t j, Fe t) {
+    const uint32_t i0 = j * kBinvQ;
+    if (i0 >= n) return;
+    Fe x, r;
+    const int cnt = (int)min((uint32_t)kBinvQ, n - i0);
+    for (int k = cnt - 1; k >= 0; --k) {
+        ld_fe(v + 2ull * (i0 + k), x);
+        if (k > 0) {
+            ld_fe(w + 2ull * (i0 + k - 1), r);
+            fe_mul(r, t, r);
+        } else {
+            r = t;
+        }
+        fe_mul(t, t, x);
+        st_fe(v + 2ull * (i0 + k), r);
+    }
+}
+
+// Block b's product into u[b]; o[j] = product of the block's other values.
+__global__ void __launch_bounds__(kBinvBlock)
+k_binv_up(const uint4* __restrict__ v, uint4* __restrict__ w, uint4* __restrict__ o, uint4* __restrict__ u,
+          uint32_t n) {
+    __shared__ uint32_t wsh[32][8];
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    const Fe acc = binv_serial(v, w, n, j);
+    Fe all;
+    const Fe oth = binv_block(acc, &all, wsh);
+    st_fe(o + 2ull * j, oth);
+    if (threadIdx.x == 0) st_fe(u + 2ull * blockIdx.x, all);
+}
+
+// With uinv[b] = 1 / (block b's product): thread j's inverses.
+__global__ void __launch_bounds__(kBinvBlock)
+k_binv_down(uint4* __restrict__ v, const uint4* __restrict__ w, const uint4* __restrict__ o,
+            const uint4* __restrict__ uinv, uint32_t n) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j * kBinvQ >= n) return;
+    Fe t, x;
+    ld_fe(uinv + 2ull * blockIdx.x, t);
+    ld_fe(o + 2ull * j, x);
+    fe_mul(t, t, x);
+    binv_unwind(v, w, n, j, t);
+}
+
+// n <= kBinvTop values: one block; the block's product is inverted once (by
+// warp 0, every lane on the same value).
+__global__ void __launch_bounds__(kBinvBlock) k_binv_top(uint4* __restrict__ v, uint4* __restrict__ w, uint32_t n) {
+    __shared__ uint32_t wsh[32][8];
+    __shared__ uint32_t ish[8];
+    const uint32_t j = threadIdx.x;
+    const Fe acc = binv_serial(v, w, n, j);
+    Fe all;
+    Fe t = binv_block(acc, &all, wsh);
+    if (threadIdx.x < 32) {
+        Fe inv;
+        fe_inv(inv, all);
+        if (threadIdx.x == 0)
+            for (int k = 0; k < 8; ++k) ish[k] = inv.v[k];
+    }
+    __syncthreads();
+    Fe inv;
+    for (int k = 0; k < 8; ++k) inv.v[k] = ish[k];
+    fe_mul(t, t, inv);
+    binv_unwind(v, w, n, j, t);
+}
+
+// ---- the chunk trees ----
+struct AffArgs {
+    const uint32_t* coff;       // chunk offsets per bucket key (K + 1)
+    uint32_t K, chunk;
+    const uint32_t* offsets;    // entry offsets per bucket key
+    const uint32_t* entries;
+    const RlcItem* items;
+    uint32_t n3;
+    const uint4* gt;
+    uint32_t t0, tn;            // this piece: chunks t0 .. t0 + tn - 1 (those below coff[K] exist)
+    uint4* pts;                 // slot s of piece chunk c, quad q: pts[(4 s + q) tn + c]
+    uint32_t* ckey;             // per piece chunk: bucket key
+    uint32_t* ce0;              // first entry
+    uint8_t* cm0;               // entries (0: no chunk)
+    uint32_t* cinf;             // bit s: slot s holds infinity
+    uint4* suf;                 // per thread of a level: up to C / 2 suffix products, [q][thread]
+    uint4* tp;                  // per thread of a level: product of its denominators (inverted in place
+                                // between the passes)
+    uint4* partials;
+    uint4* buckets;
+};
+
+// x (and with `full` y) of entry e.
+__device__ __forceinline__ void aff_entry(const AffArgs& a, uint32_t e, Fe& x, Fe& y, bool full) {
+    const uint32_t v = a.entries[e];
+    const uint32_t pidx = v & 0x7FFFFFFFu;
+    const uint4* q;
+    if (pidx < a.n3) {
+        q = a.items[pidx / 3u].pt[pidx % 3u];
+    } else {
+        q = a.gt + 4 * (((pidx - a.n3) & 1u) ? kGTab : 0);
+    }
+    ld_fe(q, x);
+    if (full) {
+        ld_fe(q + 2, y);
+        if (v >> 31) fe_neg(y, y);
+    }
+}
+
+__device__ __forceinline__ void aff_slot_get(const AffArgs& a, uint32_t c, int s, Fe& x, Fe& y, bool full) {
+    const uint4* q = a.pts + (size_t)(4 * s) * a.tn + c;
+    const uint4 q0 = q[0], q1 = q[a.tn];
+    x.v[0] = q0.x; x.v[1] = q0.y; x.v[2] = q0.z; x.v[3] = q0.w;
+    x.v[4] = q1.x; x.v[5] = q1.y; x.v[6] = q1.z; x.v[7] = q1.w;
+    if (full) {
+        const uint4 q2 = q[2 * (size_t)a.tn], q3 = q[3 * (size_t)a.tn];
+        y.v[0] = q2.x; y.v[1] = q2.y; y.v[2] = q2.z; y.v[3] = q2.w;
+        y.v[4] = q3.x; y.v[5] = q3.y; y.v[6] = q3.z; y.v[7] = q3.w;
+    }
+}
+
+__device__ __forceinline__ void aff_slot_put(const AffArgs& a, uint32_t c, int s, const Fe& x, const Fe& y) {
+    uint4* q = a.pts + (size_t)(4 * s) * a.tn + c;
+    q[0] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    q[a.tn] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+    q[2 * (size_t)a.tn] = make_uint4(y.v[0], y.v[1], y.v[2], y.v[3]);
+    q[3 * (size_t)a.tn] = make_uint4(y.v[4], y.v[5], y.v[6], y.v[7]);
+}
+
+// Pair p of piece chunk c at `level` (1: entries e0 + 2p, + 1; else slots 2p,
+// 2p + 1).  With `full` the two points are loaded whole; without, only the x
+// coordinates, and the y coordinates only when the x coordinates are equal
+// (the forward pass needs just the denominator).
+__device__ __forceinline__ int aff_pair(const AffArgs& a, int level, uint32_t c, uint32_t e0, uint32_t inf, int p,
+                                        bool full, Fe& xa, Fe& ya, bool& ia, Fe& xb, Fe& yb, bool& ib, Fe& den) {
+    if (level == 1) {
+        ia = ib = false;
+    } else {
+        ia = (inf >> (2 * p)) & 1u;
+        ib = (inf >> (2 * p + 1)) & 1u;
+    }
+    if (level == 1) {
+        aff_entry(a, e0 + 2 * p, xa, ya, full);
+        aff_entry(a, e0 + 2 * p + 1, xb, yb, full);
+    } else {
+        aff_slot_get(a, c, 2 * p, xa, ya, full);
+        aff_slot_get(a, c, 2 * p + 1, xb, yb, full);
+    }
+    if (!full && !ia && !ib) {
+        fe_sub(den, xb, xa);
+        if (!fe_is_zero(den)) return kPairGen;
+        if (level == 1) {
+            aff_entry(a, e0 + 2 * p, xa, ya, true);
+            aff_entry(a, e0 + 2 * p + 1, xb, yb, true);
+        } else {
+            aff_slot_get(a, c, 2 * p, xa, ya, true);
+            aff_slot_get(a, c, 2 * p + 1, xb, yb, true);
+        }
+    }
+    return pair_den(xa, ya, ia, xb, yb, ib, den);
+}
+
+// Points of a chunk of m0 entries at `level`: ceil(m0 / 2^(level-1)).
+__device__ __forceinline__ uint32_t aff_count(uint32_t m0, int level) {
+    return (m0 + (1u << (level - 1)) - 1u) >> (level - 1);
+}
+
+// One thread per bucket key: the key, first entry and entry count of each of
+// its chunks that falls in the piece.
+__global__ void __launch_bounds__(256) k_aff_keys(AffArgs a) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.K) return;
+    const uint32_t c0 = max(a.coff[k], a.t0), c1 = min(a.coff[k + 1], a.t0 + a.tn);
+    const uint32_t o0 = a.offsets[k], o1 = a.offsets[k + 1];
+    for (uint32_t t = c0; t < c1; ++t) {
+        const uint32_t e0 = o0 + (t - a.coff[k]) * a.chunk;
+        a.ckey[t - a.t0] = k;
+        a.ce0[t - a.t0] = e0;
+        a.cm0[t - a.t0] = (uint8_t)(min(e0 + a.chunk, o1) - e0);
+    }
+}
+
+// Forward pass of `level` (128 threads per block; thread u of `threads` has
+// the piece chunks u, u + threads, ..., fewer than 2^(level-1) of them, so
+// that neighbouring threads touch neighbouring chunks).
+__global__ void __launch_bounds__(128)
+k_aff_fwd(AffArgs a, int level, uint32_t threads) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t span = 1u << (level - 1);
+    Fe acc;
+    fe_set_u32(acc, 1);
+    if (u < threads) {
+        uint32_t np_all = 0;
+        for (uint32_t k = 0; k < span; ++k) {
+            const uint32_t c = u + k * threads;
+            if (c >= a.tn) break;
+            np_all += aff_count(a.cm0[c], level) / 2u;
+        }
+        uint32_t q = np_all;
+        for (uint32_t k = span; k-- > 0;) {
+            const uint32_t c = u + k * threads;
+            if (c >= a.tn) continue;
+            const uint32_t m0 = a.cm0[c];
+            if (m0 < 2) continue;
+            const int np = (int)(aff_count(m0, level) / 2u);
+            const uint32_t e0 = level == 1 ? a.ce0[c] : 0u;
+            const uint32_t inf = level == 1 ? 0u : a.cinf[c];
+            for (int p = np - 1; p >= 0; --p) {
+                Fe xa, ya, xb, yb, den;
+                bool ia, ib;
+                aff_pair(a, level, c, e0, inf, p, false, xa, ya, ia, xb, yb, ib, den);
+                if (q == np_all) acc = den;
+                else fe_mul(acc, acc, den);
+                --q;
+                st_fe(a.suf + 2 * ((size_t)q * threads + u), acc);
+            }
+        }
+    }
+    if (u < threads) st_fe(a.tp + 2ull * u, acc);
+}
+
+// Backward pass of `level`: the sums, the odd points moved, and after the last
+// level each chunk's point written to its bucket (a bucket of one chunk) or
+// to its partial, Jacobian with Z = 1.
+__global__ void __launch_bounds__(128)
+k_aff_bwd(AffArgs a, int level, uint32_t threads, int last) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= threads) return;
+    const uint32_t span = 1u << (level - 1);
+    Fe inv;
+    ld_fe(a.tp + 2ull * u, inv);
+    uint32_t np_all = 0;
+    for (uint32_t k = 0; k < span; ++k) {
+        const uint32_t c = u + k * threads;
+        if (c >= a.tn) break;
+        np_all += aff_count(a.cm0[c], level) / 2u;
+    }
+    uint32_t q = 0;
+    for (uint32_t k = 0; k < span; ++k) {
+        const uint32_t c = u + k * threads;
+        if (c >= a.tn) break;
+        const uint32_t m0 = a.cm0[c];
+        if (m0 == 0) continue;
+        const uint32_t m = aff_count(m0, level);
+        const int np = (int)(m / 2u);
+        const uint32_t e0 = level == 1 ? a.ce0[c] : 0u;
+        const uint32_t inf = level == 1 ? 0u : a.cinf[c];
+        uint32_t ninf = 0;
+        for (int p = 0; p < np; ++p) {
+            Fe xa, ya, xb, yb, den, ip;
+            bool ia, ib;
+            const int kase = aff_pair(a, level, c, e0, inf, p, true, xa, ya, ia, xb, yb, ib, den);
+            if (q + 1 < np_all) {
+                ld_fe(a.suf + 2 * ((size_t)(q + 1) * threads + u), ip);
+                fe_mul(ip, inv, ip);
+            } else {
+                ip = inv;
+            }
+            fe_mul(inv, inv, den);
+            ++q;
+            pair_sum(kase, xa, ya, ia, xb, yb, ib, ip);
+            aff_slot_put(a, c, p, xa, ya);
+            ninf |= (ia ? 1u : 0u) << p;
+        }
+        if (m & 1u) {
+            Fe x, y;
+            if (level == 1) {
+                aff_entry(a, e0 + m - 1, x, y, true);
+                aff_slot_put(a, c, np, x, y);
+            } else {
+                ninf |= ((inf >> (m - 1)) & 1u) << np;
+                if (np > 0) {
+                    aff_slot_get(a, c, (int)m - 1, x, y, true);
+                    aff_slot_put(a, c, np, x, y);
+                }
+            }
+        }
+        a.cinf[c] = ninf;
+        if (last) {
+            Jac r;
+            aff_slot_get(a, c, 0, r.X, r.Y, true);
+            fe_set_u32(r.Z, 1);
+            r.inf = (ninf & 1u) != 0;
+            const uint32_t key = a.ckey[c];
+            if (a.coff[key + 1] - a.coff[key] == 1) store_jac(a.buckets + kJacQ * (uint64_t)key, r);
+            else store_jac(a.partials + kJacQ * (uint64_t)(a.t0 + c), r);
+        }
+    }
+}
+
 // Buckets with 0 or >= 2 chunks: infinity, or the sum of their partials.
 // A bucket of more than kHeavyChunks chunks (skewed digits: the top windows
 // of a locate round's j-scaled magnitudes put most points of a segment into a
 // few buckets) is left to k_rlc_bucket_heavy: its key goes to `heavy`.
 constexpr uint32_t kHeavyChunks = 48;
 
+// Adds a chunk partial: affine (Z = 1, from k_rlc_chunks_aff) or Jacobian.
+template <bool kAff>
+__device__ __forceinline__ void add_partial(Jac& acc, const uint4* q) {
+    Jac p;
+    load_jac(q, p);
+    if (!kAff) jac_add(acc, p);
+    else if (!p.inf) jac_add_aff(acc, p.X, p.Y);
+}
+
+template <bool kAff>
 __global__ void __launch_bounds__(128)
 k_rlc_bucket_fin(const uint32_t* __restrict__ coff, uint32_t K, const uint4* __restrict__ partials,
                  uint4* __restrict__ buckets, uint32_t* __restrict__ heavy) {
@@ -350,12 +815,9 @@ k_rlc_bucket_fin(const uint32_t* __restrict__ coff, uint32_t K, const uint4* __r
         heavy[1 + atomicAdd(&heavy[0], 1u)] = k;
         return;
     }
-    Jac acc, p;
+    Jac acc;
     jac_set_inf(acc);
-    for (uint32_t c = c0; c < c1; ++c) {
-        load_jac(partials + kJacQ * (uint64_t)c, p);
-        jac_add(acc, p);
-    }
+    for (uint32_t c = c0; c < c1; ++c) add_partial<kAff>(acc, partials + kJacQ * (uint64_t)c);
     store_jac(buckets + kJacQ * (uint64_t)k, acc);
 }
 
@@ -374,6 +836,7 @@ __device__ __forceinline__ Jac shfl_jac(const Jac& a, int src) {
 // One warp per heavy bucket (heavy[0] of them, keys in heavy[1..]): lane l
 // sums partials l, l + 32, ..., then the 32 lane sums meet in a shuffle tree:
 // about chunks / 32 + 5 serial additions instead of chunks.
+template <bool kAff>
 __global__ void __launch_bounds__(128)
 k_rlc_bucket_heavy(const uint32_t* __restrict__ coff, const uint4* __restrict__ partials,
                    uint4* __restrict__ buckets, const uint32_t* __restrict__ heavy) {
@@ -382,12 +845,9 @@ k_rlc_bucket_heavy(const uint32_t* __restrict__ coff, const uint4* __restrict__ 
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < heavy[0]; w += warps) {
         const uint32_t k = heavy[1 + w];
         const uint32_t c0 = coff[k], c1 = coff[k + 1];
-        Jac acc, p;
+        Jac acc;
         jac_set_inf(acc);
-        for (uint32_t c = c0 + lane; c < c1; c += 32) {
-            load_jac(partials + kJacQ * (uint64_t)c, p);
-            jac_add(acc, p);
-        }
+        for (uint32_t c = c0 + lane; c < c1; c += 32) add_partial<kAff>(acc, partials + kJacQ * (uint64_t)c);
         for (int o = 16; o > 0; o >>= 1) {
             const Jac other = shfl_jac(acc, (int)(lane ^ (uint32_t)o));
             jac_add(acc, other);
@@ -742,6 +1202,7 @@ __global__ void k_msm_out(const uint4* __restrict__ pt, uint8_t* __restrict__ ou
 
 inline unsigned grid_for(uint64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+
 }  // namespace
 
 int rlc_window_bits(uint32_t len) {
@@ -765,7 +1226,7 @@ RlcVerifier::~RlcVerifier() {
                       &cursor_, &nch_, &coff_, &entries_, &partials_, &buckets_, &wu_, &wt_, &wins_, &segok_,
                       &scan_tmp_, &leaf_idx_, &leaf_m_, &leaf_x_, &leaf_s_, &leaf_out_, &in_m_, &in_x_, &in_s_,
                       &in_out_, &in_rows_, &gate_, &segpt_, &dig_a_, &dig_b_, &lmags_, &lmags_hi_, &tsave_,
-                      &loc_idx_, &found_, &heavy_})
+                      &loc_idx_, &found_, &heavy_, &aff_pts_, &aff_suf_, &aff_tp_, &aff_meta_, &binv_})
         b->release();
 }
 
@@ -848,14 +1309,28 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     tb = scan_tmp_.cap;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, nch, coff, (int)(K + 1), s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC chunk scan");
-    k_rlc_chunks<<<grid_for(chunk_cap, 128), 128, 0, s>>>(coff, (uint32_t)K, chunk, offsets, (const uint32_t*)entries_.p,
-                                                          (const RlcItem*)items_.p, 3u * n_,
-                                                          (const uint4*)be_->gtab(), (uint4*)partials_.p,
-                                                          (uint4*)buckets_.p);
-    k_rlc_bucket_fin<<<grid_for(K, 128), 128, 0, s>>>(coff, (uint32_t)K, (const uint4*)partials_.p,
-                                                      (uint4*)buckets_.p, (uint32_t*)heavy_.p);
-    k_rlc_bucket_heavy<<<be_->sms() * 4, 128, 0, s>>>(coff, (const uint4*)partials_.p, (uint4*)buckets_.p,
-                                                      (const uint32_t*)heavy_.p);
+    const bool aff = be_->rlc_affine() && chunk <= 16;
+    if (aff) {
+        // the exact chunk count sizes the trees' grids and pieces
+        uint32_t nch = 0;
+        e = cudaMemcpyAsync(&nch, coff + K, 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return be_->cuda_error(e, "RLC chunk count");
+        if (const int rc = affine_chunks(chunk, nch, chunk_cap, coff, (uint32_t)K, offsets, s)) return rc;
+        k_rlc_bucket_fin<true><<<grid_for(K, 128), 128, 0, s>>>(coff, (uint32_t)K, (const uint4*)partials_.p,
+                                                                (uint4*)buckets_.p, (uint32_t*)heavy_.p);
+        k_rlc_bucket_heavy<true><<<be_->sms() * 4, 128, 0, s>>>(coff, (const uint4*)partials_.p, (uint4*)buckets_.p,
+                                                                (const uint32_t*)heavy_.p);
+    } else {
+        k_rlc_chunks<<<grid_for(chunk_cap, 128), 128, 0, s>>>(coff, (uint32_t)K, chunk, offsets,
+                                                              (const uint32_t*)entries_.p, (const RlcItem*)items_.p,
+                                                              3u * n_, (const uint4*)be_->gtab(),
+                                                              (uint4*)partials_.p, (uint4*)buckets_.p);
+        k_rlc_bucket_fin<false><<<grid_for(K, 128), 128, 0, s>>>(coff, (uint32_t)K, (const uint4*)partials_.p,
+                                                                 (uint4*)buckets_.p, (uint32_t*)heavy_.p);
+        k_rlc_bucket_heavy<false><<<be_->sms() * 4, 128, 0, s>>>(coff, (const uint4*)partials_.p,
+                                                                 (uint4*)buckets_.p, (const uint32_t*)heavy_.p);
+    }
     k_rlc_wpart<<<grid_for((uint64_t)n_seg * W * S, 128), 128, 0, s>>>(g, (const uint4*)buckets_.p, (uint4*)wu_.p,
                                                                        (uint4*)wt_.p);
     k_rlc_wcomb<<<grid_for((uint64_t)n_seg * W, 128), 128, 0, s>>>(g, (const uint4*)wu_.p, (const uint4*)wt_.p,
@@ -867,6 +1342,92 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     if (e == cudaSuccess) e = cudaMemcpyAsync(ok.data(), segok_.p, n_seg, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC round");
+    return kOk;
+}
+
+// Grid-wide batch inversion of n values at v (2 uint4 each): levels of
+// k_binv_up (one value per block of 8 K values) down to kBinvTop values,
+// k_binv_top, then k_binv_down back up.  Scratch: for each level w (n values),
+// o (one per thread), u (one per block).
+static size_t binv_scratch_values(uint32_t n) {
+    size_t total = 0;
+    while (n > kBinvTop) {
+        const uint32_t grid = (uint32_t)(((n + kBinvQ - 1) / kBinvQ + kBinvBlock - 1) / kBinvBlock);
+        total += n + (size_t)grid * kBinvBlock + grid;
+        n = grid;
+    }
+    return total + n;
+}
+
+static cudaError_t binv_launch(uint4* v, uint32_t n, uint4* scratch, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    if (n <= kBinvTop) {
+        k_binv_top<<<1, kBinvBlock, 0, s>>>(v, scratch, n);
+        return cudaGetLastError();
+    }
+    const uint32_t grid = (uint32_t)(((n + kBinvQ - 1) / kBinvQ + kBinvBlock - 1) / kBinvBlock);
+    uint4* w = scratch;
+    uint4* o = w + 2ull * n;
+    uint4* u = o + 2ull * grid * kBinvBlock;
+    uint4* rest = u + 2ull * grid;
+    k_binv_up<<<grid, kBinvBlock, 0, s>>>(v, w, o, u, n);
+    cudaError_t e = binv_launch(u, grid, rest, s);
+    if (e != cudaSuccess) return e;
+    k_binv_down<<<grid, kBinvBlock, 0, s>>>(v, w, o, u, n);
+    return cudaGetLastError();
+}
+
+int RlcVerifier::affine_chunks(uint32_t chunk, uint64_t nch, uint64_t chunk_cap, const uint32_t* coff, uint32_t K,
+                               const uint32_t* offsets, cudaStream_t s) {
+    if (nch == 0) return kOk;
+    const int C = chunk <= 8 ? 8 : 16, c2 = C / 2;
+    int levels = 1;
+    while ((1u << levels) < chunk) ++levels;
+    // per chunk: c2 slots (64 B), c2 suffix products and one block-other product
+    // (32 B), key, first entry, infinity bits (4 B each), entries (1 B)
+    const uint64_t per_chunk = 64ull * c2 + 32ull * c2 + 32 + 13 + 80;
+    const uint64_t piece_max = std::max<uint64_t>(kAffPieceBytes / per_chunk, 1024);
+    const uint64_t piece = std::min<uint64_t>(nch, piece_max);
+    // buffers sized by the round's chunk bound (fixed by the segment lengths),
+    // not by this call's count, so that calls of one shape allocate once
+    const uint64_t cap = std::min<uint64_t>(chunk_cap, piece_max);
+    cudaError_t e;
+    if ((e = aff_pts_.ensure(cap * c2 * 64)) != cudaSuccess || (e = aff_suf_.ensure(cap * c2 * 32)) != cudaSuccess ||
+        (e = aff_tp_.ensure(cap * 32)) != cudaSuccess || (e = aff_meta_.ensure(cap * 13 + 64)) != cudaSuccess ||
+        (e = binv_.ensure(binv_scratch_values((uint32_t)cap) * 32 + 32)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC affine buffers");
+    AffArgs a;
+    a.coff = coff;
+    a.K = K;
+    a.chunk = chunk;
+    a.offsets = offsets;
+    a.entries = (const uint32_t*)entries_.p;
+    a.items = (const RlcItem*)items_.p;
+    a.n3 = 3u * n_;
+    a.gt = (const uint4*)be_->gtab();
+    a.pts = (uint4*)aff_pts_.p;
+    a.ckey = (uint32_t*)aff_meta_.p;
+    a.ce0 = a.ckey + piece;
+    a.cinf = a.ce0 + piece;
+    a.cm0 = (uint8_t*)(a.cinf + piece);
+    a.suf = (uint4*)aff_suf_.p;
+    a.tp = (uint4*)aff_tp_.p;
+    a.partials = (uint4*)partials_.p;
+    a.buckets = (uint4*)buckets_.p;
+    for (uint64_t t0 = 0; t0 < nch; t0 += piece) {
+        a.t0 = (uint32_t)t0;
+        a.tn = (uint32_t)std::min<uint64_t>(piece, nch - t0);
+        k_aff_keys<<<grid_for(K, 256), 256, 0, s>>>(a);
+        for (int level = 1; level <= levels; ++level) {
+            const uint32_t threads = (uint32_t)((a.tn + (1ull << (level - 1)) - 1) >> (level - 1));
+            const uint32_t blocks = (threads + 127) / 128;
+            k_aff_fwd<<<blocks, 128, 0, s>>>(a, level, threads);
+            if ((e = binv_launch(a.tp, threads, (uint4*)binv_.p, s)) != cudaSuccess) break;
+            k_aff_bwd<<<blocks, 128, 0, s>>>(a, level, threads, level == levels ? 1 : 0);
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) return be_->cuda_error(e, "RLC affine chunks");
+    }
     return kOk;
 }
 

@@ -53,6 +53,8 @@ public:
     static constexpr uint32_t kFanout = 8;     // children of a failing segment
     static constexpr uint32_t kLocateMax = 65535;   // longest segment a locate round searches
     static constexpr uint32_t kMaxItems = 1u << 24;
+    // device bytes the affine chunk trees use per piece of a round's chunks
+    static constexpr uint64_t kAffPieceBytes = 4ull << 30;
 
     explicit RlcVerifier(Backend* be) : be_(be) {}
 
@@ -108,6 +110,11 @@ private:
     // weighted by j = i - start + 1 within each segment).
     int run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok,
                   bool locate = false);
+    // The round's bucket chunks (at most 16 points each) summed by affine
+    // pairwise trees with grid-shared inversions (k_aff_fwd / k_aff_bwd):
+    // results into partials_ / buckets_ as affine points (Z = 1).
+    int affine_chunks(uint32_t chunk, uint64_t nch, uint64_t chunk_cap, const uint32_t* coff, uint32_t K,
+                      const uint32_t* offsets, cudaStream_t s);
     int verify_leaves(const std::vector<uint32_t>& leaves, const uint8_t* d_msgs, const uint8_t* d_xs,
                       const uint8_t* d_sigs, uint8_t* d_out, cudaStream_t s, RlcStats* stats);
     // Plain verify of the listed items; verdicts into d_out (and host_out).
@@ -137,6 +144,7 @@ private:
     DevBuf dig_a_, dig_b_;   // input digest tree levels
     DevBuf lmags_, lmags_hi_, tsave_, loc_idx_, found_;   // locate step
     DevBuf heavy_;       // count and keys of the buckets with many chunks (k_rlc_bucket_heavy)
+    DevBuf aff_pts_, aff_suf_, aff_tp_, aff_meta_, binv_;   // affine chunk trees
     std::vector<uint8_t> ok_host_;
 };
 

@@ -1,7 +1,7 @@
 """Small, self-checking GPU cases to run under a profiler.
 
     python -m ultrafastsecp256k1_b200.profile_cases verify [--n N] [--reps R]
-    python -m ultrafastsecp256k1_b200.profile_cases rlc    [--n N] [--batch B] [--reps R] [--one-per-batch]
+    python -m ultrafastsecp256k1_b200.profile_cases rlc    [--n N] [--batch B] [--reps R] [--warmup W] [--one-per-batch]
     python -m ultrafastsecp256k1_b200.profile_cases queue  [--n N] [--reps R]
 
 Each case signs its own seeded BIP-340 / ECDSA corpus on the GPU, runs the
@@ -81,6 +81,9 @@ def case_rlc(ctx, torch, a):
     d_m, d_x, d_s, expect, _ = _signed(ctx, torch, 1, a.n, 2, n_bad, bad_idx)
     d_o = torch.zeros(a.n, dtype=torch.uint8, device="cuda")
     st = torch.cuda.Stream()
+    for k in range(a.warmup):
+        ctx.schnorr_verify_rlc_device(d_m.data_ptr(), d_x.data_ptr(), d_s.data_ptr(), a.n, d_o.data_ptr(),
+                                      batch_size=a.batch, seed32=bytes([255 - k]) * 32, stream=st.cuda_stream)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for k in range(a.reps):
@@ -127,6 +130,7 @@ def main():
     ap.add_argument("--n", type=int, default=1 << 18)
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=0, help="rlc: untimed calls before the timed ones")
     ap.add_argument("--bad-every", type=int, default=8, help="rlc: one invalid signature per this many batches (0: none)")
     ap.add_argument("--one-per-batch", action="store_true", help="rlc: exactly one invalid signature in every batch")
     a = ap.parse_args()

@@ -446,13 +446,14 @@ def mixed_workload(ctx, torch, n_batches=2000, seed=3, pool=100_000):
                         d_ok.data_ptr(), 0)
         torch.cuda.ExternalStream(ctx.stream()).synchronize()
         sigs = d_s.cpu().numpy().reshape(n, 64)
+        clean = sigs.copy()
         expect = np.ones(n, np.uint8)
         bad = rng.choice(n, size=max(1, n // 200), replace=False)
         for i in bad:
             bit = int(rng.integers(0, 512))
             sigs[i, bit // 8] ^= 1 << (bit % 8)
         expect[bad] = 0
-        out[kind] = (sel, msgs[sel], d_p.cpu().numpy().reshape(n, ps), sigs, expect)
+        out[kind] = (sel, msgs[sel], d_p.cpu().numpy().reshape(n, ps), sigs, expect, clean)
     # split back into batches (each batch: its ECDSA items and its BIP-340 items)
     bounds = np.concatenate([[0], np.cumsum(sizes)])
     pos = {0: np.searchsorted(out[0][0], bounds), 1: np.searchsorted(out[1][0], bounds)}
@@ -462,7 +463,7 @@ def mixed_workload(ctx, torch, n_batches=2000, seed=3, pool=100_000):
         parts = []
         for kind in (0, 1):
             lo, hi = pos[kind][b], pos[kind][b + 1]
-            sel, m, p, s, ex = out[kind]
+            sel, m, p, s, ex, _ = out[kind]
             parts.append((kind, m[lo:hi], p[lo:hi], s[lo:hi], ex[lo:hi]))
             kinds_j.append(kind)
             starts_j.append(lo)
@@ -472,7 +473,9 @@ def mixed_workload(ctx, torch, n_batches=2000, seed=3, pool=100_000):
     corpora = {k: tuple(np.ascontiguousarray(a) for a in out[k][1:4]) for k in (0, 1)}
     expects = {k: out[k][4] for k in (0, 1)}
     ranges = (np.array(kinds_j), np.array(starts_j), np.array(counts_j))
-    return batches, total, corpora, expects, ranges
+    # the BIP-340 items before tampering (an all-valid variant of the same jobs)
+    clean1 = (corpora[1][0], corpora[1][1], np.ascontiguousarray(out[1][5]))
+    return batches, total, corpora, expects, ranges, clean1
 
 
 def bench_mixed(ctx, torch):
@@ -489,7 +492,7 @@ def bench_mixed(ctx, torch):
     once timed.  Verdicts: every form against the construction, and every item
     against the reference library on the host cores."""
     import time as _t
-    batches, total, corpora, expects, (kinds_j, starts_j, counts_j) = mixed_workload(ctx, torch)
+    batches, total, corpora, expects, (kinds_j, starts_j, counts_j), clean1 = mixed_workload(ctx, torch)
 
     def plain_pass():
         # the reference-style synchronous call per batch and kind; verdicts
@@ -559,6 +562,28 @@ def bench_mixed(ctx, torch):
     t_off, agree_n, _ = ranges_pass()
     ctx.set_key_table(18)
 
+    # BIP-340 jobs as kind 2 (one RLC batch over all of them, 16384-item
+    # segments), on these items (0.5 % invalid) and on the all-valid variant
+    kinds_r = np.where(kinds_j == 1, 2, kinds_j)
+    n_bip = len(corpora[1][0])
+
+    def jobs_pass(corp, kinds, exps):
+        t0 = _t.perf_counter()
+        got = ctx.verify_job_ranges(corp, kinds, starts_j, counts_j)
+        dt = _t.perf_counter() - t0
+        return dt, sum(int((got[k] == exps[k]).sum()) for k in corp)
+
+    ones = np.ones(n_bip, np.uint8)
+    rlc_rows = {}
+    for label, corp1, exp1 in (("tampered", corpora[1], expects[1]), ("all_valid_bip340", clean1, ones)):
+        for kind in (1, 2):
+            corp = {0: corpora[0], kind: corp1}
+            kinds = kinds_j if kind == 1 else kinds_r
+            exps = {0: expects[0], kind: exp1}
+            jobs_pass(corp, kinds, exps)
+            t, agree_x = jobs_pass(corp, kinds, exps)
+            rlc_rows[f"{label}_kind{kind}"] = {"sigs_per_s": total / t, "verdict_agreement": agree_x / total}
+
     # the plain kernel over the same items, device-resident, one launch per kind
     st = torch.cuda.Stream()
     dev = {k: [torch.from_numpy(a.reshape(-1)).cuda() for a in corpora[k]] for k in (0, 1)}
@@ -615,6 +640,11 @@ def bench_mixed(ctx, torch):
             "plain_kernel_sigs_per_s": plain_kernel_rate,
             "plain_kernel": "ufsecp_gpu_ext_{ecdsa,schnorr}_verify_device over all items of each kind, one call per "
                             "kind, inputs on the device, CUDA events",
+            "rlc_job_kind": {
+                "api": "ufsecp_gpu_ext_verify_jobs from index ranges, key table on: the BIP-340 jobs as kind 1 "
+                       "(work queue) or kind 2 (one RLC batch over all BIP-340 items, 16384-item segments); the "
+                       "ECDSA jobs kind 0 in both; on these items and with the BIP-340 items untampered",
+                **rlc_rows},
             "verdict_agreement": {"plain": agree / total, "batched": agree_b / total, "batched_one_call": agree_o / total,
                                   "ranges_cold": agree_c / total, "ranges_warm": agree_w / total,
                                   "ranges_off": agree_n / total, "plain_kernel": agree_k / total,

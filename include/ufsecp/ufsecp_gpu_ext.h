@@ -39,13 +39,22 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_device(ufsecp_gpu_ctx* c
  * by one persistent work-queue kernel (warps claim 32-item chunks from a
  * device queue head); layouts up to 65,536 items per kind replay a CUDA graph
  * captured per capacity bucket.  Synchronous, like the reference calls; the
- * verdicts equal those of the per-kind calls item for item.  Gating as the
- * reference ABI: NULL ctx -> NULL_ARG, no jobs -> OK, every out buffer is
- * cleared first, NULL buffers of a non-empty job -> NULL_ARG, kind > 1 or a
- * total above 2^26 -> BAD_INPUT. */
+ * verdicts equal those of the per-kind calls item for item.  Kind 2 is
+ * BIP-340 (the kind 1 layouts) checked by random linear combination: all
+ * kind 2 items of the call are verified by one RLC batch verify (the
+ * ufsecp_gpu_ext_schnorr_verify_rlc engine, locate step and bisection down to
+ * per-item verdicts, weights seeded by a digest of the items XOR fresh random
+ * bytes) in segments of `reserved` items (0 = 16384), after the kind 0 / 1
+ * jobs; for batches expected to be (nearly) all valid, where one MSM check
+ * per segment replaces the per-signature verifies.  Its verdicts equal the
+ * per-signature verify's.  Gating as the reference ABI: NULL ctx ->
+ * NULL_ARG, no jobs -> OK, every out buffer is cleared first, NULL buffers of
+ * a non-empty job -> NULL_ARG, kind > 2 or a total above 2^26 -> BAD_INPUT.
+ * ufsecp_gpu_ext_verify_jobs_noalloc and the serving loop take kinds 0 and 1
+ * only. */
 typedef struct {
-    uint32_t kind;                /* 0 = ECDSA, 1 = BIP-340 */
-    uint32_t reserved;            /* 0 */
+    uint32_t kind;                /* 0 = ECDSA, 1 = BIP-340, 2 = BIP-340 by RLC */
+    uint32_t reserved;            /* kind 2: RLC segment length (0 = 16384); else 0 */
     size_t count;
     const uint8_t* msg_hashes32;  /* count * 32 */
     const uint8_t* pubkeys;       /* count * 33 (ECDSA) or count * 32 (BIP-340) */

@@ -142,7 +142,7 @@ def test_jobs_gating(gpu_ctx):
     assert L.ufsecp_gpu_ext_verify_jobs(h, j, 1) == uf.UFSECP_ERR_NULL_ARG
     assert (out == 0).all()                      # cleared before the NULL check
     buf = np.zeros(64 * 4, np.uint8)
-    j = (uf.Job * 1)(uf.Job(2, 0, 4, buf.ctypes.data, buf.ctypes.data, buf.ctypes.data, out.ctypes.data))
+    j = (uf.Job * 1)(uf.Job(3, 0, 4, buf.ctypes.data, buf.ctypes.data, buf.ctypes.data, out.ctypes.data))
     assert L.ufsecp_gpu_ext_verify_jobs(h, j, 1) == uf.UFSECP_ERR_BAD_INPUT
 
 
@@ -170,3 +170,51 @@ def test_job_ranges_equal_job_lists(gpu_ctx, corpora):
         assert (got[k][~covered[k]] == 0).all()
     with pytest.raises(ValueError):
         gpu_ctx.verify_job_ranges({0: e}, [0], [5990], [20])
+
+
+def _flip_bit(c, idx):
+    m, x, s = (a.copy() for a in c)
+    for i in idx:
+        s[i, 40] ^= 0x04
+    return m, x, s
+
+
+@pytest.mark.parametrize("pattern", ["valid", "one_invalid", "dense"])
+def test_rlc_job_kind(gpu_ctx, oracle, corpora, pattern):
+    """Kind 2 jobs (BIP-340 checked by one RLC batch over all of the call's
+    kind 2 items, locate step and bisection down to per-item verdicts) mixed
+    with kind 0 / 1 jobs: every verdict equals the oracle's, for all-valid
+    items, one invalid item in a segment and dense invalid items, with the
+    default and with small segment lengths."""
+    (e, s, we, ws) = corpora
+    clean = schnorr_corpus(oracle, 5000, seed=83, tamper=0.0)
+    if pattern == "one_invalid":
+        clean = _flip_bit(clean, [1234])
+    elif pattern == "dense":
+        clean = _flip_bit(clean, range(7, 5000, 9))
+    want_rlc = oracle.schnorr_verify_batch(*clean)
+    for segment in (0, 256, 1000):
+        jobs = [(0,) + _slice(e, 0, 700), (2,) + _slice(clean, 0, 1500) + (segment,), (1,) + _slice(s, 0, 900),
+                (2,) + _slice(clean, 1500, 1501), (2,) + _slice(clean, 1501, 1501), (2,) + _slice(clean, 1501, 5000)]
+        got = gpu_ctx.verify_jobs(jobs)
+        assert (got[0] == we[:700]).all() and (got[2] == ws[:900]).all()
+        assert (np.concatenate([got[1], got[3], got[4], got[5]]) == want_rlc).all(), segment
+
+
+def test_rlc_job_kind_gating(gpu_ctx):
+    L = uf.load_library()
+    m = np.zeros((4, 32), np.uint8)
+    x = np.zeros((4, 32), np.uint8)
+    sg = np.zeros((4, 64), np.uint8)
+    out = np.full(4, 7, np.uint8)
+    tab = np.zeros(1, uf._JOB_DTYPE)
+    tab[0] = (3, 0, 4, m.ctypes.data, x.ctypes.data, sg.ctypes.data, out.ctypes.data)
+    P = ctypes.POINTER(uf.Job)
+    assert L.ufsecp_gpu_ext_verify_jobs(gpu_ctx.handle, tab.ctypes.data_as(P), 1) == uf.UFSECP_ERR_BAD_INPUT
+    assert not out.any()
+    tab[0]["kind"] = 2
+    out[:] = 7
+    assert L.ufsecp_gpu_ext_verify_jobs(gpu_ctx.handle, tab.ctypes.data_as(P), 1) == uf.UFSECP_OK
+    assert not out.any()                       # s = 0 fails the strict parse
+    assert L.ufsecp_gpu_ext_verify_jobs_noalloc(gpu_ctx.handle, tab.ctypes.data_as(P), 1, None) == \
+        uf.UFSECP_ERR_BAD_INPUT

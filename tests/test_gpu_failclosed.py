@@ -187,3 +187,24 @@ def test_server_cancellation_token(served):
         # a token that never fires changes nothing
         rid = srv.submit_cancellable([(1, m, x, s)], lambda: False)
         assert (srv.wait(rid, 30_000)[0] == want).all()
+
+
+@pytest.mark.parametrize("kind,code", KINDS)
+def test_rlc_jobs_fail_closed(gpu_ctx, valid_big, kind, code):
+    """Kind 2 jobs (BIP-340 by RLC) mixed with kind 1 jobs: a failure in the
+    queue part (while the RLC items are being staged) or in the first RLC
+    round leaves every verdict byte of the call cleared."""
+    m, x, s = valid_big
+    jobs = [(1, m[:100_000], x[:100_000], s[:100_000]), (2, m[100_000:200_000], x[100_000:200_000],
+                                                          s[100_000:200_000]), (2, m[200_000:], x[200_000:], s[200_000:])]
+    L = uf.load_library()
+    for after, only_rlc in ((0, False), (0, True)):
+        js = jobs[1:] if only_rlc else jobs
+        tab, keep, out_all, offs = uf._job_table(js)
+        out_all[:] = 7
+        _arm(gpu_ctx, after, kind)
+        rc = L.ufsecp_gpu_ext_verify_jobs(gpu_ctx.handle, tab.ctypes.data_as(ctypes.POINTER(uf.Job)), len(js))
+        assert rc == code
+        assert not out_all.any()
+    got = gpu_ctx.verify_jobs(jobs)
+    assert all(g.all() for g in got)

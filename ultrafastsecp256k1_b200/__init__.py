@@ -230,7 +230,9 @@ def _job_table(jobs):
     little more than the three buffer addresses."""
     keep, meta = [], []
     total = 0
-    for kind, m, p, s in jobs:
+    for job in jobs:
+        kind, m, p, s = job[:4]
+        segment = int(job[4]) if len(job) > 4 else 0      # kind 2: RLC segment length (0 = default)
         m, p, s = _flat_u8(m), _flat_u8(p), _flat_u8(s)
         n = m.size >> 5
         if p.size != (33 if kind == 0 else 32) * n:
@@ -238,7 +240,7 @@ def _job_table(jobs):
         if s.size != 64 * n:
             raise ValueError(f"sigs64: expected {64 * n} bytes, got {s.size}")
         keep.append((m, p, s))
-        meta.append((kind, 0, n, _addr(m) if n else 0, _addr(p) if n else 0, _addr(s) if n else 0, total))
+        meta.append((kind, segment, n, _addr(m) if n else 0, _addr(p) if n else 0, _addr(s) if n else 0, total))
         total += n
     out_all = np.zeros(max(1, total), np.uint8)
     tab = np.array(meta, _JOB_DTYPE) if meta else np.zeros(1, _JOB_DTYPE)
@@ -353,8 +355,10 @@ class GpuContext:
 
     # ---- ufsecp_gpu_ext.h -------------------------------------------------------
     def verify_jobs(self, jobs):
-        """ufsecp_gpu_ext_verify_jobs: jobs = [(kind, msgs, pubs, sigs), ...] with kind 0
-        ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys); returns one verdict array per job."""
+        """ufsecp_gpu_ext_verify_jobs: jobs = [(kind, msgs, pubs, sigs[, segment]), ...] with
+        kind 0 ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys) / 2 BIP-340 checked by RLC
+        (32-byte keys; `segment` = RLC segment length, 0 = default); returns one verdict
+        array per job."""
         tab, keep, out_all, offs = _job_table(jobs)
         self._check(self.L.ufsecp_gpu_ext_verify_jobs(self._ctx, tab.ctypes.data_as(ctypes.POINTER(Job)), len(jobs)),
                     "verify_jobs")

@@ -117,6 +117,8 @@ ufsecp_error_t guarded_call(F&& run) {
     }
 }
 
+void fresh_seed(uint8_t seed[32]);
+
 ufsecp_error_t unsupported(ufsecp_gpu_ctx* ctx, size_t count) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     if (count == 0) return UFSECP_OK;
@@ -495,16 +497,22 @@ ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_
         const ufsecp_gpu_ext_job_t& J = jobs[j];
         if (J.count == 0) continue;
         if (!J.msg_hashes32 || !J.pubkeys || !J.sigs64 || !J.out_results) return UFSECP_ERR_NULL_ARG;
-        if (J.kind > 1) return UFSECP_ERR_BAD_INPUT;
+        if (J.kind > 2) return UFSECP_ERR_BAD_INPUT;
     }
     if (total > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
     int rc;
     try {
         std::vector<uf::VerifyJob> v(n_jobs);
-        for (size_t j = 0; j < n_jobs; ++j)
+        uint32_t segment = 0;
+        for (size_t j = 0; j < n_jobs; ++j) {
             v[j] = uf::VerifyJob{(int)jobs[j].kind, jobs[j].count, jobs[j].msg_hashes32, jobs[j].pubkeys,
                                  jobs[j].sigs64, jobs[j].out_results};
-        rc = ctx->backend->verify_jobs(v.data(), n_jobs);
+            // the first kind 2 job that names a segment length sets it for the call
+            if (jobs[j].kind == 2 && jobs[j].count && !segment) segment = jobs[j].reserved;
+        }
+        uint8_t rand32[32];
+        fresh_seed(rand32);
+        rc = ctx->backend->verify_jobs(v.data(), n_jobs, segment, rand32);
     } catch (const std::bad_alloc&) {
         rc = UFSECP_ERR_GPU_MEMORY;
     } catch (...) {

@@ -571,8 +571,63 @@ int Backend::key_table_stats(uint64_t* lookups, uint64_t* hits, uint64_t* slots)
     return kOk;
 }
 
-int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs) {
+int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs, uint32_t rlc_segment, const uint8_t* rand32) {
     if (!ready_) return set_error(kErrGpuDevice, "context not ready");
+    size_t n_rlc = 0;
+    for (size_t j = 0; j < n_jobs; ++j) n_rlc += (jobs[j].kind == 2 && jobs[j].count) ? 1 : 0;
+    if (n_rlc == 0) return verify_queue_jobs(jobs, n_jobs);
+    std::vector<VerifyJob> queue, rlc_jobs;
+    queue.reserve(n_jobs - n_rlc);
+    rlc_jobs.reserve(n_rlc);
+    for (size_t j = 0; j < n_jobs; ++j) {
+        if (jobs[j].kind == 2) {
+            if (jobs[j].count) rlc_jobs.push_back(jobs[j]);
+        } else {
+            queue.push_back(jobs[j]);
+        }
+    }
+    uint8_t zero[32] = {0};
+    const uint8_t* r32 = rand32 ? rand32 : zero;
+    const uint32_t seg = rlc_segment ? rlc_segment : kRlcJobSegment;
+    RlcVerifier& R = rlc();
+    int rc = kOk;
+    size_t j = 0, off = 0;
+    if (!queue.empty()) {
+        // the first RLC pass's items are copied into pinned staging by helper
+        // threads while the kind 0 / 1 jobs run (their packing and device time)
+        if ((rc = R.stage_jobs(rlc_jobs.data(), rlc_jobs.size(), &j, &off)) != kOk) return rc;
+        const size_t n = R.staged();
+        const int helpers = std::max(1, pack_threads_ - 1);
+        std::vector<std::thread> th;
+        for (int t = 0; t < helpers; ++t)
+            th.emplace_back([&R, n, t, helpers]() { R.pack_staged(n * t / helpers, n * (t + 1) / helpers); });
+        rc = verify_queue_jobs(queue.data(), queue.size());
+        for (std::thread& x : th) x.join();
+        if (rc != kOk) return rc;
+        if ((rc = R.run_staged(seg, r32, nullptr)) != kOk) return rc;
+    }
+    // the rest (all of it without kind 0 / 1 jobs), kMaxItems items per pass
+    while (j < rlc_jobs.size()) {
+        if ((rc = R.stage_jobs(rlc_jobs.data(), rlc_jobs.size(), &j, &off)) != kOk) return rc;
+        if (R.staged() == 0) break;
+        parallel_copy(R.staged(), [&R](size_t lo, size_t hi) { R.pack_staged(lo, hi); });
+        if ((rc = R.run_staged(seg, r32, nullptr)) != kOk) return rc;
+    }
+    clear_error();
+    return kOk;
+}
+
+void Backend::parallel_copy(size_t n, const std::function<void(size_t, size_t)>& fn) {
+    if (pack_threads_ > 1 && n >= kPackSplitItems) {
+        if (!pack_pool_) pack_pool_.reset(new PackPool(pack_threads_));
+        const int parts = pack_pool_->threads();
+        pack_pool_->run(parts, [&](int p) { fn(n * p / parts, n * (p + 1) / parts); });
+    } else {
+        fn(0, n);
+    }
+}
+
+int Backend::verify_queue_jobs(const VerifyJob* jobs, size_t n_jobs) {
     NvtxRange range("ufsecp verify_jobs");
     if (key_log2_ && !keys_) {
         auto kt = std::make_unique<KeyTable>();

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <atomic>
 #include <map>
+#include <functional>
 #include <memory>
 #include <string>
 
@@ -79,8 +80,13 @@ public:
                     uint8_t* d_pubs, uint8_t* d_sigs, uint8_t* d_ok, cudaStream_t stream);
     // Mixed ECDSA / BIP-340 jobs (host buffers) in one persistent-queue launch;
     // synchronous.  Keys go through the context's resident key table when it
-    // is on (set_key_table).
-    int verify_jobs(const VerifyJob* jobs, size_t n_jobs);
+    // is on (set_key_table).  Kind 2 jobs (BIP-340 by RLC) are verified after
+    // the others by the RLC verifier, all in one batch of `rlc_segment`-item
+    // segments (0 = kRlcJobSegment), its weights seeded by the items' digest
+    // XOR rand32.
+    int verify_jobs(const VerifyJob* jobs, size_t n_jobs, uint32_t rlc_segment = 0,
+                    const uint8_t* rand32 = nullptr);
+    static constexpr uint32_t kRlcJobSegment = 16384;
     // Resident key table of verify_jobs: 0 = off, 8..24 = an empty table of
     // 2^log2 slots (the current table emptied in place when it has that size,
     // else a new one made on the next verify_jobs call).  The default is the
@@ -216,6 +222,14 @@ private:
     int queue_pair_grid_ = 0;
     std::unique_ptr<BatchSlot> batch_[2];   // slots of the synchronous mixed-batch call (two for large calls)
     std::unique_ptr<KeyTable> keys_;        // resident key table of verify_jobs (made on first use)
+    int verify_queue_jobs(const VerifyJob* jobs, size_t n_jobs);   // kinds 0 and 1
+
+public:
+    // fn(lo, hi) over [0, n) split between the staging-copy threads (the
+    // caller included) when n is large enough to pay for them.
+    void parallel_copy(size_t n, const std::function<void(size_t, size_t)>& fn);
+
+private:
     uint32_t key_log2_ = 18;
     std::unique_ptr<RlcVerifier> rlc_;
     std::map<uint32_t, int> rlc_window_;   // tuned window bits per RLC batch size

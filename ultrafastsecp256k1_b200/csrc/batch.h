@@ -25,7 +25,7 @@
 namespace uf {
 
 struct VerifyJob {
-    int kind;             // 0 ECDSA (33-byte keys), 1 BIP-340 (32-byte x-only keys)
+    int kind;             // 0 ECDSA (33-byte keys), 1 BIP-340 (32-byte x-only keys), 2 BIP-340 by RLC
     size_t count;
     const uint8_t* msgs;  // count x 32, host memory
     const uint8_t* pubs;

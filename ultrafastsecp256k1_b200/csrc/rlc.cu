@@ -1228,6 +1228,7 @@ RlcVerifier::~RlcVerifier() {
                       &in_out_, &in_rows_, &gate_, &segpt_, &dig_a_, &dig_b_, &lmags_, &lmags_hi_, &tsave_,
                       &loc_idx_, &found_, &heavy_, &aff_pts_, &aff_suf_, &aff_tp_, &aff_meta_, &binv_})
         b->release();
+    job_host_.release();
 }
 
 int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t s, std::vector<uint8_t>& ok,
@@ -1625,6 +1626,91 @@ int RlcVerifier::verify_host(const uint8_t* msgs, const uint8_t* xs, const uint8
     e = cudaMemcpyAsync(out, in_out_.p, n, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC copy out");
+    return kOk;
+}
+
+int RlcVerifier::stage_jobs(const VerifyJob* jobs, size_t n_jobs, size_t* j, size_t* off) {
+    part_.clear();
+    start_.clear();
+    uint64_t n = 0;
+    while (*j < n_jobs && n < kMaxItems) {
+        const VerifyJob& J = jobs[*j];
+        if (*off >= J.count) {
+            ++*j;
+            *off = 0;
+            continue;
+        }
+        const size_t take = std::min<size_t>(J.count - *off, kMaxItems - n);
+        part_.push_back(VerifyJob{J.kind, take, J.msgs + 32 * *off, J.pubs + 32 * *off, J.sigs + 64 * *off,
+                                  J.out + *off});
+        start_.push_back(n);
+        n += take;
+        *off += take;
+    }
+    staged_ = n;
+    if (n == 0) return kOk;
+    cudaError_t e;
+    if ((e = in_m_.ensure(32ull * n)) != cudaSuccess || (e = in_x_.ensure(32ull * n)) != cudaSuccess ||
+        (e = in_s_.ensure(64ull * n)) != cudaSuccess || (e = in_out_.ensure(n)) != cudaSuccess ||
+        (e = job_host_.ensure(129ull * n)) != cudaSuccess)
+        return be_->cuda_error(e, "RLC job staging buffers");
+    return kOk;
+}
+
+void RlcVerifier::pack_staged(size_t lo, size_t hi) {
+    const uint64_t n = staged_;
+    uint8_t* hm = (uint8_t*)job_host_.p;
+    uint8_t* hx = hm + 32 * n;
+    uint8_t* hs = hx + 32 * n;
+    size_t q = std::upper_bound(start_.begin(), start_.end(), (uint64_t)lo) - start_.begin() - 1;
+    for (size_t i = lo; i < hi && q < part_.size(); ++q) {
+        const VerifyJob& P = part_[q];
+        const size_t a0 = i - start_[q], a1 = std::min<size_t>(P.count, hi - start_[q]);
+        memcpy(hm + 32 * i, P.msgs + 32 * a0, 32 * (a1 - a0));
+        memcpy(hx + 32 * i, P.pubs + 32 * a0, 32 * (a1 - a0));
+        memcpy(hs + 64 * i, P.sigs + 64 * a0, 64 * (a1 - a0));
+        i += a1 - a0;
+    }
+}
+
+int RlcVerifier::run_staged(uint32_t segment, const uint8_t rand32[32], RlcStats* stats) {
+    const uint64_t n = staged_;
+    if (n == 0) return kOk;
+    const cudaStream_t s = be_->stream();
+    uint8_t* hm = (uint8_t*)job_host_.p;
+    uint8_t* hx = hm + 32 * n;
+    uint8_t* hs = hx + 32 * n;
+    uint8_t* ho = hs + 64 * n;
+    uint8_t* dm = (uint8_t*)in_m_.p;
+    uint8_t* dx = (uint8_t*)in_x_.p;
+    uint8_t* ds = (uint8_t*)in_s_.p;
+    cudaError_t e = cudaMemcpyAsync(dm, hm, 32 * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, hx, 32 * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, hs, 64 * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC job copy in");
+    uint8_t seed[32];
+    int rc = input_digest(dm, dx, ds, (uint32_t)n, s, seed);
+    if (rc != kOk) return rc;
+    for (int k = 0; k < 32; ++k) seed[k] ^= rand32[k];
+    rc = verify(dm, dx, ds, (uint32_t)n, segment, seed, 0, (uint8_t*)in_out_.p, nullptr, s, stats);
+    if (rc != kOk) return rc;
+    e = cudaMemcpyAsync(ho, in_out_.p, n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return be_->cuda_error(e, "RLC job copy out");
+    for (size_t q = 0; q < part_.size(); ++q) memcpy(part_[q].out, ho + start_[q], part_[q].count);
+    return kOk;
+}
+
+int RlcVerifier::verify_jobs_host(const VerifyJob* jobs, size_t n_jobs, uint32_t segment, const uint8_t rand32[32],
+                                  RlcStats* stats) {
+    NvtxRange range("RLC jobs");
+    size_t j = 0, off = 0;
+    while (j < n_jobs) {
+        if (const int rc = stage_jobs(jobs, n_jobs, &j, &off)) return rc;
+        if (staged_ == 0) break;
+        be_->parallel_copy(staged_, [&](size_t lo, size_t hi) { pack_staged(lo, hi); });
+        if (const int rc = run_staged(segment, rand32, stats)) return rc;
+    }
     return kOk;
 }
 

@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "backend.h"
+#include "batch.h"
 
 namespace uf {
 
@@ -74,6 +75,24 @@ public:
     // back on the backend's stream.
     int verify_host(const uint8_t* msgs, const uint8_t* xs, const uint8_t* sigs, uint32_t n, uint32_t batch_size,
                     const uint8_t seed[32], int window_bits, uint8_t* out, uint8_t* h_batch_ok, RlcStats* stats);
+
+    // Host-buffer BIP-340 jobs (kind 2 of verify_jobs) as one RLC batch of
+    // `segment`-item segments: the jobs' items are copied in back to back (at
+    // most kMaxItems per pass; a job may be split between passes), the
+    // weights seeded by input_digest() of the pass XOR rand32, and each job's
+    // verdicts copied back to its own buffer.  Synchronous.
+    int verify_jobs_host(const VerifyJob* jobs, size_t n_jobs, uint32_t segment, const uint8_t rand32[32],
+                         RlcStats* stats);
+    // verify_jobs_host in three steps, so that the host copies can overlap
+    // other device work: stage_jobs takes the jobs from (*j, *off) on, up to
+    // kMaxItems items (advancing *j, *off), and sizes the buffers;
+    // pack_staged copies staged items [lo, hi) into pinned staging (host
+    // memory only: any thread, ranges split between threads);
+    // run_staged verifies them and writes each job's verdicts.
+    int stage_jobs(const VerifyJob* jobs, size_t n_jobs, size_t* j, size_t* off);
+    uint64_t staged() const { return staged_; }
+    void pack_staged(size_t lo, size_t hi);
+    int run_staged(uint32_t segment, const uint8_t rand32[32], RlcStats* stats);
 
     // Rows of the reference batch API, [x(P) 32 | message 32 | signature 64]
     // (ufsecp_schnorr_batch_verify, src/cpu/src/impl/ufsecp_taproot.cpp:703).
@@ -145,6 +164,10 @@ private:
     DevBuf lmags_, lmags_hi_, tsave_, loc_idx_, found_;   // locate step
     DevBuf heavy_;       // count and keys of the buckets with many chunks (k_rlc_bucket_heavy)
     DevBuf aff_pts_, aff_suf_, aff_tp_, aff_meta_, binv_;   // affine chunk trees
+    HostBuf job_host_;   // pinned staging of verify_jobs_host
+    std::vector<VerifyJob> part_;   // the staged job pieces, and their first items
+    std::vector<uint64_t> start_;
+    uint64_t staged_ = 0;
     std::vector<uint8_t> ok_host_;
 };
 

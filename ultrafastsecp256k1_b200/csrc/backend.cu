@@ -599,6 +599,14 @@ int Backend::verify_jobs(const VerifyJob* jobs, size_t n_jobs, uint32_t rlc_segm
         const size_t n = R.staged();
         const int helpers = std::max(1, pack_threads_ - 1);
         std::vector<std::thread> th;
+        // joined on every way out, an exception from the queue part included
+        struct JoinAll {
+            std::vector<std::thread>& v;
+            ~JoinAll() {
+                for (std::thread& x : v)
+                    if (x.joinable()) x.join();
+            }
+        } join_all{th};
         for (int t = 0; t < helpers; ++t)
             th.emplace_back([&R, n, t, helpers]() { R.pack_staged(n * t / helpers, n * (t + 1) / helpers); });
         rc = verify_queue_jobs(queue.data(), queue.size());

@@ -280,7 +280,12 @@ k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint32_t* __restr
     if (p < 3u * len) {
         pidx = 3u * g.seg[2 * s] + p;
         m = mags[pidx];
-        if (mags_hi) mhi = mags_hi[pidx];
+        if (mags_hi) {
+            // locate round: bits 128.. of the magnitude, bit 31 = the point enters negated
+            mhi = mags_hi[pidx];
+            neg = (mhi >> 31) != 0;
+            mhi &= 0x7FFFFFFFu;
+        }
     } else {
         const uint32_t j = 2u * s + (p - 3u * len);
         pidx = g.n3 + j;
@@ -931,17 +936,27 @@ k_rlc_finish(RoundGeo g, const uint4* __restrict__ wins, const uint32_t* __restr
 // candidate is verified by the plain kernel, so a verdict never rests on the
 // search.
 
-// Per item of the listed segments: its three magnitudes times j = i - i0 + 1
-// (up to 129 + 17 bits: four words in lmags, the fifth in lmags_hi).
+// Per item of the listed segments, the locate round's magnitudes for the
+// weight j a with j = i - i0 + 1: R's magnitude a times j (up to 128 + 16
+// bits: four words in lmags, the fifth in lmags_hi), and for the two P
+// points the GLV halves of j (a e) mod n, re-split so that they stay below
+// 2^128 (the check round's halves times j would need up to 16 more bits, and
+// so more windows of entries).  The stored points are P1 = s1 P and
+// P2 = s2 lambda P (signs folded into y), so a e = k1 + s lambda k2 with
+// s = s1 s2 (read off the two stored y coordinates), and for a new split
+// K = j a e = t1 k1' + t2 lambda k2' the terms are t1 k1' P1 + (t2 s) k2' P2;
+// bit 31 of lmags_hi marks a term whose point enters negated.
 __global__ void __launch_bounds__(256)
-k_rlc_scale(const uint32_t* __restrict__ seg, const uint4* __restrict__ mags, uint4* __restrict__ lmags,
-            uint32_t* __restrict__ lmags_hi) {
+k_rlc_scale(const uint32_t* __restrict__ seg, const uint4* __restrict__ mags, const RlcItem* __restrict__ items,
+            uint4* __restrict__ lmags, uint32_t* __restrict__ lmags_hi) {
+    const Sc LAM = {{0x1B23BD72u, 0xDF02967Cu, 0x20816678u, 0x122E22EAu,
+                     0x8812645Au, 0xA5261C02u, 0xC05C30E0u, 0x5363AD4Cu}};
     const uint32_t s = blockIdx.x;
     const uint32_t i0 = seg[2 * s], len = seg[2 * s + 1];
-    for (uint32_t k = threadIdx.x; k < 3u * len; k += blockDim.x) {
-        const uint64_t pidx = 3ull * i0 + k;
-        const uint32_t j = k / 3u + 1u;
-        const uint4 m = mags[pidx];
+    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
+        const uint64_t i = (uint64_t)i0 + k;
+        const uint32_t j = k + 1u;
+        const uint4 m = mags[3 * i];
         uint64_t c = (uint64_t)m.x * j;
         uint4 r;
         r.x = (uint32_t)c;
@@ -951,8 +966,27 @@ k_rlc_scale(const uint32_t* __restrict__ seg, const uint4* __restrict__ mags, ui
         r.z = (uint32_t)c;
         c = (uint64_t)m.w * j + (c >> 32);
         r.w = (uint32_t)c;
-        lmags[pidx] = r;
-        lmags_hi[pidx] = (uint32_t)(c >> 32);
+        lmags[3 * i] = r;
+        lmags_hi[3 * i] = (uint32_t)(c >> 32);
+        const uint4 a1 = mags[3 * i + 1], a2 = mags[3 * i + 2];
+        Sc k1 = {{a1.x, a1.y, a1.z, a1.w, 0, 0, 0, 0}}, k2 = {{a2.x, a2.y, a2.z, a2.w, 0, 0, 0, 0}};
+        // s = +1 when the stored P1 and P2 have the same y
+        const uint4* y1 = items[i].pt[1] + 2;
+        const uint4* y2 = items[i].pt[2] + 2;
+        const uint4 u0 = y1[0], u1 = y1[1], v0 = y2[0], v1 = y2[1];
+        const bool flip = ((u0.x ^ v0.x) | (u0.y ^ v0.y) | (u0.z ^ v0.z) | (u0.w ^ v0.w) | (u1.x ^ v1.x) |
+                           (u1.y ^ v1.y) | (u1.z ^ v1.z) | (u1.w ^ v1.w)) != 0;
+        Sc t, K, jj = {{j, 0, 0, 0, 0, 0, 0, 0}};
+        sc_mul(t, k2, LAM);
+        if (flip) sc_neg(t, t);
+        sc_add(K, k1, t);
+        sc_mul(K, K, jj);
+        GlvSplit g;
+        glv_split(g, K);
+        lmags[3 * i + 1] = make_uint4(g.k1[0], g.k1[1], g.k1[2], g.k1[3]);
+        lmags[3 * i + 2] = make_uint4(g.k2[0], g.k2[1], g.k2[2], g.k2[3]);
+        lmags_hi[3 * i + 1] = g.neg1 ? 0x80000000u : 0u;
+        lmags_hi[3 * i + 2] = (g.neg2 != flip) ? 0x80000000u : 0u;
     }
 }
 
@@ -1238,7 +1272,8 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     const uint32_t n_seg = (uint32_t)(seg.size() / 2);
     uint32_t maxlen = 0;
     for (uint32_t k = 0; k < n_seg; ++k) maxlen = std::max(maxlen, seg[2 * k + 1]);
-    // a locate round's magnitudes carry the factor j <= maxlen: 129 + bits(maxlen) bits
+    // a locate round's R magnitudes carry the factor j <= maxlen: 128 + bits(maxlen)
+    // bits, + 1 for the signed top digit (its P halves stay below 2^128)
     int mag_bits = 129;
     if (locate)
         for (uint32_t v = maxlen; v; v >>= 1) ++mag_bits;
@@ -1293,7 +1328,8 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     if (e == cudaSuccess) e = cudaMemsetAsync(heavy_.p, 0, 4, s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC round set-up");
     if (locate)
-        k_rlc_scale<<<n_seg, 256, 0, s>>>(d_seg, (const uint4*)mags_.p, (uint4*)lmags_.p, (uint32_t*)lmags_hi_.p);
+        k_rlc_scale<<<n_seg, 256, 0, s>>>(d_seg, (const uint4*)mags_.p, (const RlcItem*)items_.p, (uint4*)lmags_.p,
+                                          (uint32_t*)lmags_hi_.p);
     k_rlc_tsum<<<n_seg, 256, 0, s>>>(g, (const uint32_t*)tsc_.p, (const uint8_t*)okb_.p, (uint4*)segmag_.p,
                                      (uint8_t*)segneg_.p, (uint32_t*)segbad_.p, locate ? 1 : 0);
     k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, mags_hi, (const uint4*)segmag_.p,

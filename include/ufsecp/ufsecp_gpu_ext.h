@@ -153,6 +153,10 @@ UFSECP_API ufsecp_error_t ufsecp_gpu_ext_schnorr_verify_rlc_device(ufsecp_gpu_ct
  * rlc_located: failing segments the locate step resolved. */
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_stats(ufsecp_gpu_ctx* ctx, uint64_t out[4]);
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_located(ufsecp_gpu_ctx* ctx, uint64_t* located);
+/* Items of the last RLC call whose x-only key was resident in the context's
+ * key table (ufsecp_gpu_ext_set_key_table; keys enter it through
+ * ufsecp_gpu_ext_verify_jobs): their lift_x square root was skipped. */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_rlc_key_hits(ufsecp_gpu_ctx* ctx, uint64_t* hits);
 
 /* Locate step of RLC verification (on = 1, the default; 0 = bisection only).
  * A failing batch S with sum T = sum a_i D_i != infinity (D_i = R_i + e_i P_i

@@ -353,3 +353,28 @@ def test_rlc_input_digest_matches_hashlib(gpu_ctx, oracle, n):
         m2 = m.copy()
         m2[n - 1, 0] ^= 1
         assert gpu_ctx.rlc_input_digest(m2, x, s) != gpu_ctx.rlc_input_digest(m, x, s)
+
+
+def test_rlc_uses_resident_keys(oracle):
+    """Keys left in the context's key table by a mixed-job call give the RLC
+    prep their y without a square root (entry 0 of the slot's table), and a
+    key the table knows to be off the curve fails as lift_x would: verdicts
+    equal the oracle's with and without resident keys."""
+    m, x, s = schnorr_corpus(oracle, 3000, seed=91, tamper=0.03)
+    x = x.copy()
+    x[::37, 7] ^= 0x10                    # some keys off the curve (the oracle decides which)
+    idx = np.array([i % 3000 for i in range(6000)])
+    m, x, s = m[idx].copy(), x[idx].copy(), s[idx].copy()
+    want = oracle.schnorr_verify_batch(m, x, s)
+    with uf.GpuContext(0) as ctx:
+        out0, _ = ctx.schnorr_verify_rlc(m, x, s, batch_size=512, seed32=SEED)
+        assert ctx.rlc_stats()["key_hits"] == 0         # no table made yet
+        assert (out0 == want).all()
+        assert all((g == w).all() for g, w in zip(ctx.verify_jobs([(1, m, x, s)]), [want]))
+        out1, _ = ctx.schnorr_verify_rlc(m, x, s, batch_size=512, seed32=SEED)
+        st = ctx.rlc_stats()
+        assert (out1 == want).all()
+        assert st["key_hits"] >= 0.9 * len(m)
+        ctx.set_key_table(0)
+        out2, _ = ctx.schnorr_verify_rlc(m, x, s, batch_size=512, seed32=SEED)
+        assert (out2 == want).all() and ctx.rlc_stats()["key_hits"] == 0

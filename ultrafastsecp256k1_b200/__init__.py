@@ -139,6 +139,7 @@ _SIGS = {
     "ufsecp_gpu_ext_server_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats), ctypes.c_int]),
     "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "ufsecp_gpu_ext_rlc_key_hits": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_set_key_table": (ctypes.c_int, [_vp, ctypes.c_uint32]),
     "ufsecp_gpu_ext_set_rlc_locate": (ctypes.c_int, [_vp, ctypes.c_int]),
     "ufsecp_gpu_ext_rlc_located": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
@@ -461,7 +462,10 @@ class GpuContext:
         self._check(self.L.ufsecp_gpu_ext_rlc_stats(self._ctx, v), "rlc_stats")
         loc = ctypes.c_uint64()
         self._check(self.L.ufsecp_gpu_ext_rlc_located(self._ctx, ctypes.byref(loc)), "rlc_located")
-        return {"rounds": v[0], "segments": v[1], "leaf_items": v[2], "window_bits": v[3], "located": loc.value}
+        kh = ctypes.c_uint64()
+        self._check(self.L.ufsecp_gpu_ext_rlc_key_hits(self._ctx, ctypes.byref(kh)), "rlc_key_hits")
+        return {"rounds": v[0], "segments": v[1], "leaf_items": v[2], "window_bits": v[3], "located": loc.value,
+                "key_hits": kh.value}
 
     def set_rlc_locate(self, on: bool):
         """ufsecp_gpu_ext_set_rlc_locate: the locate step of RLC verification on / off."""

@@ -844,6 +844,12 @@ ufsecp_error_t ufsecp_gpu_ext_rlc_located(ufsecp_gpu_ctx* ctx, uint64_t* located
     return UFSECP_OK;
 }
 
+ufsecp_error_t ufsecp_gpu_ext_rlc_key_hits(ufsecp_gpu_ctx* ctx, uint64_t* hits) {
+    if (!ctx || !hits) return UFSECP_ERR_NULL_ARG;
+    *hits = ctx->rlc_stats.key_hits;
+    return UFSECP_OK;
+}
+
 ufsecp_error_t ufsecp_gpu_ext_schnorr_batch_verify(ufsecp_gpu_ctx* ctx, const uint8_t* entries, size_t n) {
     if (!ctx) return UFSECP_ERR_NULL_ARG;
     if (n == 0) return UFSECP_OK;

@@ -93,6 +93,8 @@ public:
     // tuning file's key_table_log2, else UFSECP_B200_KEY_TABLE, else 18.
     int set_key_table(uint32_t log2);
     uint32_t key_table_log2() const { return key_log2_; }
+    // The table itself once made (null before the first mixed-job call).
+    const KeyTable* key_table() const { return keys_.get(); }
     // lookups, hits since the table was made; slots (0 = off / not made yet)
     int key_table_stats(uint64_t* lookups, uint64_t* hits, uint64_t* slots);
     // RLC batch verifier of BIP-340 signatures (created on first use).

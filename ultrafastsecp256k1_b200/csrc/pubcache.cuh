@@ -121,6 +121,22 @@ __device__ __forceinline__ uint32_t key_resolve(PubCacheSlot* slots, uint32_t ma
     return kNoSlot;
 }
 
+// Read-only probe (no slot is claimed): the slot index holding the key when it
+// is READY (its table built) or BAD (known off the curve), else kNoSlot.
+// For callers that only need the decompressed key (entry 0 of the table is
+// the key's point itself) and build nothing.
+__device__ __forceinline__ uint32_t key_lookup(const PubCacheSlot* slots, uint32_t mask, const Fe& x, bool odd) {
+    const uint32_t h = key_hash(x, odd);
+    for (int p = 0; p < kKeyProbes; ++p) {
+        const uint32_t idx = (h + (uint32_t)p) & mask;
+        const PubCacheSlot& s = slots[idx];
+        const uint32_t st = slot_state(s);
+        if (st == kSlotEmpty) return kNoSlot;
+        if ((st == kSlotReady || st == kSlotBad) && slot_has_key(s, x, odd)) return idx;
+    }
+    return kNoSlot;
+}
+
 // The verify kernels' view of an item's slot (resolved before the launch).
 struct SlotPubCache {
     const PubCacheSlot* slot;   // null: no slot

@@ -17,6 +17,7 @@
 
 #include "dev_tables.cuh"
 #include "kernels.h"
+#include "keytable.h"
 #include "sign.cuh"
 #include "grpinv.cuh"
 #include "verify.cuh"
@@ -108,9 +109,11 @@ __device__ __forceinline__ void load_point(uint32_t pidx, const RlcItem* __restr
 __global__ void __launch_bounds__(128)
 k_rlc_prep(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ xs, const uint8_t* __restrict__ sigs,
            uint32_t n, RlcSeed seed, RlcItem* __restrict__ items, uint4* __restrict__ mags,
-           uint32_t* __restrict__ tsc, uint8_t* __restrict__ okb, uint8_t* __restrict__ out) {
+           uint32_t* __restrict__ tsc, uint8_t* __restrict__ okb, uint8_t* __restrict__ out,
+           const PubCacheSlot* __restrict__ keys, uint32_t key_mask, unsigned long long* __restrict__ key_hits) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const unsigned live = __activemask();       // the warp's threads with an item
     uint32_t mw[8], pw[8], sw[16];
     load_words8(mw, msgs + 32ull * i);
     load_words8(pw, xs + 32ull * i);
@@ -123,7 +126,28 @@ k_rlc_prep(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ xs, con
     words_be_to_limbs(s.v, sw + 8);
     words_be_to_limbs(px.v, pw);
     bool ok = limbs_lt_p(r) && !sc_is_zero(s) && limbs_lt_n(s.v) && limbs_lt_p(px.v);
-    if (ok) ok = lift_x_parity(py, px, false);
+    // a key resident in the context's key table (left by earlier mixed-job
+    // calls) gives its y without the square root; a key known to be off the
+    // curve fails as lift_x would
+    bool lifted = false;
+    if (ok && keys) {
+        const uint32_t idx = key_lookup(keys, key_mask, px, false);
+        if (idx != kNoSlot) {
+            const PubCacheSlot& ks = keys[idx];
+            if (slot_state(ks) == kSlotBad) {
+                ok = false;
+            } else {
+                Fe kx;
+                load_aff(ks.tab, kx, py);     // entry 0 of the table: the key's point
+            }
+            lifted = true;
+        }
+    }
+    if (keys) {
+        const unsigned hits = __ballot_sync(live, lifted);
+        if (hits && (threadIdx.x & 31u) == (uint32_t)(__ffs(live) - 1)) atomicAdd(key_hits, (unsigned long long)__popc(hits));
+    }
+    if (ok && !lifted) ok = lift_x_parity(py, px, false);
     if (ok) {
         for (int k = 0; k < 8; ++k) rx.v[k] = r[k];
         ok = lift_x_parity(ry, rx, false);
@@ -1260,7 +1284,7 @@ RlcVerifier::~RlcVerifier() {
                       &cursor_, &nch_, &coff_, &entries_, &partials_, &buckets_, &wu_, &wt_, &wins_, &segok_,
                       &scan_tmp_, &leaf_idx_, &leaf_m_, &leaf_x_, &leaf_s_, &leaf_out_, &in_m_, &in_x_, &in_s_,
                       &in_out_, &in_rows_, &gate_, &segpt_, &dig_a_, &dig_b_, &lmags_, &lmags_hi_, &tsave_,
-                      &loc_idx_, &found_, &heavy_, &aff_pts_, &aff_suf_, &aff_tp_, &aff_meta_, &binv_})
+                      &loc_idx_, &found_, &heavy_, &aff_pts_, &aff_suf_, &aff_tp_, &aff_meta_, &binv_, &keyhit_})
         b->release();
     job_host_.release();
 }
@@ -1575,9 +1599,23 @@ int RlcVerifier::verify(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_
         return be_->cuda_error(e, "RLC item buffers");
     RlcSeed sd;
     memcpy(sd.b, seed, 32);
+    // keys resident in the context's key table skip their square root
+    const KeyTable* kt = be_->key_table();
+    const bool use_keys = kt && kt->on();
+    if (use_keys && ((e = keyhit_.ensure(8)) != cudaSuccess || (e = cudaMemsetAsync(keyhit_.p, 0, 8, s)) != cudaSuccess))
+        return be_->cuda_error(e, "RLC key counter");
     k_rlc_prep<<<grid_for(n, 128), 128, 0, s>>>(d_msgs, d_xs, d_sigs, n, sd, (RlcItem*)items_.p, (uint4*)mags_.p,
-                                                (uint32_t*)tsc_.p, (uint8_t*)okb_.p, d_out);
+                                                (uint32_t*)tsc_.p, (uint8_t*)okb_.p, d_out,
+                                                use_keys ? kt->slots() : nullptr, use_keys ? kt->mask() : 0u,
+                                                use_keys ? (unsigned long long*)keyhit_.p : nullptr);
     if ((e = cudaGetLastError()) != cudaSuccess) return be_->cuda_error(e, "RLC prep");
+    if (stats && use_keys) {
+        unsigned long long hits = 0;
+        e = cudaMemcpyAsync(&hits, keyhit_.p, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return be_->cuda_error(e, "RLC key counter");
+        stats->key_hits += hits;
+    }
     std::vector<uint32_t> seg, next, leaves, loc, loc_round;
     for (uint32_t b = 0; b < n; b += batch_size) {
         seg.push_back(b);

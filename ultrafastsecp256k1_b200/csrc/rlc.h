@@ -45,6 +45,7 @@ struct RlcStats {
     uint64_t leaf_items = 0;      // items verified one by one (bisection leaves and locate candidates)
     int window_bits = 0;          // window of the first round
     uint64_t located = 0;         // failing segments resolved by a locate round
+    uint64_t key_hits = 0;        // items whose key came from the context's key table
 };
 
 class RlcVerifier {
@@ -165,6 +166,7 @@ private:
     DevBuf heavy_;       // count and keys of the buckets with many chunks (k_rlc_bucket_heavy)
     DevBuf aff_pts_, aff_suf_, aff_tp_, aff_meta_, binv_;   // affine chunk trees
     HostBuf job_host_;   // pinned staging of verify_jobs_host
+    DevBuf keyhit_;      // key-table hits of the prep pass
     std::vector<VerifyJob> part_;   // the staged job pieces, and their first items
     std::vector<uint64_t> start_;
     uint64_t staged_ = 0;

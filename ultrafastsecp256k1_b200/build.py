@@ -67,7 +67,10 @@ VARIANTS = {"kernels_verify.cu": _VARIANT_FLAGS + _WINDOW_FLAGS, "kernels_probe.
             # small calls are latency-bound: the two-lane kernel takes variant 6's
             # code generation (field ops inlined into out-of-line point ops)
             "kernels_pair.cu": [("", ["-DUF_NOINLINE_POINT", "-DUF_PTX_MUL"])],
-            "rlc.cu": [("", _BEST_FLAGS)], "kernels_ops.cu": [("", _BEST_FLAGS)]}
+            "rlc.cu": [("", _BEST_FLAGS)], "kernels_ops.cu": [("", _BEST_FLAGS)],
+            # the RLC kernels with one serial chain per segment or window run few
+            # threads: field and point operations inlined, for overlap inside a chain
+            "rlc_serial.cu": [("", ["-DUF_PTX_MUL"])]}
 
 
 def _sources():

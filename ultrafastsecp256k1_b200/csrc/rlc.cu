@@ -22,10 +22,14 @@
 #include "grpinv.cuh"
 #include "verify.cuh"
 #include "nvtx.h"
+#include "rlc_dev.cuh"
+#include "rlc_serial.h"
 
 namespace uf {
 
 namespace {
+
+using namespace rlcdev;
 
 struct RlcItem {
     uint4 pt[3][4];     // affine R, +-P, +-lambda P (x then y, 8 words each)
@@ -39,39 +43,6 @@ struct RlcSeed {
 // buckets (one thread each) and the S partial results are combined by one
 // thread; S = 2^floor((c - 1) / 2) balances the two serial chains.
 inline int sub_ranges(int c) { return 1 << ((c - 1) / 2); }
-
-__device__ __forceinline__ void store_aff(uint4* q, const Fe& x, const Fe& y) {
-    q[0] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
-    q[1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
-    q[2] = make_uint4(y.v[0], y.v[1], y.v[2], y.v[3]);
-    q[3] = make_uint4(y.v[4], y.v[5], y.v[6], y.v[7]);
-}
-
-__device__ __forceinline__ void load_aff(const uint4* q, Fe& x, Fe& y) {
-    const uint4 a = q[0], b = q[1], c = q[2], d = q[3];
-    x.v[0] = a.x; x.v[1] = a.y; x.v[2] = a.z; x.v[3] = a.w;
-    x.v[4] = b.x; x.v[5] = b.y; x.v[6] = b.z; x.v[7] = b.w;
-    y.v[0] = c.x; y.v[1] = c.y; y.v[2] = c.z; y.v[3] = c.w;
-    y.v[4] = d.x; y.v[5] = d.y; y.v[6] = d.z; y.v[7] = d.w;
-}
-
-// Jacobian point in global memory: X, Y, Z and the infinity flag (7 x uint4).
-constexpr int kJacQ = 7;
-
-__device__ __forceinline__ void store_jac(uint4* q, const Jac& P) {
-    store_aff(q, P.X, P.Y);
-    q[4] = make_uint4(P.Z.v[0], P.Z.v[1], P.Z.v[2], P.Z.v[3]);
-    q[5] = make_uint4(P.Z.v[4], P.Z.v[5], P.Z.v[6], P.Z.v[7]);
-    q[6] = make_uint4(P.inf ? 1u : 0u, 0u, 0u, 0u);
-}
-
-__device__ __forceinline__ void load_jac(const uint4* q, Jac& P) {
-    load_aff(q, P.X, P.Y);
-    const uint4 a = q[4], b = q[5];
-    P.Z.v[0] = a.x; P.Z.v[1] = a.y; P.Z.v[2] = a.z; P.Z.v[3] = a.w;
-    P.Z.v[4] = b.x; P.Z.v[5] = b.y; P.Z.v[6] = b.z; P.Z.v[7] = b.w;
-    P.inf = q[6].x != 0;
-}
 
 // Signed digit of window w (c bits) of a magnitude m + hi 2^128 < 2^160 (the
 // recoding of booth_recode in ecmult.cuh with a run-time window width).
@@ -201,16 +172,6 @@ k_rlc_prep(const uint8_t* __restrict__ msgs, const uint8_t* __restrict__ xs, con
     mags[3ull * i + 2] = make_uint4(g.k2[0], g.k2[1], g.k2[2], g.k2[3]);
     for (int k = 0; k < 8; ++k) tsc[8ull * i + k] = t.v[k];
 }
-
-// Round geometry in device memory: seg[2s], seg[2s+1] = first item, length of
-// segment s; pwf[s] = first (point, window) index of segment s, pwf[S] = total.
-struct RoundGeo {
-    const uint32_t* seg;
-    const uint32_t* pwf;
-    uint32_t n_seg;
-    uint32_t n3;             // 3 * items of the call: index of the first generator point
-    int c, W, B, S;          // window bits, windows, buckets per window, sub-ranges per window
-};
 
 // largest k < n with a[k] <= t (a non-decreasing, a[0] = 0 <= t)
 __device__ __forceinline__ uint32_t upper_index(const uint32_t* __restrict__ a, uint32_t n, uint32_t t) {
@@ -817,138 +778,6 @@ k_aff_bwd(AffArgs a, int level, uint32_t threads, int last) {
     }
 }
 
-// Buckets with 0 or >= 2 chunks: infinity, or the sum of their partials.
-// A bucket of more than kHeavyChunks chunks (skewed digits: the top windows
-// of a locate round's j-scaled magnitudes put most points of a segment into a
-// few buckets) is left to k_rlc_bucket_heavy: its key goes to `heavy`.
-constexpr uint32_t kHeavyChunks = 48;
-
-// Adds a chunk partial: affine (Z = 1, from k_rlc_chunks_aff) or Jacobian.
-template <bool kAff>
-__device__ __forceinline__ void add_partial(Jac& acc, const uint4* q) {
-    Jac p;
-    load_jac(q, p);
-    if (!kAff) jac_add(acc, p);
-    else if (!p.inf) jac_add_aff(acc, p.X, p.Y);
-}
-
-template <bool kAff>
-__global__ void __launch_bounds__(128)
-k_rlc_bucket_fin(const uint32_t* __restrict__ coff, uint32_t K, const uint4* __restrict__ partials,
-                 uint4* __restrict__ buckets, uint32_t* __restrict__ heavy) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= K) return;
-    const uint32_t c0 = coff[k], c1 = coff[k + 1];
-    if (c1 - c0 == 1) return;
-    if (c1 - c0 > kHeavyChunks) {
-        heavy[1 + atomicAdd(&heavy[0], 1u)] = k;
-        return;
-    }
-    Jac acc;
-    jac_set_inf(acc);
-    for (uint32_t c = c0; c < c1; ++c) add_partial<kAff>(acc, partials + kJacQ * (uint64_t)c);
-    store_jac(buckets + kJacQ * (uint64_t)k, acc);
-}
-
-// Jacobian point from lane `src` of the warp (every lane calls it).
-__device__ __forceinline__ Jac shfl_jac(const Jac& a, int src) {
-    Jac b;
-    for (int k = 0; k < 8; ++k) {
-        b.X.v[k] = __shfl_sync(0xFFFFFFFFu, a.X.v[k], src);
-        b.Y.v[k] = __shfl_sync(0xFFFFFFFFu, a.Y.v[k], src);
-        b.Z.v[k] = __shfl_sync(0xFFFFFFFFu, a.Z.v[k], src);
-    }
-    b.inf = __shfl_sync(0xFFFFFFFFu, a.inf ? 1 : 0, src) != 0;
-    return b;
-}
-
-// One warp per heavy bucket (heavy[0] of them, keys in heavy[1..]): lane l
-// sums partials l, l + 32, ..., then the 32 lane sums meet in a shuffle tree:
-// about chunks / 32 + 5 serial additions instead of chunks.
-template <bool kAff>
-__global__ void __launch_bounds__(128)
-k_rlc_bucket_heavy(const uint32_t* __restrict__ coff, const uint4* __restrict__ partials,
-                   uint4* __restrict__ buckets, const uint32_t* __restrict__ heavy) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < heavy[0]; w += warps) {
-        const uint32_t k = heavy[1 + w];
-        const uint32_t c0 = coff[k], c1 = coff[k + 1];
-        Jac acc;
-        jac_set_inf(acc);
-        for (uint32_t c = c0 + lane; c < c1; c += 32) add_partial<kAff>(acc, partials + kJacQ * (uint64_t)c);
-        for (int o = 16; o > 0; o >>= 1) {
-            const Jac other = shfl_jac(acc, (int)(lane ^ (uint32_t)o));
-            jac_add(acc, other);
-        }
-        if (lane == 0) store_jac(buckets + kJacQ * (uint64_t)k, acc);
-    }
-}
-
-// One thread per (segment, window, sub-range j of m buckets):
-// T_j = sum_b bucket_b, U_j = sum_b (b - j m + 1) bucket_b by running sums.
-__global__ void __launch_bounds__(128)
-k_rlc_wpart(RoundGeo g, const uint4* __restrict__ buckets, uint4* __restrict__ wu, uint4* __restrict__ wt) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= g.n_seg * (uint32_t)(g.W * g.S)) return;
-    const uint32_t sw = q / (uint32_t)g.S, j = q - sw * (uint32_t)g.S;
-    const int m = g.B / g.S;
-    const uint4* base = buckets + kJacQ * ((uint64_t)sw * g.B + (uint64_t)j * m);
-    Jac run, tot, b;
-    jac_set_inf(run);
-    jac_set_inf(tot);
-    for (int k = m - 1; k >= 0; --k) {
-        load_jac(base + kJacQ * k, b);
-        jac_add(run, b);
-        jac_add(tot, run);
-    }
-    store_jac(wu + kJacQ * (uint64_t)q, tot);
-    store_jac(wt + kJacQ * (uint64_t)q, run);
-}
-
-// One thread per (segment, window): window sum = sum_j U_j + m sum_j j T_j.
-__global__ void __launch_bounds__(128)
-k_rlc_wcomb(RoundGeo g, const uint4* __restrict__ wu, const uint4* __restrict__ wt, uint4* __restrict__ wins) {
-    const uint32_t sw = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sw >= g.n_seg * (uint32_t)g.W) return;
-    const uint64_t q0 = (uint64_t)sw * g.S;
-    Jac acc, run, jt, p;
-    jac_set_inf(acc);
-    jac_set_inf(run);
-    jac_set_inf(jt);
-    for (int j = g.S - 1; j >= 1; --j) {
-        load_jac(wt + kJacQ * (q0 + j), p);
-        jac_add(run, p);
-        jac_add(jt, run);
-    }
-    for (int m = g.B / g.S; m > 1; m >>= 1) jac_dbl(jt);
-    for (int j = 0; j < g.S; ++j) {
-        load_jac(wu + kJacQ * (q0 + j), p);
-        jac_add(acc, p);
-    }
-    jac_add(acc, jt);
-    store_jac(wins + kJacQ * (uint64_t)sw, acc);
-}
-
-// One thread per segment: Horner over the windows; ok = 1 if the sum is
-// infinity, | 2 if the segment holds an item that failed to parse.
-__global__ void __launch_bounds__(64)
-k_rlc_finish(RoundGeo g, const uint4* __restrict__ wins, const uint32_t* __restrict__ segbad,
-             uint8_t* __restrict__ segok, uint4* __restrict__ segpt) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= g.n_seg) return;
-    const uint4* base = wins + kJacQ * (uint64_t)s * g.W;
-    Jac acc, w;
-    load_jac(base + kJacQ * (g.W - 1), acc);
-    for (int k = g.W - 2; k >= 0; --k) {
-        for (int d = 0; d < g.c; ++d) jac_dbl(acc);
-        load_jac(base + kJacQ * k, w);
-        jac_add(acc, w);
-    }
-    segok[s] = (uint8_t)((acc.inf ? 1 : 0) | (segbad[s] ? 2 : 0));
-    store_jac(segpt + kJacQ * (uint64_t)s, acc);
-}
-
 // ---------------------------------------------------------------- locate --
 // A failing segment S (its sum T = sum a_i D_i != infinity, D_i the defect of
 // item i: R_i + e_i P_i - s_i G, infinity for a valid item) with exactly one
@@ -1378,27 +1207,21 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return be_->cuda_error(e, "RLC chunk count");
         if (const int rc = affine_chunks(chunk, nch, chunk_cap, coff, (uint32_t)K, offsets, s)) return rc;
-        k_rlc_bucket_fin<true><<<grid_for(K, 128), 128, 0, s>>>(coff, (uint32_t)K, (const uint4*)partials_.p,
-                                                                (uint4*)buckets_.p, (uint32_t*)heavy_.p);
-        k_rlc_bucket_heavy<true><<<be_->sms() * 4, 128, 0, s>>>(coff, (const uint4*)partials_.p, (uint4*)buckets_.p,
-                                                                (const uint32_t*)heavy_.p);
+        e = launch_rlc_bucket_merge(true, coff, (uint32_t)K, (const uint4*)partials_.p, (uint4*)buckets_.p,
+                                    (uint32_t*)heavy_.p, be_->sms() * 4, s);
+        if (e != cudaSuccess) return be_->cuda_error(e, "RLC bucket merge");
     } else {
         k_rlc_chunks<<<grid_for(chunk_cap, 128), 128, 0, s>>>(coff, (uint32_t)K, chunk, offsets,
                                                               (const uint32_t*)entries_.p, (const RlcItem*)items_.p,
                                                               3u * n_, (const uint4*)be_->gtab(),
                                                               (uint4*)partials_.p, (uint4*)buckets_.p);
-        k_rlc_bucket_fin<false><<<grid_for(K, 128), 128, 0, s>>>(coff, (uint32_t)K, (const uint4*)partials_.p,
-                                                                 (uint4*)buckets_.p, (uint32_t*)heavy_.p);
-        k_rlc_bucket_heavy<false><<<be_->sms() * 4, 128, 0, s>>>(coff, (const uint4*)partials_.p,
-                                                                 (uint4*)buckets_.p, (const uint32_t*)heavy_.p);
+        e = launch_rlc_bucket_merge(false, coff, (uint32_t)K, (const uint4*)partials_.p, (uint4*)buckets_.p,
+                                    (uint32_t*)heavy_.p, be_->sms() * 4, s);
+        if (e != cudaSuccess) return be_->cuda_error(e, "RLC bucket merge");
     }
-    k_rlc_wpart<<<grid_for((uint64_t)n_seg * W * S, 128), 128, 0, s>>>(g, (const uint4*)buckets_.p, (uint4*)wu_.p,
-                                                                       (uint4*)wt_.p);
-    k_rlc_wcomb<<<grid_for((uint64_t)n_seg * W, 128), 128, 0, s>>>(g, (const uint4*)wu_.p, (const uint4*)wt_.p,
-                                                                  (uint4*)wins_.p);
-    k_rlc_finish<<<grid_for(n_seg, 64), 64, 0, s>>>(g, (const uint4*)wins_.p, (const uint32_t*)segbad_.p,
-                                                   (uint8_t*)segok_.p, (uint4*)segpt_.p);
-    e = cudaGetLastError();
+    e = launch_rlc_windows(g, (const uint4*)buckets_.p, (uint4*)wu_.p, (uint4*)wt_.p, (uint4*)wins_.p,
+                           (const uint32_t*)segbad_.p, (uint8_t*)segok_.p, (uint4*)segpt_.p, s);
+    if (e == cudaSuccess) e = cudaGetLastError();
     ok.resize(n_seg);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ok.data(), segok_.p, n_seg, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -241,21 +241,21 @@ k_rlc_tsum(RoundGeo g, const uint32_t* __restrict__ tsc, const uint8_t* __restri
     }
 }
 
-// One thread per (point, window): pass 0 counts the non-zero digits of every
-// bucket key, pass 1 writes entry = point index | sign << 31 at the bucket's
-// cursor.  Key = (segment * W + window) * B + |digit| - 1.
 // One thread per point of the round: its segment (one search), magnitude and
 // sign are read once and all W of its c-bit digits go to their buckets.
-// pass 0 counts entries per (segment, window, |digit|) key, pass 1 writes
-// them at the scanned offsets (order within a bucket is arbitrary: bucket sums
-// do not depend on it).
+// pass 0 counts entries per (segment, window, |digit|) key (key = (segment W
+// + window) B + |digit| - 1) and keeps each entry's rank, pass 1 writes entry
+// = point index | sign << 31 at the key's scanned offset + rank (order within
+// a bucket is arbitrary: bucket sums do not depend on it).
 __global__ void __launch_bounds__(256)
 k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint32_t* __restrict__ mags_hi,
              const uint4* __restrict__ segmag, const uint8_t* __restrict__ segneg, uint32_t total,
-             uint32_t* __restrict__ counts, uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries, int pass) {
+             uint32_t* __restrict__ counts, uint32_t* __restrict__ ranks, const uint32_t* __restrict__ offsets,
+             uint32_t* __restrict__ entries, int pass) {
     const uint32_t W = (uint32_t)g.W;
+    const uint32_t npts = total / W;
     const uint32_t tp = blockIdx.x * blockDim.x + threadIdx.x;     // point of the round
-    if (tp >= total / W) return;
+    if (tp >= npts) return;
     const uint32_t s = upper_index(g.pwf, g.n_seg, tp * W);
     const uint32_t p = tp - g.pwf[s] / W;
     const uint32_t len = g.seg[2 * s + 1];
@@ -282,12 +282,10 @@ k_rlc_digits(RoundGeo g, const uint4* __restrict__ mags, const uint32_t* __restr
         const int d = booth_digit(m, mhi, (int)w, g.c);
         if (d == 0) continue;
         const uint32_t key = key0 + w * (uint32_t)g.B + (uint32_t)((d < 0 ? -d : d) - 1);
-        if (pass == 0) {
-            atomicAdd(&counts[key], 1u);
-        } else {
-            const uint32_t pos = atomicAdd(&cursor[key], 1u);
-            entries[pos] = pidx | (((d < 0) != neg) ? 0x80000000u : 0u);
-        }
+        // the count pass's atomic returns the entry's rank in its bucket; the
+        // scatter pass writes it there, with no atomic of its own
+        if (pass == 0) ranks[(size_t)w * npts + tp] = atomicAdd(&counts[key], 1u);
+        else entries[offsets[key] + ranks[(size_t)w * npts + tp]] = pidx | (((d < 0) != neg) ? 0x80000000u : 0u);
     }
 }
 
@@ -1152,7 +1150,8 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     if ((e = segs_.ensure(host.size() * 4)) != cudaSuccess || (e = segmag_.ensure(32ull * n_seg)) != cudaSuccess ||
         (e = segneg_.ensure(2ull * n_seg)) != cudaSuccess || (e = segbad_.ensure(4ull * n_seg)) != cudaSuccess ||
         (e = counts_.ensure((K + 1) * 4)) != cudaSuccess || (e = offsets_.ensure((K + 1) * 4)) != cudaSuccess ||
-        (e = cursor_.ensure((K + 1) * 4)) != cudaSuccess || (e = nch_.ensure((K + 1) * 4)) != cudaSuccess ||
+        (e = cursor_.ensure(std::max<uint64_t>(total, 1) * 4)) != cudaSuccess ||
+        (e = nch_.ensure((K + 1) * 4)) != cudaSuccess ||
         (e = coff_.ensure((K + 1) * 4)) != cudaSuccess ||
         (e = entries_.ensure(std::max<uint64_t>(total, 1) * 4)) != cudaSuccess ||
         (e = partials_.ensure(chunk_cap * 112)) != cudaSuccess || (e = buckets_.ensure(K * 112)) != cudaSuccess ||
@@ -1170,7 +1169,6 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     const RoundGeo g{d_seg, d_seg + 2 * n_seg, n_seg, 3u * n_, c, W, B, S};
     uint32_t* counts = (uint32_t*)counts_.p;
     uint32_t* offsets = (uint32_t*)offsets_.p;
-    uint32_t* cursor = (uint32_t*)cursor_.p;
     uint32_t* nch = (uint32_t*)nch_.p;
     uint32_t* coff = (uint32_t*)coff_.p;
     const uint4* mags = locate ? (const uint4*)lmags_.p : (const uint4*)mags_.p;
@@ -1185,16 +1183,16 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
                                           (uint32_t*)lmags_hi_.p);
     k_rlc_tsum<<<n_seg, 256, 0, s>>>(g, (const uint32_t*)tsc_.p, (const uint8_t*)okb_.p, (uint4*)segmag_.p,
                                      (uint8_t*)segneg_.p, (uint32_t*)segbad_.p, locate ? 1 : 0);
+    uint32_t* ranks = (uint32_t*)cursor_.p;
     k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, mags_hi, (const uint4*)segmag_.p,
                                                                  (const uint8_t*)segneg_.p, (uint32_t)total, counts,
-                                                                 nullptr, nullptr, 0);
+                                                                 ranks, nullptr, nullptr, 0);
     size_t tb = scan_tmp_.cap;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, counts, offsets, (int)(K + 1), s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(cursor, offsets, K * 4, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC scan");
     k_rlc_digits<<<grid_for(total / (size_t)W, 256), 256, 0, s>>>(g, mags, mags_hi, (const uint4*)segmag_.p,
                                                                  (const uint8_t*)segneg_.p, (uint32_t)total, nullptr,
-                                                                 cursor, (uint32_t*)entries_.p, 1);
+                                                                 ranks, offsets, (uint32_t*)entries_.p, 1);
     k_rlc_nchunks<<<grid_for(K + 1, 256), 256, 0, s>>>(counts, (uint32_t)K, chunk, nch);
     tb = scan_tmp_.cap;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tb, nch, coff, (int)(K + 1), s);

@@ -154,6 +154,7 @@ private:
     // per item
     DevBuf items_, mags_, tsc_, okb_;
     // per round
+    // cursor_: each entry's rank in its bucket (k_rlc_digits)
     DevBuf segs_, segmag_, segneg_, segbad_, counts_, offsets_, cursor_, nch_, coff_, entries_, partials_,
         buckets_, wu_, wt_, wins_, segok_, scan_tmp_;
     // leaves

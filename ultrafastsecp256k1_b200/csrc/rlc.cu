@@ -1379,7 +1379,12 @@ int RlcVerifier::locate(const std::vector<uint32_t>& round_idx, const std::vecto
         stats->rounds++;
         stats->segments += n_loc;
     }
-    k_rlc_locate<<<n_loc, 256, 0, s>>>((const uint4*)tsave_.p, (const uint4*)segpt_.p, (const uint32_t*)segs_.p,
+    // one thread per baby / giant step: ceil(sqrt(len + 1)) of them, rounded
+    // up to whole warps (fewer threads per block let more blocks share an SM)
+    uint32_t m = 1;
+    while (m * m < maxlen + 1) ++m;
+    const unsigned loc_threads = std::min(256u, (m + 31u) & ~31u);
+    k_rlc_locate<<<n_loc, loc_threads, 0, s>>>((const uint4*)tsave_.p, (const uint4*)segpt_.p, (const uint32_t*)segs_.p,
                                        (uint32_t*)found_.p);
     std::vector<uint32_t> found(n_loc);
     e = cudaGetLastError();

@@ -343,7 +343,9 @@ def run_ours(args):
     mixed = None
     rlc = None
     serving = None
-    if rank == 0:
+    # single-GPU sections: measured in the one-GPU run only (a multi-GPU run
+    # would hold every GPU while rank 0 alone runs them)
+    if rank == 0 and world == 1:
         try:
             c1 = bench_c1(ctx, torch)
         except Exception as e:   # reference library missing on this box

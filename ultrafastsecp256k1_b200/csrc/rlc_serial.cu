@@ -1,9 +1,11 @@
-// The RLC kernels with one serial chain per bucket, segment or window (the
-// merge of a bucket's chunk sums, running sums, window combination, Horner).  They run a
-// few thousand threads at most, so a chain's latency, not the issue rate,
-// sets their time; this file is compiled with the field and point operations
-// inlined, so that the independent products inside a doubling or an addition
-// overlap.
+// The RLC kernels with one serial chain per bucket, segment or window: the
+// merge of a bucket's chunk sums, the running sums, the window combination
+// and Horner.  The last three run a few thousand threads at most, so a
+// chain's latency, not the issue rate, sets their time, and the merge's
+// chains are short and uneven.  This file is compiled with the field and
+// point operations inlined, so that the independent products inside a
+// doubling or an addition overlap (measured faster for these kernels, slower
+// for the wide kernels of rlc.cu).
 #include "rlc_serial.h"
 
 #include "point.cuh"

@@ -804,7 +804,8 @@ k_rlc_scale(const uint32_t* __restrict__ seg, const uint4* __restrict__ mags, co
                      0x8812645Au, 0xA5261C02u, 0xC05C30E0u, 0x5363AD4Cu}};
     const uint32_t s = blockIdx.x;
     const uint32_t i0 = seg[2 * s], len = seg[2 * s + 1];
-    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
+    // blockIdx.y: which blockDim.x items of the segment
+    for (uint32_t k = blockIdx.y * blockDim.x + threadIdx.x; k < len; k += gridDim.y * blockDim.x) {
         const uint64_t i = (uint64_t)i0 + k;
         const uint32_t j = k + 1u;
         const uint4 m = mags[3 * i];
@@ -1179,8 +1180,9 @@ int RlcVerifier::run_round(const std::vector<uint32_t>& seg, int c, cudaStream_t
     if (e == cudaSuccess) e = cudaMemsetAsync(heavy_.p, 0, 4, s);
     if (e != cudaSuccess) return be_->cuda_error(e, "RLC round set-up");
     if (locate)
-        k_rlc_scale<<<n_seg, 256, 0, s>>>(d_seg, (const uint4*)mags_.p, (const RlcItem*)items_.p, (uint4*)lmags_.p,
-                                          (uint32_t*)lmags_hi_.p);
+        k_rlc_scale<<<dim3(n_seg, (maxlen + 255) / 256), 256, 0, s>>>(d_seg, (const uint4*)mags_.p,
+                                                                      (const RlcItem*)items_.p, (uint4*)lmags_.p,
+                                                                      (uint32_t*)lmags_hi_.p);
     k_rlc_tsum<<<n_seg, 256, 0, s>>>(g, (const uint32_t*)tsc_.p, (const uint8_t*)okb_.p, (uint4*)segmag_.p,
                                      (uint8_t*)segneg_.p, (uint32_t*)segbad_.p, locate ? 1 : 0);
     uint32_t* ranks = (uint32_t*)cursor_.p;

@@ -1603,19 +1603,6 @@ int RlcVerifier::run_staged(uint32_t segment, const uint8_t rand32[32], RlcStats
     return kOk;
 }
 
-int RlcVerifier::verify_jobs_host(const VerifyJob* jobs, size_t n_jobs, uint32_t segment, const uint8_t rand32[32],
-                                  RlcStats* stats) {
-    NvtxRange range("RLC jobs");
-    size_t j = 0, off = 0;
-    while (j < n_jobs) {
-        if (const int rc = stage_jobs(jobs, n_jobs, &j, &off)) return rc;
-        if (staged_ == 0) break;
-        be_->parallel_copy(staged_, [&](size_t lo, size_t hi) { pack_staged(lo, hi); });
-        if (const int rc = run_staged(segment, rand32, stats)) return rc;
-    }
-    return kOk;
-}
-
 int RlcVerifier::input_digest(const uint8_t* d_msgs, const uint8_t* d_xs, const uint8_t* d_sigs, uint32_t n,
                               cudaStream_t s, uint8_t out[32]) {
     // two ping-pong digest arrays: n leaves, then n / kTreeFan nodes per level

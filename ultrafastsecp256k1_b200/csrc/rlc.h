@@ -78,18 +78,13 @@ public:
                     const uint8_t seed[32], int window_bits, uint8_t* out, uint8_t* h_batch_ok, RlcStats* stats);
 
     // Host-buffer BIP-340 jobs (kind 2 of verify_jobs) as one RLC batch of
-    // `segment`-item segments: the jobs' items are copied in back to back (at
-    // most kMaxItems per pass; a job may be split between passes), the
-    // weights seeded by input_digest() of the pass XOR rand32, and each job's
-    // verdicts copied back to its own buffer.  Synchronous.
-    int verify_jobs_host(const VerifyJob* jobs, size_t n_jobs, uint32_t segment, const uint8_t rand32[32],
-                         RlcStats* stats);
-    // verify_jobs_host in three steps, so that the host copies can overlap
-    // other device work: stage_jobs takes the jobs from (*j, *off) on, up to
-    // kMaxItems items (advancing *j, *off), and sizes the buffers;
-    // pack_staged copies staged items [lo, hi) into pinned staging (host
-    // memory only: any thread, ranges split between threads);
-    // run_staged verifies them and writes each job's verdicts.
+    // segment-length segments, in three steps so that the host copies can
+    // overlap other device work: stage_jobs takes the jobs from (*j, *off) on,
+    // up to kMaxItems items (advancing *j, *off; a job may be split between
+    // passes), and sizes the buffers; pack_staged copies staged items [lo, hi)
+    // into pinned staging (host memory only: any thread, ranges split between
+    // threads); run_staged verifies them (weights seeded by input_digest() of
+    // the pass XOR rand32) and writes each job's verdicts.  Synchronous.
     int stage_jobs(const VerifyJob* jobs, size_t n_jobs, size_t* j, size_t* off);
     uint64_t staged() const { return staged_; }
     void pack_staged(size_t lo, size_t hi);
@@ -166,7 +161,7 @@ private:
     DevBuf lmags_, lmags_hi_, tsave_, loc_idx_, found_;   // locate step
     DevBuf heavy_;       // count and keys of the buckets with many chunks (k_rlc_bucket_heavy)
     DevBuf aff_pts_, aff_suf_, aff_tp_, aff_meta_, binv_;   // affine chunk trees
-    HostBuf job_host_;   // pinned staging of verify_jobs_host
+    HostBuf job_host_;   // pinned staging of the staged jobs
     DevBuf keyhit_;      // key-table hits of the prep pass
     std::vector<VerifyJob> part_;   // the staged job pieces, and their first items
     std::vector<uint64_t> start_;

@@ -218,3 +218,32 @@ def test_rlc_job_kind_gating(gpu_ctx):
     assert not out.any()                       # s = 0 fails the strict parse
     assert L.ufsecp_gpu_ext_verify_jobs_noalloc(gpu_ctx.handle, tab.ctypes.data_as(P), 1, None) == \
         uf.UFSECP_ERR_BAD_INPUT
+
+
+def test_rlc_job_kind_beyond_one_pass(gpu_ctx):
+    """More kind 2 items than one RLC pass takes (2^24): the jobs are cut
+    between passes (one job straddles the boundary) and every verdict lands
+    in its own job's buffer.  Items are a GPU-signed, all-valid 2^20 corpus
+    tiled, with three invalid items (one flipped bit of s) on both sides of
+    the cut; verdicts by construction."""
+    import torch
+    from ultrafastsecp256k1_b200.autotune import signed_batch
+    base = 1 << 20
+    d_m, d_x, d_s = signed_batch(gpu_ctx, torch, 1, base, seed=97)
+    d_s.view(base, 64)[::50, 40] ^= 0x04   # undo signed_batch's flips: an all-valid corpus
+    m0, x0, s0 = (t.cpu().numpy().reshape(base, -1) for t in (d_m, d_x, d_s))
+    want0 = np.ones(base, np.uint8)
+    reps, extra = 16, 5000
+    n = reps * base + extra
+    m = np.concatenate([m0] * reps + [m0[:extra]])
+    x = np.concatenate([x0] * reps + [x0[:extra]])
+    s = np.concatenate([s0] * reps + [s0[:extra]])
+    want = np.concatenate([want0] * reps + [want0[:extra]])
+    for i in ((1 << 24) - 3, (1 << 24) + 11, n - 2):
+        s[i, 40] ^= 0x02
+        want[i] = 0
+    cut = (1 << 24) - 1000               # a job across the first pass's end
+    jobs = [(2, m[:cut], x[:cut], s[:cut]), (2, m[cut:cut + 3000], x[cut:cut + 3000], s[cut:cut + 3000]),
+            (2, m[cut + 3000:], x[cut + 3000:], s[cut + 3000:])]
+    got = np.concatenate(gpu_ctx.verify_jobs(jobs))
+    assert got.shape == want.shape and (got == want).all()

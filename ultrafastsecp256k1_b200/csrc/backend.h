@@ -114,10 +114,10 @@ public:
     // the tuning file's rlc_locate or UFSECP_B200_RLC_LOCATE may turn it off.
     bool rlc_locate() const { return rlc_locate_; }
     void set_rlc_locate(bool on) { rlc_locate_ = on; }
-    // Whether RLC bucket chunks (of at most 16 points) are summed in affine
-    // coordinates with block-shared inversions (k_rlc_chunks_aff) instead of
-    // mixed Jacobian additions.  On by default; the tuning file's rlc_affine
-    // or UFSECP_B200_RLC_AFFINE may turn it off.
+    // Whether RLC bucket chunks (of at most 16 points) are summed by affine
+    // pairwise trees with grid-shared inversions (k_aff_fwd / k_aff_bwd)
+    // instead of mixed Jacobian additions (k_rlc_chunks).  On by default; the
+    // tuning file's rlc_affine or UFSECP_B200_RLC_AFFINE may turn it off.
     bool rlc_affine() const { return rlc_affine_; }
     void set_rlc_affine(bool on) { rlc_affine_ = on; }
     int queue_grid() const { return queue_grid_; }

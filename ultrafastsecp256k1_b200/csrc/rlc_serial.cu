@@ -84,7 +84,7 @@ k_rlc_finish(RoundGeo g, const uint4* __restrict__ wins, const uint32_t* __restr
 // A bucket of more than kHeavyChunks chunks (skewed digits: the top windows
 // of a locate round's j-scaled magnitudes put most points of a segment into a
 // few buckets) is left to k_rlc_bucket_heavy: its key goes to `heavy`.
-// Adds a chunk partial: affine (Z = 1, from k_rlc_chunks_aff) or Jacobian.
+// Adds a chunk partial: affine (Z = 1, from the affine chunk trees) or Jacobian.
 template <bool kAff>
 __device__ __forceinline__ void add_partial(Jac& acc, const uint4* q) {
     Jac p;

@@ -65,6 +65,23 @@ typedef struct {
 UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_ext_job_t* jobs,
                                                      size_t n_jobs);
 
+/* One host-buffer batch over several contexts (no reference counterpart):
+ * the items are cut into n_ctx contiguous shares (the first count % n_ctx
+ * shares one item longer), each verified on its own context, in its own host
+ * thread, by ufsecp_gpu_ecdsa_verify_batch (kind 0, 33-byte keys) or
+ * ufsecp_gpu_schnorr_verify_batch (kind 1, 32-byte x-only keys).  Verdicts
+ * are per item, so no data crosses between devices; with one context per GPU
+ * the shares run on all of them at once.  The contexts must be distinct and
+ * not used by other threads during the call.  Gating as the single-context
+ * calls: NULL ctxs or a NULL context -> NULL_ARG, count 0 -> OK, n_ctx 0, a
+ * context listed twice, kind > 1 or count > 2^26 -> BAD_INPUT; the verdict
+ * buffer is cleared first and again after any share fails, whose code is
+ * returned (the first failing share's). */
+UFSECP_API ufsecp_error_t ufsecp_gpu_ext_verify_batch_sharded(ufsecp_gpu_ctx* const* ctxs, size_t n_ctx,
+                                                              uint32_t kind, const uint8_t* msg_hashes32,
+                                                              const uint8_t* pubkeys, const uint8_t* sigs64,
+                                                              size_t count, uint8_t* out_results);
+
 /* Host-side fault injection, for testing fail-closed behaviour (no
  * reference counterpart; nothing faults on the device).  Once armed, the
  * (after + 1)-th fault point the context crosses fails, and the injector

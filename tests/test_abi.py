@@ -5,6 +5,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 import ultrafastsecp256k1_b200 as uf
@@ -149,3 +150,19 @@ def test_reference_c_example_on_the_gpu():
     assert "generator_mul_batch not supported on this backend." in run.stdout
     assert "ecdsa_verify_batch returned: OK" in run.stdout
     assert "Done." in run.stdout
+
+
+def test_sharded_gating_without_contexts():
+    """ufsecp_gpu_ext_verify_batch_sharded's argument checks that need no context."""
+    L = uf.load_library()
+    buf = np.zeros(64 * 4, np.uint8)
+    out = np.full(4, 7, np.uint8)
+    nulls = (uf._vp * 2)(None, None)
+    a = (buf.ctypes.data, buf.ctypes.data, buf.ctypes.data, 4, out.ctypes.data)
+    assert L.ufsecp_gpu_ext_verify_batch_sharded(None, 1, 1, *a) == uf.UFSECP_ERR_NULL_ARG
+    assert L.ufsecp_gpu_ext_verify_batch_sharded(nulls, 2, 1, buf.ctypes.data, buf.ctypes.data, buf.ctypes.data, 0,
+                                                 out.ctypes.data) == uf.UFSECP_OK
+    assert L.ufsecp_gpu_ext_verify_batch_sharded(nulls, 0, 1, *a) == uf.UFSECP_ERR_BAD_INPUT
+    assert L.ufsecp_gpu_ext_verify_batch_sharded(nulls, 2, 2, *a) == uf.UFSECP_ERR_BAD_INPUT
+    assert L.ufsecp_gpu_ext_verify_batch_sharded(nulls, 2, 1, *a) == uf.UFSECP_ERR_NULL_ARG
+    assert (out == 7).all()                      # nothing checked later than the contexts was touched

@@ -140,6 +140,8 @@ _SIGS = {
     "ufsecp_gpu_ext_server_destroy": (None, [_vp]),
     "ufsecp_gpu_ext_rlc_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ufsecp_gpu_ext_rlc_key_hits": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "ufsecp_gpu_ext_verify_batch_sharded": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_size_t, ctypes.c_uint32,
+                                                           _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "ufsecp_gpu_ext_set_key_table": (ctypes.c_int, [_vp, ctypes.c_uint32]),
     "ufsecp_gpu_ext_set_rlc_locate": (ctypes.c_int, [_vp, ctypes.c_int]),
     "ufsecp_gpu_ext_rlc_located": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
@@ -250,6 +252,24 @@ def _job_table(jobs):
         o += _addr(out_all)
         o[tab["count"] == 0] = 0
     return tab, keep, out_all, [(t[6], t[2]) for t in meta]
+
+
+def verify_batch_sharded(ctxs, kind: int, msg_hashes32, pubkeys, sigs64) -> np.ndarray:
+    """ufsecp_gpu_ext_verify_batch_sharded: one host-buffer batch cut into
+    contiguous shares over the contexts in `ctxs` (GpuContext objects, e.g. one
+    per GPU), each share verified on its context in its own host thread;
+    kind 0 ECDSA (33-byte keys) / 1 BIP-340 (32-byte keys)."""
+    m, p, s = _flat_u8(msg_hashes32), _flat_u8(pubkeys), _flat_u8(sigs64)
+    n = m.size >> 5
+    out = np.zeros(max(1, n), np.uint8)
+    arr = (_vp * max(1, len(ctxs)))(*[c.handle for c in ctxs])
+    L = load_library()
+    rc = L.ufsecp_gpu_ext_verify_batch_sharded(arr, len(ctxs), kind, _addr(m) if n else None,
+                                               _addr(p) if n else None, _addr(s) if n else None, n,
+                                               _addr(out) if n else None)
+    if rc != UFSECP_OK:
+        raise UfsecpError(rc, "verify_batch_sharded")
+    return out[:n]
 
 
 def backend_count() -> int:

@@ -15,6 +15,7 @@
 #include <random>
 #include <algorithm>
 
+#include <thread>
 #include <vector>
 
 #include "backend.h"
@@ -522,6 +523,59 @@ ufsecp_error_t ufsecp_gpu_ext_verify_jobs(ufsecp_gpu_ctx* ctx, const ufsecp_gpu_
     if (rc != UFSECP_OK)
         for (size_t j = 0; j < n_jobs; ++j) clear_out(jobs[j].out_results, jobs[j].count, 1);
     return (ufsecp_error_t)rc;
+}
+
+ufsecp_error_t ufsecp_gpu_ext_verify_batch_sharded(ufsecp_gpu_ctx* const* ctxs, size_t n_ctx, uint32_t kind,
+                                                  const uint8_t* msg_hashes32, const uint8_t* pubkeys,
+                                                  const uint8_t* sigs64, size_t count, uint8_t* out_results) {
+    if (!ctxs) return UFSECP_ERR_NULL_ARG;
+    if (count == 0) return UFSECP_OK;
+    if (n_ctx == 0 || kind > 1 || count > kMaxBatch) return UFSECP_ERR_BAD_INPUT;
+    for (size_t k = 0; k < n_ctx; ++k) {
+        if (!ctxs[k]) return UFSECP_ERR_NULL_ARG;
+        for (size_t q = 0; q < k; ++q)
+            if (ctxs[q] == ctxs[k]) return UFSECP_ERR_BAD_INPUT;
+    }
+    if (!clear_out(out_results, count, 1)) return UFSECP_ERR_BAD_INPUT;
+    if (!msg_hashes32 || !pubkeys || !sigs64 || !out_results) return UFSECP_ERR_NULL_ARG;
+    const size_t ps = kind == 0 ? 33 : 32;
+    std::vector<ufsecp_error_t> rc(n_ctx, UFSECP_OK);
+    try {
+        std::vector<std::thread> th;
+        struct JoinAll {
+            std::vector<std::thread>& v;
+            ~JoinAll() {
+                for (std::thread& x : v)
+                    if (x.joinable()) x.join();
+            }
+        } join_all{th};
+        size_t off = 0;
+        for (size_t k = 0; k < n_ctx; ++k) {
+            const size_t share = count / n_ctx + (k < count % n_ctx ? 1 : 0);
+            if (share)
+                th.emplace_back([&, k, off, share]() {
+                    rc[k] = kind == 0 ? ufsecp_gpu_ecdsa_verify_batch(ctxs[k], msg_hashes32 + 32 * off,
+                                                                      pubkeys + ps * off, sigs64 + 64 * off, share,
+                                                                      out_results + off)
+                                      : ufsecp_gpu_schnorr_verify_batch(ctxs[k], msg_hashes32 + 32 * off,
+                                                                        pubkeys + ps * off, sigs64 + 64 * off, share,
+                                                                        out_results + off);
+                });
+            off += share;
+        }
+    } catch (const std::bad_alloc&) {
+        clear_out(out_results, count, 1);
+        return UFSECP_ERR_GPU_MEMORY;
+    } catch (...) {
+        clear_out(out_results, count, 1);
+        return UFSECP_ERR_INTERNAL;
+    }
+    for (size_t k = 0; k < n_ctx; ++k)
+        if (rc[k] != UFSECP_OK) {
+            clear_out(out_results, count, 1);
+            return rc[k];
+        }
+    return UFSECP_OK;
 }
 
 ufsecp_error_t ufsecp_gpu_ext_inject_fault(ufsecp_gpu_ctx* ctx, uint32_t after, int kind) {
